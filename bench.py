@@ -1,0 +1,318 @@
+#!/usr/bin/env python
+"""FDTD throughput benchmark: Mcell-updates/s of the Yee step loop on one B200 per rank.
+
+Workload (default): 512^3 cells (513^3 = 135,005,697 nodes), 1 mm cells, 10-cell CPML, 200
+seeded random dielectric spheres (radius 5-40 cells, eps_r U[1,10], sigma U[0,0.05] S/m), 20 % of
+them one-pole Debye (delta eps U[1,5], one seeded tau in [5,50] ps), one 50-ohm port driven by a
+Gaussian pulse (f0 10 GHz, fc 5 GHz). A step is one time step over the whole grid (fused E+H march,
+Debye ADE, source, port V/I probe). Fields are 6.5 GB per buffer set, far larger than the 126 MB
+L2, so no flush is needed between timed steps.
+
+value: whole-job nodes x steps / device time of the K timed steps (CUDA events on the session's
+stream, max over ranks). Ranks run independent replicas (weak scaling): the reference solves one
+grid on one device, and the north star keeps a grid on one GPU.
+
+--impl reference: the CPU baseline arm (rank 0 only): the oracle (a C++ restatement of the
+reference's own CPU FDTD, cpu.rs) on all host cores, on a bounded sample of full time steps of the
+same grid.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+BYTES_PER_NODE = 48  # read + write of Ex Ey Ez Hx Hy Hz, f32
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=2000)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--cells", type=int, default=512, help="cells per axis (512 is the benchmark workload)")
+    p.add_argument("--separate", action="store_true", help="time the unfused H and E kernels instead")
+    p.add_argument("--cpu-steps", type=int, default=8, help="full time steps the CPU baseline times")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-e2e", action="store_true")
+    return p.parse_args()
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "MEASURED_PEAKS.json hbm_gbs (of measured)"
+    except Exception:
+        return 6650.0, "profiling recipe fallback 6.65 TB/s (of fallback)"
+
+
+def workload(cells: int, steps: int, fused: bool = True):
+    from fieldgrid_b200 import workloads as W
+    pml = 10 if cells >= 256 else max(4, cells // 16)
+    count = 200 if cells >= 256 else max(8, cells // 3)
+    rmin, rmax = (5, 40) if cells >= 256 else (2, max(3, cells // 12))
+    return W.spheres(cells=cells, pml=pml, steps=steps, count=count, rmin=rmin, rmax=rmax, fused=fused)
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms while running."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_id: str):
+        self.path = tempfile.mktemp(prefix="clocks_", suffix=".csv")
+        self.proc = None
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", device_id, f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        rows = []
+        with open(self.path) as f:
+            for line in f:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) >= 8:
+                    rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return None
+        sm = [float(r[0]) for r in rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[q] for r in rows for q in range(4) if r[4 + q].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def device_id(local_rank: int) -> str:
+    try:
+        import torch
+        u = str(torch.cuda.get_device_properties(local_rank).uuid)
+        return u if u.startswith("GPU-") else "GPU-" + u
+    except Exception:
+        vis = os.environ.get("CUDA_VISIBLE_DEVICES", "")
+        ids = [v for v in vis.split(",") if v.strip()]
+        return ids[local_rank] if local_rank < len(ids) else str(local_rank)
+
+
+def traffic_for(variant: str, workload_name: str):
+    """DRAM bytes per launch of the dominant kernel from a committed ncu capture, when one exists
+    for this kernel variant and workload."""
+    path = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        e = d.get(variant, {}).get(workload_name)
+        return None if e is None else float(e)
+    except Exception:
+        return None
+
+
+def run_reference(args):
+    """The CPU arm: the oracle's State::step on the host cores."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    from oracle import oracle as O
+    sc = workload(args.cells, args.steps + args.warmup)
+    n = sc.grid.dims()
+    nn = n[0] * n[1] * n[2]
+    t = time.time()
+    osim = O.OracleSim(*sc.args(), bits=32)
+    setup_s = time.time() - t
+    k = max(1, min(args.steps, args.cpu_steps))
+    w = max(1, min(args.warmup, 1))
+    sec = O.time_steps(osim, 0, sc.pulse, sc.extras, w, k)
+    value = nn * k / sec / 1e6
+    cores = O.threads()
+    line = {
+        "impl": "reference", "metric": "Mcell-updates/s", "value": value, "unit": "Mcell/s", "n_gpus": args.gpus,
+        "steps": k, "warmup": w, "ms_per_step": 1e3 * sec / k, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": sc.name, "nodes": nn, "cells": sc.grid.cells(), "setup_s": round(setup_s, 2)},
+        "cpu_baseline": {"value": value, "unit": "Mcell/s", "cores": cores, "kind": "port",
+                         "sample": f"{k} full time steps of the {n[0]}x{n[1]}x{n[2]}-node grid after {w} warm-up "
+                                   f"step(s); C++ restatement of cpu.rs, OpenMP over x-planes"},
+        "e2e": {"value": value, "unit": "Mcell/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def cpu_baseline(args, sc):
+    from oracle import oracle as O
+    n = sc.grid.dims()
+    nn = n[0] * n[1] * n[2]
+    osim = O.OracleSim(*sc.args(), bits=32)
+    k = max(1, args.cpu_steps)
+    sec = O.time_steps(osim, 0, sc.pulse, sc.extras, 1, k)
+    del osim
+    return {"value": nn * k / sec / 1e6, "unit": "Mcell/s", "cores": O.threads(), "kind": "port",
+            "sample": f"{k} full time steps of the {n[0]}x{n[1]}x{n[2]}-node grid after 1 warm-up step; "
+                      f"C++ restatement of the reference's CPU FDTD (cpu.rs), OpenMP over x-planes"}
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1 and "OMP_NUM_THREADS" not in os.environ:
+        os.environ["OMP_NUM_THREADS"] = str(max(1, (os.cpu_count() or 8) // world))
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=torch.device("cuda", local))
+
+    from fieldgrid_b200 import fdtd
+    from fieldgrid_b200.gpu import Gpu, Options
+
+    K, W = args.steps, max(args.warmup, 3)
+    kt_steps = 10
+    t = time.time()
+    sc = workload(args.cells, W + K + kt_steps, fused=not args.separate)
+    t_mat = time.time() - t
+    t = time.time()
+    sim = fdtd.Sim.try_new(*sc.args())
+    t_setup = time.time() - t
+    n = sim.dims()
+    nn = n[0] * n[1] * n[2]
+    g = Gpu.open(Options(device=local))
+    t = time.time()
+    s = fdtd.Session(g, sim, 0, sc.pulse, sc.extras)
+    t_session = time.time() - t
+    log(f"rank {rank}: {sc.name}, {nn} nodes, classes {sim.coef_classes()}, debye edges {sim.count('debye_edges')}, "
+        f"materials {t_mat:.1f}s setup {t_setup:.1f}s upload {t_session:.2f}s, {s.variant}")
+    stream = torch.cuda.ExternalStream(s.stream)
+    s.step(W)
+    s.sync()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    sampler = ClockSampler(device_id(local))
+    time.sleep(0.3)
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    s.step(K)
+    ev1.record(stream)
+    ev1.synchronize()
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    if world > 1:
+        dist.barrier()
+    ms = ev0.elapsed_time(ev1)
+    t_max = torch.tensor([ms], device="cuda", dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(t_max, op=dist.ReduceOp.MAX)
+    ms_max = float(t_max.item())
+    value = world * nn * K / (ms_max / 1e3) / 1e6
+
+    # per-kernel device times of the same step (events between eager launches)
+    kt = s.kernel_times(kt_steps)
+    launches = s.launches_per_step
+    energy = s.energy()
+    variant = s.variant
+    classes = sim.coef_classes()
+    debye_edges = sim.count("debye_edges")
+    s.close()
+    dom_name, dom_ms = max(kt.items(), key=lambda x: x[1])
+    peak, peak_src = measured_peaks()
+    achieved = BYTES_PER_NODE * nn / (dom_ms / 1e3) / 1e9
+    total_kt = sum(kt.values())
+
+    e2e = None
+    if not args.no_e2e:
+        import copy
+        ex = copy.copy(sc.extras)
+        ex.max_steps = K
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        t0 = time.perf_counter()
+        rec = fdtd.run(g, sim, 0, sc.pulse, ex)
+        torch.cuda.synchronize()
+        t_e2e = time.perf_counter() - t0
+        te = torch.tensor([t_e2e], device="cuda", dtype=torch.float64)
+        if world > 1:
+            dist.all_reduce(te, op=dist.ReduceOp.MAX)
+        t_e2e = float(te.item())
+        e2e = {"value": world * nn * K / t_e2e / 1e6, "unit": "Mcell/s",
+               "h2d_bytes_per_step": rec.h2d / K, "d2h_bytes_per_step": rec.d2h / K,
+               "run": f"one fg_run of {K} steps on host buffers: pack + upload of the grid, the steps, energy checks "
+                      f"every {ex.check_every or 1000}, read-back of the series; wall clock, max over ranks",
+               "h2d_bytes_per_run": rec.h2d, "d2h_bytes_per_run": rec.d2h}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        del sim
+        cpu = cpu_baseline(args, sc)
+
+    if rank == 0:
+        line = {
+            "metric": "Mcell-updates/s", "value": value, "unit": "Mcell/s", "n_gpus": world, "steps": K,
+            "warmup": W, "ms_per_step": ms_max / K, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": sc.name, "nodes": nn, "cells": sc.grid.cells(), "pml": sc.info.get("pml"),
+                       "spheres": sc.info.get("spheres"), "parallelism": f"replicas x{world}",
+                       "l2": "inputs larger than L2 (6.5 GB of fields per buffer set)",
+                       "variant": variant, "coef_classes": classes, "debye_edges": debye_edges,
+                       "launches_per_step": launches, "setup_s": round(t_setup, 2)},
+            "hbm_fraction_of_algorithmic": BYTES_PER_NODE * value * 1e6 / world / 1e9 / peak,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": traffic_for(dom_name, sc.name), "kernel": dom_name,
+                         "bytes_per_launch": BYTES_PER_NODE * nn, "kernel_ms": dom_ms, "peak_source": peak_src},
+            "kernel_ms": {k: round(v, 5) for k, v in kt.items()},
+            "kernel_share": {k: round(v / total_kt, 4) for k, v in kt.items()},
+            "gpu_launches": launches * K,
+            "clocks": clocks,
+            "e2e": e2e,
+            "cpu_baseline": cpu,
+            "energy_after": energy,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,680 @@
+// The device side of one run: buffers in HBM, the per-step kernel sequence, CUDA-graph capture of
+// the step loop, energy checks and read-back. This is the B200 counterpart of run.rs:390-758
+// (buffers, pipelines, dispatch loop) with pack() (run.rs:205-376) folded into session_new.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <set>
+#include <string>
+#include <vector>
+
+#include "../../include/fieldgrid.h"
+#include "engine.hpp"
+#include "kernels.cuh"
+#include "stencil_fused.cuh"
+#include "stencil_separate.cuh"
+
+namespace fg {
+
+#define FG_CUDA(call)                                                                              \
+    do {                                                                                           \
+        cudaError_t e_ = (call);                                                                   \
+        if (e_ != cudaSuccess) {                                                                   \
+            err = std::string(#call) + ": " + cudaGetErrorString(e_);                              \
+            return FG_ERR_CUDA;                                                                    \
+        }                                                                                          \
+    } while (0)
+
+int gpu_open(int device, Gpu** out, std::string& err) {
+    *out = nullptr;
+    int count = 0;
+    cudaError_t e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess || count == 0) {
+        err = std::string("no CUDA device: ") + (e != cudaSuccess ? cudaGetErrorString(e) : "none found");
+        return FG_ERR_NO_DEVICE;
+    }
+    if (device < 0) device = 0;
+    if (device >= count) {
+        err = "CUDA device " + std::to_string(device) + " does not exist";
+        return FG_ERR_NO_DEVICE;
+    }
+    FG_CUDA(cudaSetDevice(device));
+    cudaDeviceProp prop;
+    FG_CUDA(cudaGetDeviceProperties(&prop, device));
+    auto* g = new Gpu;
+    g->device = device;
+    g->name = prop.name;
+    *out = g;
+    return FG_OK;
+}
+
+void gpu_close(Gpu* g) { delete g; }
+
+struct Session {
+    Gpu* gpu = nullptr;
+    cudaStream_t stream = nullptr;
+    Geom geom{};
+    StepConst sc{};
+    bool fused = true;
+    int cid_bytes = 1;
+    // device buffers (sub-allocations of one arena)
+    char* arena = nullptr;
+    size_t arena_bytes = 0;
+    float *e = nullptr, *h = nullptr, *e2 = nullptr, *h2 = nullptr;
+    float *psi = nullptr, *psi_h2 = nullptr;
+    void* node_class = nullptr;
+    Coef* classes = nullptr;
+    AxisNode* axes = nullptr;
+    unsigned* counter = nullptr;
+    float* series = nullptr;
+    float* plane = nullptr;
+    float* ntff = nullptr;
+    unsigned* patch = nullptr;
+    DevSource* sources = nullptr;
+    DevInductor* inductors = nullptr;
+    DevProbe* probes = nullptr;
+    DevPortEdge* port_edges = nullptr;
+    DevLoop* loops = nullptr;
+    DevWire* wires = nullptr;
+    DevSheet* sheets = nullptr;
+    float* branch = nullptr;
+    float* currents = nullptr;
+    long long* debye_f = nullptr;
+    float* debye_dd = nullptr;
+    float* debye_old = nullptr;
+    float* debye_state = nullptr;
+    float* debye_table = nullptr;
+    double* partial = nullptr;
+    // counts
+    int n_sources = 0, n_inductors = 0, n_ports = 0, n_wires = 0, n_sheets = 0, n_debye = 0, n_patches = 0;
+    int plane_k = 0;
+    uint64_t plane_len = 0, ntff_len = 0, series_len = 0;
+    long long psi_total = 0;
+    double t0 = 0, tau = 0;
+    uint64_t steps = 0;
+    uint64_t launches = 0;
+    FusedShape shape{};
+    std::string variant;
+    uint64_t h2d_bytes = 0, d2h_bytes = 0;
+    // when set, enqueue_step records an event before every launch (per-kernel timing)
+    std::vector<std::pair<const char*, cudaEvent_t>>* marks = nullptr;
+    // graphs
+    int graph_steps = 0;
+    cudaGraphExec_t graph_many = nullptr;
+    cudaGraphExec_t graph_two = nullptr;   // an even pair, for the ping-pong parity
+    cudaGraphExec_t graph_one[2] = {nullptr, nullptr};
+};
+
+static constexpr int ENERGY_BLOCKS = 1024;
+
+namespace {
+
+template <typename T>
+T* carve(char*& cur, size_t count) {
+    T* p = reinterpret_cast<T*>(cur);
+    size_t bytes = ((count * sizeof(T)) + 255) & ~size_t(255);
+    cur += std::max<size_t>(bytes, 256);
+    return p;
+}
+
+size_t carve_size(size_t bytes) { return std::max<size_t>((bytes + 255) & ~size_t(255), 256); }
+
+// One time step. `parity` selects the ping-pong direction of the fused step (input = parity 0
+// buffers on even steps). The separate step updates in place.
+int enqueue_step(Session& s, int parity, std::string& err) {
+    const Geom& g = s.geom;
+    cudaStream_t st = s.stream;
+    auto mark = [&](const char* name) {
+        if (!s.marks) return;
+        cudaEvent_t ev;
+        cudaEventCreate(&ev);
+        cudaEventRecord(ev, st);
+        s.marks->push_back({name, ev});
+    };
+    float *e_in = s.e, *h_in = s.h, *e_out = s.e, *h_out = s.h;
+    if (s.fused && parity) { e_in = s.e2; h_in = s.h2; e_out = s.e; h_out = s.h; }
+    else if (s.fused) { e_out = s.e2; h_out = s.h2; }
+    if (!s.fused) {
+        dim3 blk(64, 4, 1), grd((g.n2 + 63) / 64, (g.n1 + 3) / 4, g.n0);
+        mark("update_h");
+        k_update_h<<<grd, blk, 0, st>>>(g, s.e, s.h, s.psi, s.sc.k_mu, s.counter);
+        if (s.n_wires) { mark("wire_h"); k_wire_h<<<(s.n_wires + 127) / 128, 128, 0, st>>>(s.wires, s.n_wires, s.e, s.h); }
+        if (s.n_sheets) { mark("sheet_pre"); k_sheet_pre<<<(s.n_sheets + 127) / 128, 128, 0, st>>>(s.sheets, s.n_sheets, s.e, s.h); }
+        if (s.n_debye) { mark("debye_pre"); k_debye_pre<<<(s.n_debye + 255) / 256, 256, 0, st>>>(s.debye_f, s.n_debye, s.e, s.debye_old); }
+        mark("update_e");
+        switch (s.cid_bytes) {
+            case 1: k_update_e<uint8_t><<<grd, blk, 0, st>>>(g, (const uint8_t*)s.node_class, s.classes, s.h, s.e, s.psi); break;
+            case 2: k_update_e<uint16_t><<<grd, blk, 0, st>>>(g, (const uint16_t*)s.node_class, s.classes, s.h, s.e, s.psi); break;
+            default: k_update_e<uint32_t><<<grd, blk, 0, st>>>(g, (const uint32_t*)s.node_class, s.classes, s.h, s.e, s.psi); break;
+        }
+    } else {
+        if (s.n_wires) {
+            // thin-wire terms join H before the march reads it (run.rs:620-623); E is the step's input
+            mark("wire_h");
+            k_wire_h<<<(s.n_wires + 127) / 128, 128, 0, st>>>(s.wires, s.n_wires, e_in, h_in);
+        }
+        mark("fused_step");
+        int rc = launch_fused(s.shape, s.cid_bytes, g, s.node_class, s.classes, e_in, h_in, e_out, h_out, s.psi,
+                              parity ? s.psi_h2 : s.psi, parity ? s.psi : s.psi_h2, s.sc.k_mu, s.counter,
+                              s.n_wires > 0, st);
+        if (rc) { err = "fused step launch failed"; return FG_ERR_CUDA; }
+        if (s.n_sheets) {
+            mark("sheet_pre");
+            k_sheet_pre<<<(s.n_sheets + 127) / 128, 128, 0, st>>>(s.sheets, s.n_sheets, e_in, h_out);
+        }
+    }
+    float* e_now = s.fused ? e_out : s.e;
+    float* h_now = s.fused ? h_out : s.h;
+    if (s.n_sheets) mark("sheet_post");
+    if (s.n_sheets) k_sheet_post<<<(s.n_sheets + 127) / 128, 128, 0, st>>>(s.sheets, s.n_sheets, s.branch, s.currents, e_now);
+    if (s.n_debye) {
+        mark("debye_post");
+        const float* saved = s.fused ? nullptr : s.debye_old;
+        switch (s.cid_bytes) {
+            case 1: k_debye_post<uint8_t><<<(s.n_debye + 255) / 256, 256, 0, st>>>(s.debye_f, s.debye_dd, s.n_debye, saved, e_in, (const uint8_t*)s.node_class, s.classes, g.cs, s.debye_table, s.debye_state, e_now); break;
+            case 2: k_debye_post<uint16_t><<<(s.n_debye + 255) / 256, 256, 0, st>>>(s.debye_f, s.debye_dd, s.n_debye, saved, e_in, (const uint16_t*)s.node_class, s.classes, g.cs, s.debye_table, s.debye_state, e_now); break;
+            default: k_debye_post<uint32_t><<<(s.n_debye + 255) / 256, 256, 0, st>>>(s.debye_f, s.debye_dd, s.n_debye, saved, e_in, (const uint32_t*)s.node_class, s.classes, g.cs, s.debye_table, s.debye_state, e_now); break;
+        }
+    }
+    if (s.n_sources || s.n_inductors) mark("lumped");
+    if (s.n_sources || s.n_inductors) k_lumped<<<1, 256, 0, st>>>(s.sources, s.n_sources, s.inductors, s.n_inductors, s.sc, s.counter, e_now);
+    if (s.n_ports) mark("probe");
+    if (s.n_ports) k_probe<<<s.n_ports, 256, 0, st>>>(s.probes, s.port_edges, s.loops, g.cs, e_now, h_now, s.counter, s.sc, s.series);
+    if (s.plane_len) {
+        long long q = (long long)g.n0 * g.n1;
+        mark("field_dft");
+        k_field_dft<<<unsigned((q + 127) / 128), 128, 0, st>>>(g, s.plane_k, s.sc, s.counter, e_now, h_now, s.plane);
+    }
+    if (s.ntff_len) mark("ntff");
+    if (s.ntff_len) k_ntff<<<(s.n_patches + 127) / 128, 128, 0, st>>>(s.patch, s.n_patches, g.cs, s.sc, s.counter, e_now, h_now, s.ntff);
+    mark(nullptr);
+    return FG_OK;
+}
+
+uint64_t count_launches(const Session& s) {
+    uint64_t n = 1;  // the field update (fused) or H update (separate)
+    if (!s.fused) n += 1 + (s.n_debye ? 1 : 0);
+    if (s.n_wires) n++;
+    if (s.n_sheets) n += 2;
+    if (s.n_debye) n++;
+    if (s.n_sources || s.n_inductors) n++;
+    if (s.n_ports) n++;
+    if (s.plane_len) n++;
+    if (s.ntff_len) n++;
+    return n;
+}
+
+int capture(Session& s, int steps, int parity0, cudaGraphExec_t* out, std::string& err) {
+    cudaGraph_t graph;
+    FG_CUDA(cudaStreamBeginCapture(s.stream, cudaStreamCaptureModeThreadLocal));
+    int rc = FG_OK;
+    for (int q = 0; q < steps && rc == FG_OK; ++q) rc = enqueue_step(s, (parity0 + q) & 1, err);
+    cudaError_t ce = cudaStreamEndCapture(s.stream, &graph);
+    if (rc) return rc;
+    if (ce != cudaSuccess) { err = std::string("cudaStreamEndCapture: ") + cudaGetErrorString(ce); return FG_ERR_CUDA; }
+    ce = cudaGraphInstantiate(out, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ce != cudaSuccess) { err = std::string("cudaGraphInstantiate: ") + cudaGetErrorString(ce); return FG_ERR_CUDA; }
+    return FG_OK;
+}
+
+}  // namespace
+
+int session_new(Gpu* gpu, const HostSim& sim, const RunSpec& rs, Session** out, std::string& err) {
+    *out = nullptr;
+    if (!gpu) { err = "no GPU: this engine has no CPU path"; return FG_ERR_NO_DEVICE; }
+    FG_CUDA(cudaSetDevice(gpu->device));
+    if (rs.driven >= sim.port_src.size()) { err = "the driven port does not exist"; return FG_ERR_INVALID; }
+    auto s = std::make_unique<Session>();
+    s->gpu = gpu;
+    s->fused = rs.fused;
+    const size_t n0 = sim.n[0], n1 = sim.n[1], n2 = sim.n[2], nn = sim.nn;
+    if (n0 >= (1u << 31) || n1 >= (1u << 31) || n2 >= (1u << 31)) { err = "grid dimension too large"; return FG_ERR_INVALID; }
+    Geom& g = s->geom;
+    g.n0 = int(n0); g.n1 = int(n1); g.n2 = int(n2);
+    g.pml = int(sim.pml);
+    g.nn = (long long)nn;
+    g.cs = (long long)((nn + 31) & ~size_t(31));
+    const long long cs = g.cs;
+    auto fidx = [&](uint64_t key) { return (long long)(key / nn) * cs + (long long)(key % nn); };
+
+    // psi slabs (run.rs:214-225)
+    long long psi_total = 0;
+    for (int e = 0; e < 2; ++e)
+        for (int c = 0; c < 3; ++c)
+            for (int a = 0; a < 3; ++a) {
+                g.psi_off[e * 9 + c * 3 + a] = psi_total;
+                if (a != c && sim.pml > 0) {
+                    size_t m[3] = {n0, n1, n2};
+                    m[a] = 2 * sim.pml;
+                    psi_total += (long long)(m[0] * m[1] * m[2]);
+                }
+            }
+    s->psi_total = psi_total;
+    const long long psi_h = psi_total - g.psi_off[9];  // the H slabs, ping-ponged in the fused step
+
+    // class ids narrowed to the smallest width that holds them
+    const size_t ncls = sim.classes.size();
+    s->cid_bytes = ncls <= 256 ? 1 : (ncls <= 65536 ? 2 : 4);
+
+    // sparse lists (pack, run.rs:243-340)
+    std::vector<DevSource> src;
+    for (auto& q : sim.port_src[rs.driven]) src.push_back(DevSource{(long long)q.comp * cs + (long long)q.id, q.src});
+    std::vector<DevInductor> ind;
+    for (auto& q : sim.inductors) ind.push_back(DevInductor{(long long)q.comp * cs + (long long)q.id, q.ke, q.ki, 0.f});
+    std::vector<DevWire> wires;
+    for (auto& w : sim.wires) {
+        DevWire d;
+        d.h = fidx(w.h);
+        for (int t = 0; t < 4; ++t) { d.e[t] = fidx(w.e[t]); d.c[t] = w.c[t]; }
+        wires.push_back(d);
+    }
+    std::vector<DevSheet> sheets;
+    for (auto& q : sim.sheets) {  // run.rs:261-289: z-directed sheets and k == 0 are skipped
+        if (q.comp == 2 || q.id % n2 == 0) continue;
+        long long hc = q.comp == 0 ? 1 : 0;
+        DevSheet d{};
+        d.f = (long long)q.comp * cs + (long long)q.id;
+        d.ha = hc * cs + (long long)q.id;
+        d.hb = hc * cs + (long long)q.id - 1;
+        d.len = float(q.len);
+        d.c = float(q.c);
+        d.r = float(q.r);
+        d.adaptive = q.adaptive ? 1.f : 0.f;
+        d.ma = 0.5f;
+        d.mb = 0.5f;
+        d.face_a = unsigned(q.faces[0]);
+        d.face_b = unsigned(q.faces[1]);
+        sheets.push_back(d);
+    }
+    std::vector<long long> debye_f;
+    std::vector<float> debye_dd;
+    for (auto& q : sim.debye_edges) {
+        debye_f.push_back((long long)q.comp * cs + (long long)q.id);
+        debye_dd.push_back(float(q.dd));
+    }
+    std::vector<float> debye_table{float(sim.poles.size())};
+    for (auto& [x, a] : sim.poles) {
+        double d = 1.0 + 0.5 * x * sim.dt;
+        debye_table.push_back(float((1.0 - 0.5 * x * sim.dt) / d));
+        debye_table.push_back(float(EPS0 * a * x / d));
+    }
+    std::vector<DevProbe> probes;
+    std::vector<DevPortEdge> pedges;
+    std::vector<DevLoop> loops;
+    for (auto& p : sim.ports) {  // run.rs:305-340 with port_loop (run.rs:102-127)
+        const int axis = int(p.columns[0][0].comp);
+        const int u = (axis + 1) % 3, v = (axis + 2) % 3;
+        const auto& mid = p.columns[p.columns.size() / 2];
+        DevProbe d{axis, int(pedges.size()), 0, int(loops.size()), 0};
+        const double polarity = p.reference_above ? -1.0 : 1.0;
+        const double weight = polarity / double(p.columns.size());
+        for (auto& col : p.columns)
+            for (auto& e : col)
+                pedges.push_back(DevPortEdge{(long long)sim.idx(e.at[0], e.at[1], e.at[2]),
+                                             float(sim.ax[axis].d[e.at[axis]] * weight)});
+        d.count = int(pedges.size()) - d.first;
+        double height = 0.0;
+        for (auto& e : mid) height += sim.ax[axis].d[e.at[axis]];
+        std::set<std::pair<size_t, size_t>> nodes;
+        for (auto& c : p.columns) nodes.insert({c[0].at[u], c[0].at[v]});
+        for (auto& e : mid) {
+            const size_t k = e.at[axis];
+            const double share = polarity * sim.ax[axis].d[k] / height;
+            auto at = [&](size_t a, size_t b) {
+                size_t q[3];
+                q[u] = a; q[v] = b; q[axis] = k;
+                return sim.idx(q[0], q[1], q[2]);
+            };
+            std::map<std::pair<size_t, int>, int> turns;
+            for (auto [a, b] : nodes) {
+                turns[{at(a, b), v}] += 1;
+                turns[{at(a - 1, b), v}] -= 1;
+                turns[{at(a, b), u}] -= 1;
+                turns[{at(a, b - 1), u}] += 1;
+            }
+            for (auto& [kc, t] : turns) {
+                if (t == 0) continue;
+                const size_t id = kc.first;
+                const int comp = kc.second;
+                const size_t pc = comp == 0 ? id / (n1 * n2) : (comp == 1 ? (id / n2) % n1 : id % n2);
+                const double w = double(t) * sim.ax[comp].dd[pc];
+                loops.push_back(DevLoop{(long long)comp * cs + (long long)id, float(w * share)});
+            }
+        }
+        d.loop_count = int(loops.size()) - d.loop_first;
+        probes.push_back(d);
+    }
+    for (auto& q : pedges)
+        if (float(q.id) >= float(1u << 24)) { err = "grid too large for f32 port indices"; return FG_ERR_PORT_INDEX; }
+
+    pulse_shape(rs.fc, s->t0, s->tau);
+    StepConst& sc = s->sc;
+    sc.k_mu = float(sim.dt / MU0);
+    sc.dt = float(sim.dt);
+    sc.t0 = float(s->t0);
+    sc.tau = float(s->tau);
+    sc.w0 = float(2.0 * PI * rs.f0);
+    sc.nf = int(std::min<size_t>(rs.freqs.size(), 4));
+    for (int q = 0; q < 4; ++q) sc.omega[q] = q < sc.nf ? float(2.0 * PI * rs.freqs[q]) : 0.f;
+    sc.cap = unsigned(std::min<uint64_t>(rs.max_steps, 0xffffffffu));
+    sc.ports = int(sim.ports.size());
+    s->n_sources = int(src.size());
+    s->n_inductors = int(ind.size());
+    s->n_ports = int(probes.size());
+    s->n_wires = int(wires.size());
+    s->n_sheets = int(sheets.size());
+    s->n_debye = int(debye_f.size());
+    s->plane_k = int(rs.has_plane_k ? rs.plane_k : 0);
+    s->plane_len = rs.has_plane_k ? uint64_t(n0) * n1 * sc.nf * 10 : 0;
+    if (rs.has_plane_k && rs.plane_k >= n2) { err = "plane_k is outside the grid"; return FG_ERR_INVALID; }
+    s->n_patches = rs.has_ntff ? int(rs.ntff.size() / 13) : 0;
+    s->ntff_len = (s->n_patches > 0 && sc.nf > 0) ? uint64_t(s->n_patches) * sc.nf * 12 : 0;
+    for (size_t q = 0; q < size_t(s->n_patches) * 13; ++q)
+        if (q % 13 != 0 && rs.ntff[q] >= nn) { err = "an NTFF patch index is outside the grid"; return FG_ERR_INVALID; }
+    s->series_len = uint64_t(sc.cap) * sc.ports * 2;
+    const size_t states = sim.sheet_states;
+    const size_t nr_nc = sim.sheet_table.size() >= 2 ? size_t(sim.sheet_table[0]) + 2 * size_t(sim.sheet_table[1]) : 0;
+    (void)states;
+
+    // size the arena
+    const size_t fields = size_t(3 * cs);
+    size_t need = 0;
+    const int field_sets = s->fused ? 2 : 1;
+    need += carve_size(fields * 4) * 2 * field_sets;
+    need += carve_size(size_t(std::max<long long>(psi_total, 1)) * 4);
+    if (s->fused) need += carve_size(size_t(std::max<long long>(psi_h, 1)) * 4);
+    need += carve_size(nn * size_t(s->cid_bytes));
+    need += carve_size(ncls * sizeof(Coef));
+    need += carve_size((n0 + n1 + n2) * sizeof(AxisNode));
+    need += carve_size(64);
+    need += carve_size(std::max<uint64_t>(s->series_len, 1) * 4);
+    need += carve_size(std::max<uint64_t>(s->plane_len, 1) * 4);
+    need += carve_size(std::max<uint64_t>(s->ntff_len, 1) * 4);
+    need += carve_size(std::max<size_t>(rs.ntff.size(), 1) * 4);
+    need += carve_size(std::max<size_t>(src.size(), 1) * sizeof(DevSource));
+    need += carve_size(std::max<size_t>(ind.size(), 1) * sizeof(DevInductor));
+    need += carve_size(std::max<size_t>(probes.size(), 1) * sizeof(DevProbe));
+    need += carve_size(std::max<size_t>(pedges.size(), 1) * sizeof(DevPortEdge));
+    need += carve_size(std::max<size_t>(loops.size(), 1) * sizeof(DevLoop));
+    need += carve_size(std::max<size_t>(wires.size(), 1) * sizeof(DevWire));
+    need += carve_size(std::max<size_t>(sheets.size(), 1) * sizeof(DevSheet));
+    need += carve_size(std::max<size_t>(sim.sheet_table.size(), 1) * 4);
+    need += carve_size(std::max<size_t>(sheets.size() * nr_nc, 1) * 4);
+    need += carve_size(std::max<size_t>(debye_f.size(), 1) * 8);
+    need += carve_size(std::max<size_t>(debye_f.size(), 1) * 4) * 2;
+    need += carve_size(std::max<size_t>(debye_f.size() * sim.poles.size(), 1) * 4);
+    need += carve_size(debye_table.size() * 4);
+    need += carve_size(ENERGY_BLOCKS * 8);
+    size_t free_b = 0, total_b = 0;
+    FG_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    if (need + (size_t(256) << 20) > free_b) {
+        err = std::to_string(sim.cells()) + " cells is more than this GPU can hold";
+        return FG_ERR_TOO_LARGE;
+    }
+    FG_CUDA(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
+    FG_CUDA(cudaMalloc(&s->arena, need));
+    s->arena_bytes = need;
+    char* cur = s->arena;
+    s->e = carve<float>(cur, fields);
+    s->h = carve<float>(cur, fields);
+    if (s->fused) { s->e2 = carve<float>(cur, fields); s->h2 = carve<float>(cur, fields); }
+    s->psi = carve<float>(cur, size_t(std::max<long long>(psi_total, 1)));
+    if (s->fused) {
+        // the H slabs of the second set live at psi_h2 - psi_off[9] so the same offsets apply
+        float* hb = carve<float>(cur, size_t(std::max<long long>(psi_h, 1)));
+        s->psi_h2 = hb - g.psi_off[9];
+    }
+    s->node_class = carve<char>(cur, nn * size_t(s->cid_bytes));
+    s->classes = carve<Coef>(cur, ncls);
+    s->axes = carve<AxisNode>(cur, n0 + n1 + n2);
+    s->counter = carve<unsigned>(cur, 16);
+    s->series = carve<float>(cur, std::max<uint64_t>(s->series_len, 1));
+    s->plane = carve<float>(cur, std::max<uint64_t>(s->plane_len, 1));
+    s->ntff = carve<float>(cur, std::max<uint64_t>(s->ntff_len, 1));
+    s->patch = carve<unsigned>(cur, std::max<size_t>(rs.ntff.size(), 1));
+    s->sources = carve<DevSource>(cur, std::max<size_t>(src.size(), 1));
+    s->inductors = carve<DevInductor>(cur, std::max<size_t>(ind.size(), 1));
+    s->probes = carve<DevProbe>(cur, std::max<size_t>(probes.size(), 1));
+    s->port_edges = carve<DevPortEdge>(cur, std::max<size_t>(pedges.size(), 1));
+    s->loops = carve<DevLoop>(cur, std::max<size_t>(loops.size(), 1));
+    s->wires = carve<DevWire>(cur, std::max<size_t>(wires.size(), 1));
+    s->sheets = carve<DevSheet>(cur, std::max<size_t>(sheets.size(), 1));
+    s->branch = carve<float>(cur, std::max<size_t>(sim.sheet_table.size(), 1));
+    s->currents = carve<float>(cur, std::max<size_t>(sheets.size() * nr_nc, 1));
+    s->debye_f = carve<long long>(cur, std::max<size_t>(debye_f.size(), 1));
+    s->debye_dd = carve<float>(cur, std::max<size_t>(debye_f.size(), 1));
+    s->debye_old = carve<float>(cur, std::max<size_t>(debye_f.size(), 1));
+    s->debye_state = carve<float>(cur, std::max<size_t>(debye_f.size() * sim.poles.size(), 1));
+    s->debye_table = carve<float>(cur, debye_table.size());
+    s->partial = carve<double>(cur, ENERGY_BLOCKS);
+    if (size_t(cur - s->arena) > need) { err = "internal: arena overflow"; return FG_ERR_INVALID; }
+
+    cudaStream_t st = s->stream;
+    FG_CUDA(cudaMemsetAsync(s->arena, 0, need, st));
+    // node classes, narrowed on the host in parallel
+    {
+        std::vector<uint8_t> narrow(nn * size_t(s->cid_bytes));
+        const uint32_t* src_c = sim.node_class.data();
+        if (s->cid_bytes == 1) {
+#pragma omp parallel for schedule(static)
+            for (long long q = 0; q < (long long)nn; ++q) narrow[q] = uint8_t(src_c[q]);
+        } else if (s->cid_bytes == 2) {
+            uint16_t* d = reinterpret_cast<uint16_t*>(narrow.data());
+#pragma omp parallel for schedule(static)
+            for (long long q = 0; q < (long long)nn; ++q) d[q] = uint16_t(src_c[q]);
+        } else {
+            std::memcpy(narrow.data(), src_c, nn * 4);
+        }
+        FG_CUDA(cudaMemcpyAsync(s->node_class, narrow.data(), narrow.size(), cudaMemcpyHostToDevice, st));
+        s->h2d_bytes += narrow.size();
+        FG_CUDA(cudaStreamSynchronize(st));
+    }
+    FG_CUDA(cudaMemcpyAsync(s->classes, sim.classes.data(), ncls * sizeof(Coef), cudaMemcpyHostToDevice, st));
+    std::vector<AxisNode> axes;
+    for (int a = 0; a < 3; ++a) axes.insert(axes.end(), sim.ax[a].node.begin(), sim.ax[a].node.end());
+    FG_CUDA(cudaMemcpyAsync(s->axes, axes.data(), axes.size() * sizeof(AxisNode), cudaMemcpyHostToDevice, st));
+    g.ax[0] = s->axes;
+    g.ax[1] = s->axes + n0;
+    g.ax[2] = s->axes + n0 + n1;
+    s->h2d_bytes += ncls * sizeof(Coef) + axes.size() * sizeof(AxisNode);
+    auto up = [&](void* dst, const void* srcp, size_t bytes) -> int {
+        s->h2d_bytes += bytes;
+        if (bytes) FG_CUDA(cudaMemcpyAsync(dst, srcp, bytes, cudaMemcpyHostToDevice, st));
+        return FG_OK;
+    };
+    int rc = FG_OK;
+    rc |= up(s->patch, rs.ntff.data(), rs.ntff.size() * 4);
+    rc |= up(s->sources, src.data(), src.size() * sizeof(DevSource));
+    rc |= up(s->inductors, ind.data(), ind.size() * sizeof(DevInductor));
+    rc |= up(s->probes, probes.data(), probes.size() * sizeof(DevProbe));
+    rc |= up(s->port_edges, pedges.data(), pedges.size() * sizeof(DevPortEdge));
+    rc |= up(s->loops, loops.data(), loops.size() * sizeof(DevLoop));
+    rc |= up(s->wires, wires.data(), wires.size() * sizeof(DevWire));
+    rc |= up(s->sheets, sheets.data(), sheets.size() * sizeof(DevSheet));
+    rc |= up(s->branch, sim.sheet_table.data(), sim.sheet_table.size() * 4);
+    rc |= up(s->debye_f, debye_f.data(), debye_f.size() * 8);
+    rc |= up(s->debye_dd, debye_dd.data(), debye_dd.size() * 4);
+    rc |= up(s->debye_table, debye_table.data(), debye_table.size() * 4);
+    if (rc) return FG_ERR_CUDA;
+    FG_CUDA(cudaStreamSynchronize(st));
+
+    s->shape = choose_shape(g, s->cid_bytes, s->n_wires > 0);
+    s->variant = s->fused ? fused_name(s->shape) : std::string("separate H+E, 64x4 threads");
+    s->launches = count_launches(*s);
+    // graphs: a block of even length (the fused step alternates buffers), a pair and singles
+    s->graph_steps = 32;
+    rc = capture(*s, s->graph_steps, 0, &s->graph_many, err);
+    if (!rc) rc = capture(*s, 2, 0, &s->graph_two, err);
+    if (!rc) rc = capture(*s, 1, 0, &s->graph_one[0], err);
+    if (!rc && s->fused) rc = capture(*s, 1, 1, &s->graph_one[1], err);
+    if (rc) { session_free(s.release()); return rc; }
+    *out = s.release();
+    return FG_OK;
+}
+
+void session_free(Session* s) {
+    if (!s) return;
+    if (s->gpu) cudaSetDevice(s->gpu->device);
+    if (s->stream) cudaStreamSynchronize(s->stream);
+    if (s->graph_many) cudaGraphExecDestroy(s->graph_many);
+    if (s->graph_two) cudaGraphExecDestroy(s->graph_two);
+    for (auto& gx : s->graph_one)
+        if (gx) cudaGraphExecDestroy(gx);
+    if (s->arena) cudaFree(s->arena);
+    if (s->stream) cudaStreamDestroy(s->stream);
+    delete s;
+}
+
+int session_step(Session* s, uint64_t k, std::string& err) {
+    FG_CUDA(cudaSetDevice(s->gpu->device));
+    uint64_t done = 0;
+    // the fused step alternates buffers: a whole graph block needs an even start
+    while (done < k) {
+        const uint64_t left = k - done;
+        const int parity = s->fused ? int(s->steps & 1) : 0;
+        if (parity == 0 && left >= uint64_t(s->graph_steps)) {
+            FG_CUDA(cudaGraphLaunch(s->graph_many, s->stream));
+            done += s->graph_steps;
+            s->steps += s->graph_steps;
+        } else if (parity == 0 && left >= 2) {
+            FG_CUDA(cudaGraphLaunch(s->graph_two, s->stream));
+            done += 2;
+            s->steps += 2;
+        } else {
+            FG_CUDA(cudaGraphLaunch(s->graph_one[parity], s->stream));
+            done += 1;
+            s->steps += 1;
+        }
+    }
+    FG_CUDA(cudaGetLastError());
+    return FG_OK;
+}
+
+int session_sync(Session* s, std::string& err) {
+    FG_CUDA(cudaSetDevice(s->gpu->device));
+    FG_CUDA(cudaStreamSynchronize(s->stream));
+    return FG_OK;
+}
+
+// The buffers that hold the latest fields: after an odd number of fused steps, the second set.
+static void latest(const Session* s, float** e, float** h) {
+    if (s->fused && (s->steps & 1)) { *e = s->e2; *h = s->h2; }
+    else { *e = s->e; *h = s->h; }
+}
+
+int session_energy(Session* s, double* out, std::string& err) {
+    FG_CUDA(cudaSetDevice(s->gpu->device));
+    float *e, *h;
+    latest(s, &e, &h);
+    k_energy<<<ENERGY_BLOCKS, 256, 0, s->stream>>>(s->geom, e, h, s->partial);
+    FG_CUDA(cudaGetLastError());
+    std::vector<double> part(ENERGY_BLOCKS);
+    FG_CUDA(cudaMemcpyAsync(part.data(), s->partial, ENERGY_BLOCKS * 8, cudaMemcpyDeviceToHost, s->stream));
+    s->d2h_bytes += ENERGY_BLOCKS * 8;
+    FG_CUDA(cudaStreamSynchronize(s->stream));
+    double sum = 0.0;
+    for (double v : part) sum += v;
+    *out = sum;
+    return FG_OK;
+}
+
+uint64_t session_steps(const Session* s) { return s->steps; }
+
+int session_read(Session* s, const std::string& which, float* dst, uint64_t len, std::string& err) {
+    FG_CUDA(cudaSetDevice(s->gpu->device));
+    FG_CUDA(cudaStreamSynchronize(s->stream));
+    auto copy = [&](const float* src, uint64_t n) -> int {
+        if (n > len) { err = "destination too small for " + which; return FG_ERR_INVALID; }
+        if (n) FG_CUDA(cudaMemcpy(dst, src, n * 4, cudaMemcpyDeviceToHost));
+        s->d2h_bytes += n * 4;
+        return FG_OK;
+    };
+    if (which == "series") {
+        uint64_t n = std::min<uint64_t>(s->steps, s->sc.cap) * uint64_t(s->sc.ports) * 2;
+        return copy(s->series, n);
+    }
+    if (which == "plane") return copy(s->plane, s->plane_len);
+    if (which == "ntff") return copy(s->ntff, s->ntff_len);
+    if (which == "e" || which == "h") {
+        float *e, *h;
+        latest(s, &e, &h);
+        const float* src = which == "e" ? e : h;
+        const uint64_t nn = uint64_t(s->geom.nn);
+        if (3 * nn > len) { err = "destination too small for " + which; return FG_ERR_INVALID; }
+        for (int c = 0; c < 3; ++c) FG_CUDA(cudaMemcpy(dst + c * nn, src + c * s->geom.cs, nn * 4, cudaMemcpyDeviceToHost));
+        s->d2h_bytes += 3 * nn * 4;
+        return FG_OK;
+    }
+    err = "unknown buffer " + which;
+    return FG_ERR_INVALID;
+}
+
+void* session_stream(Session* s) { return s->stream; }
+uint64_t session_launches_per_step(const Session* s) { return s->launches; }
+uint64_t session_device_bytes(const Session* s) { return s->arena_bytes; }
+const char* session_variant(const Session* s) { return s->variant.c_str(); }
+uint64_t session_ports(const Session* s) { return uint64_t(s->sc.ports); }
+uint64_t session_plane_len(const Session* s) { return s->plane_len; }
+uint64_t session_ntff_len(const Session* s) { return s->ntff_len; }
+double session_t0(const Session* s) { return s->t0; }
+
+int session_kernel_times(Session* s, uint64_t steps, std::vector<std::pair<std::string, double>>& out,
+                         std::string& err);
+
+// Per-kernel device times, printed like report_kernel_times (run.rs:153-176). It steps the
+// session, so the run loop calls it only after its last step.
+void session_profile(Session* s) {
+    std::string err;
+    std::vector<std::pair<std::string, double>> t;
+    if (session_kernel_times(s, 20, t, err)) {
+        std::fprintf(stderr, "fdtd kernel times unavailable: %s\n", err.c_str());
+        return;
+    }
+    double step = 0.0;
+    for (auto& [name, ms] : t) {
+        std::fprintf(stderr, "fdtd kernel %s: %.1f us over 20 launches\n", name.c_str(), 1e3 * ms);
+        step += ms;
+    }
+    std::fprintf(stderr, "fdtd kernel time per step: %.1f us (%s)\n", 1e3 * step, s->variant.c_str());
+}
+
+// Launches `steps` steps one kernel at a time with an event before each launch.
+int session_kernel_times(Session* s, uint64_t steps, std::vector<std::pair<std::string, double>>& out,
+                         std::string& err) {
+    FG_CUDA(cudaSetDevice(s->gpu->device));
+    std::vector<std::pair<const char*, cudaEvent_t>> marks;
+    std::vector<std::pair<std::string, double>> sums;
+    std::vector<int> counts;
+    for (uint64_t q = 0; q < steps; ++q) {
+        marks.clear();
+        s->marks = &marks;
+        int rc = enqueue_step(*s, s->fused ? int(s->steps & 1) : 0, err);
+        s->marks = nullptr;
+        if (rc) return rc;
+        s->steps += 1;
+        FG_CUDA(cudaStreamSynchronize(s->stream));
+        for (size_t m = 0; m + 1 < marks.size(); ++m) {
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, marks[m].second, marks[m + 1].second);
+            if (sums.size() <= m) { sums.push_back({marks[m].first, 0.0}); counts.push_back(0); }
+            sums[m].second += ms;
+            counts[m] += 1;
+        }
+        for (auto& mk : marks) cudaEventDestroy(mk.second);
+    }
+    out.clear();
+    for (size_t m = 0; m < sums.size(); ++m) out.push_back({sums[m].first, sums[m].second / std::max(counts[m], 1)});
+    FG_CUDA(cudaGetLastError());
+    return FG_OK;
+}
+
+uint64_t session_h2d_bytes(const Session* s) { return s->h2d_bytes; }
+uint64_t session_d2h_bytes(const Session* s) { return s->d2h_bytes; }
+
+}  // namespace fg

@@ -1,0 +1,311 @@
+// Device-side types and the per-step kernels other than the field stencil: thin-wire H terms,
+// resistive sheets, Debye ADE, lumped sources and inductors, port V/I probes, the plane DFT, the
+// NTFF accumulation and the energy reduction. Each names the reference code it restates
+// (crates/sims-field/src/fdtd/cpu.rs, the CPU path whose results are the parity target).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "host.hpp"
+
+namespace fg {
+
+// Node geometry shared by every kernel. Fields are component-major with component stride `cs`
+// (>= nn, padded to 32 floats) and node id (i*n1 + j)*n2 + k.
+struct Geom {
+    int n0, n1, n2;
+    int pml;
+    long long nn;
+    long long cs;
+    const AxisNode* ax[3];
+    long long psi_off[18];  // offsets of the 12 psi slabs: [field*9 + comp*3 + axis], field 0 = E, 1 = H
+};
+
+struct DevSheet {           // pack() sheet record (run.rs:259-289), named
+    long long f, ha, hb;    // field indices (comp*cs + id)
+    float len, c, r, adaptive;
+    float aa, bb, ab, ma, mb, old, i_old;
+    unsigned face_a, face_b;
+};
+
+struct DevSource { long long f; float src; };           // run.rs:243-246
+struct DevInductor { long long f; float ke, ki, cur; };  // run.rs:247-250
+struct DevPortEdge { long long id; float w; };           // run.rs:314-317
+struct DevLoop { long long f; float w; };                // run.rs:326-328 (f = (3+comp-3)*cs + id)
+struct DevProbe { int comp, first, count, loop_first, loop_count; };
+struct DevWire { long long h; long long e[4]; float c[4]; };
+
+struct StepConst {          // per-run scalars (run.rs:433-464 Params)
+    float k_mu, dt, t0, tau, w0;
+    int nf;
+    float omega[4];
+    unsigned cap;
+    int ports;
+};
+
+__device__ __forceinline__ long long psi_at(const Geom& g, int a, int i, int j, int k, int s) {
+    const int w = 2 * g.pml;
+    if (a == 0) return ((long long)s * g.n1 + j) * g.n2 + k;
+    if (a == 1) return ((long long)i * w + s) * g.n2 + k;
+    return ((long long)i * g.n1 + j) * w + s;
+}
+
+// The step index n of the running step: the first kernel of step n raised the counter to n + 1.
+__device__ __forceinline__ unsigned step_index(const unsigned* counter) { return *(volatile const unsigned*)counter - 1u; }
+
+// cpu.rs:270-273: h[w.h] += sum of four c*E terms, after the H update, with E not yet updated.
+__global__ void k_wire_h(const DevWire* __restrict__ w, int count, const float* __restrict__ e, float* __restrict__ h) {
+    int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= count) return;
+    DevWire x = w[s];
+    float t0 = x.c[0] * e[x.e[0]], t1 = x.c[1] * e[x.e[1]], t2 = x.c[2] * e[x.e[2]], t3 = x.c[3] * e[x.e[3]];
+    h[x.h] += ((t0 + t1) + t2) + t3;
+}
+
+// cpu.rs:169-193 on one sheet edge: before the E update, with the new H.
+__device__ __forceinline__ void sheet_before(DevSheet& s, float old, float ha, float hb) {
+    s.old = old;
+    float aa = s.aa + ha * ha, bb = s.bb + hb * hb, ab = s.ab + ha * hb;
+    s.aa = aa;
+    s.bb = bb;
+    s.ab = ab;
+    float sum = aa + bb;
+    if (sum <= 1e-30f) return;
+    float scale = 1.0f;
+    if (s.adaptive != 0.0f) {
+        scale = s.ma + s.mb;
+        float tot = aa + bb - 2.0f * ab;
+        if (tot > 1e-30f) scale = fminf(fmaxf(sum / tot, 0.5f), 4.0f);
+    }
+    s.ma = scale * aa / sum;
+    s.mb = scale * bb / sum;
+}
+
+__global__ void k_sheet_pre(DevSheet* __restrict__ sh, int count, const float* __restrict__ e, const float* __restrict__ h) {
+    int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= count) return;
+    DevSheet s = sh[q];
+    sheet_before(s, e[s.f], h[s.ha], h[s.hb]);
+    sh[q] = s;
+}
+
+// cpu.rs:195-237: the sheet current from the branch table after the E update.
+__global__ void k_sheet_post(DevSheet* __restrict__ sh, int count, const float* __restrict__ br, float* __restrict__ cur,
+                             float* __restrict__ e) {
+    int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= count) return;
+    DevSheet s = sh[q];
+    const int nr = int(br[0]), nc = int(br[1]);
+    const int stride = 2 + nr + 2 * nc, faces = 4 + 2 * nr + 4 * nc;
+    const int fa = faces + int(s.face_a) * stride, fb = faces + int(s.face_b) * stride;
+    const long long base = (long long)q * (nr + 2 * nc);
+    const float ma = s.ma, mb = s.mb;
+    float hist = (ma * br[fa + 1] + mb * br[fb + 1]) * s.i_old;
+    for (int k = 0; k < nr; ++k) hist -= (ma * br[fa + 2 + k] + mb * br[fb + 2 + k]) * cur[base + k];
+    for (int k = 0; k < nc; ++k) {
+        int o = 2 + nr + 2 * k;
+        float cr = ma * br[fa + o] + mb * br[fb + o];
+        float ci = ma * br[fa + o + 1] + mb * br[fb + o + 1];
+        long long u = base + nr + 2 * k;
+        hist -= cr * cur[u] - ci * cur[u + 1];
+    }
+    float a = s.r * (ma * br[fa] + mb * br[fb]);
+    float ef = e[s.f];
+    float ibar = (0.5f * s.len * (ef + s.old) + s.r * hist) / (a + 0.5f * s.len * s.c);
+    e[s.f] = ef - s.c * ibar;
+    s.i_old = 2.0f * ibar - s.i_old;
+    for (int k = 0; k < nr; ++k) {
+        int p = 4 + 2 * k;
+        cur[base + k] = br[p] * cur[base + k] + br[p + 1] * ibar;
+    }
+    for (int k = 0; k < nc; ++k) {
+        int p = 4 + 2 * nr + 4 * k;
+        long long u = base + nr + 2 * k;
+        float ur = cur[u], ui = cur[u + 1];
+        cur[u] = br[p] * ur - br[p + 1] * ui + br[p + 2] * ibar;
+        cur[u + 1] = br[p] * ui + br[p + 1] * ur + br[p + 3] * ibar;
+    }
+    sh[q] = s;
+}
+
+// cpu.rs:281-283: the E of each Debye edge before the E update.
+__global__ void k_debye_pre(const long long* __restrict__ f, int count, const float* __restrict__ e, float* __restrict__ old) {
+    int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q < count) old[q] = e[f[q]];
+}
+
+// cpu.rs:239-260: E -= cb * sum_k 0.5 (1 + b_k) s_k; s_k = b_k s_k + dd c_k (E_new - E_old).
+// `eold` is either the saved copy (separate step) or the step's input buffer (fused step).
+template <typename CID>
+__global__ void k_debye_post(const long long* __restrict__ f, const float* __restrict__ dd, int count,
+                             const float* __restrict__ eold_saved, const float* __restrict__ eold_field,
+                             const CID* __restrict__ node_class, const Coef* __restrict__ classes, long long cs,
+                             const float* __restrict__ table, float* __restrict__ state, float* __restrict__ e) {
+    int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= count) return;
+    const long long fi = f[q];
+    const int c = int(fi / cs);
+    const long long id = fi - c * cs;
+    const float cb = classes[node_class[id]].cb[c];
+    const float old = eold_saved ? eold_saved[q] : eold_field[fi];
+    const int np = int(table[0]);
+    float s0 = 0.0f;
+    for (int k = 0; k < np; ++k) s0 += 0.5f * (1.0f + table[1 + 2 * k]) * state[(long long)k * count + q];
+    const float next = e[fi] - cb * s0;
+    e[fi] = next;
+    const float de = next - old;
+    const float w = dd[q];
+    for (int k = 0; k < np; ++k) {
+        long long p = (long long)k * count + q;
+        state[p] = table[1 + 2 * k] * state[p] + w * table[2 + 2 * k] * de;
+    }
+}
+
+// cpu.rs:262-265
+__device__ __forceinline__ float pulse_at(const StepConst& sc, float t) {
+    float x = (t - sc.t0) / sc.tau;
+    return expf(-x * x) * cosf(sc.w0 * (t - sc.t0));
+}
+
+// cpu.rs:291-303: the driven port's soft source at t = (n + 1/2) dt, then the inductor ADE.
+// One block; the source edges of a port are distinct, as are the inductor edges.
+__global__ void k_lumped(const DevSource* __restrict__ src, int ns, DevInductor* __restrict__ ind, int ni,
+                         StepConst sc, const unsigned* __restrict__ counter, float* __restrict__ e) {
+    const unsigned n = step_index(counter);
+    const float t = (float(n) + 0.5f) * sc.dt;
+    const float p = pulse_at(sc, t);
+    for (int q = threadIdx.x; q < ns; q += blockDim.x) {
+        DevSource s = src[q];
+        e[s.f] -= s.src * p;
+    }
+    __syncthreads();
+    for (int q = threadIdx.x; q < ni; q += blockDim.x) {
+        DevInductor d = ind[q];
+        float x = e[d.f] - d.ke * d.cur;
+        e[d.f] = x;
+        ind[q].cur = d.cur + d.ki * x;
+    }
+}
+
+// cpu.rs:309-334: per port V = -sum E*w over its edges and I = sum H*w around the loop, summed
+// in f64 like the CPU path; one block per port.
+__global__ void k_probe(const DevProbe* __restrict__ defs, const DevPortEdge* __restrict__ pe, const DevLoop* __restrict__ lp,
+                        long long cs, const float* __restrict__ e, const float* __restrict__ h,
+                        const unsigned* __restrict__ counter, StepConst sc, float* __restrict__ series) {
+    __shared__ double sv[256], si[256];
+    const DevProbe d = defs[blockIdx.x];
+    double v = 0.0, cur = 0.0;
+    for (int q = threadIdx.x; q < d.count; q += blockDim.x) {
+        DevPortEdge x = pe[d.first + q];
+        v -= double(e[(long long)d.comp * cs + x.id] * x.w);
+    }
+    for (int q = threadIdx.x; q < d.loop_count; q += blockDim.x) {
+        DevLoop x = lp[d.loop_first + q];
+        cur += double(h[x.f] * x.w);
+    }
+    sv[threadIdx.x] = v;
+    si[threadIdx.x] = cur;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) {
+            sv[threadIdx.x] += sv[threadIdx.x + s];
+            si[threadIdx.x] += si[threadIdx.x + s];
+        }
+        __syncthreads();
+    }
+    const unsigned n = step_index(counter);
+    if (threadIdx.x == 0 && n < sc.cap) {
+        long long o = ((long long)n * sc.ports + blockIdx.x) * 2;
+        series[o] = float(sv[0]);
+        series[o + 1] = float(si[0]);
+    }
+}
+
+// cpu.rs:336-361: running DFT of Ex, Ey, Ez (at (n+1) dt) and Hx, Hy (at (n+1/2) dt) on the
+// z-plane k = plane_k; phases formed in f32 like the CPU path.
+__global__ void k_field_dft(Geom g, int plane_k, StepConst sc, const unsigned* __restrict__ counter,
+                            const float* __restrict__ e, const float* __restrict__ h, float* __restrict__ acc) {
+    const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= (long long)g.n0 * g.n1) return;
+    const unsigned n = step_index(counter);
+    const float te = (float(n) + 1.0f) * sc.dt, th = (float(n) + 0.5f) * sc.dt;
+    const long long id = q * g.n2 + plane_k;
+    const float f[5] = {e[id], e[g.cs + id], e[2 * g.cs + id], h[id], h[g.cs + id]};
+    float* out = acc + q * sc.nf * 10;
+    for (int k = 0; k < sc.nf; ++k) {
+        const float w = sc.omega[k];
+        const float ce0 = cosf(w * te) * sc.dt, ce1 = -sinf(w * te) * sc.dt;
+        const float ch0 = cosf(w * th) * sc.dt, ch1 = -sinf(w * th) * sc.dt;
+#pragma unroll
+        for (int c = 0; c < 5; ++c) {
+            const float p0 = c >= 3 ? ch0 : ce0, p1 = c >= 3 ? ch1 : ce1;
+            out[k * 10 + 2 * c] += f[c] * p0;
+            out[k * 10 + 2 * c + 1] += f[c] * p1;
+        }
+    }
+}
+
+// cpu.rs:363-415: per NTFF patch, tangential E (2-edge mean) and H (4-edge mean), J = n x H,
+// M = E x n, accumulated with dt e^{-j w t}.
+__global__ void k_ntff(const unsigned* __restrict__ pidx, int patches, long long cs, StepConst sc,
+                       const unsigned* __restrict__ counter, const float* __restrict__ e, const float* __restrict__ h,
+                       float* __restrict__ acc) {
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= patches) return;
+    const unsigned n = step_index(counter);
+    const unsigned* b = pidx + (long long)g * 13;
+    const unsigned meta = b[0];
+    const int axis = meta & 3;
+    const float side = (meta & 4) ? 1.0f : -1.0f;
+    const int u = (axis + 1) % 3, v = (axis + 2) % 3;
+    float ef[3] = {0, 0, 0}, hf[3] = {0, 0, 0};
+    ef[u] = 0.5f * (e[u * cs + b[1]] + e[u * cs + b[2]]);
+    ef[v] = 0.5f * (e[v * cs + b[3]] + e[v * cs + b[4]]);
+    hf[u] = 0.25f * (h[u * cs + b[5]] + h[u * cs + b[6]] + h[u * cs + b[7]] + h[u * cs + b[8]]);
+    hf[v] = 0.25f * (h[v * cs + b[9]] + h[v * cs + b[10]] + h[v * cs + b[11]] + h[v * cs + b[12]]);
+    float nrm[3] = {0, 0, 0};
+    nrm[axis] = side;
+    const float jv[3] = {nrm[1] * hf[2] - nrm[2] * hf[1], nrm[2] * hf[0] - nrm[0] * hf[2], nrm[0] * hf[1] - nrm[1] * hf[0]};
+    const float mv[3] = {ef[1] * nrm[2] - ef[2] * nrm[1], ef[2] * nrm[0] - ef[0] * nrm[2], ef[0] * nrm[1] - ef[1] * nrm[0]};
+    const float te = (float(n) + 1.0f) * sc.dt, th = (float(n) + 0.5f) * sc.dt;
+    float* out = acc + (long long)g * sc.nf * 12;
+    for (int k = 0; k < sc.nf; ++k) {
+        const float wf = sc.omega[k];
+        const float pe0 = cosf(-wf * te) * sc.dt, pe1 = sinf(-wf * te) * sc.dt;
+        const float ph0 = cosf(-wf * th) * sc.dt, ph1 = sinf(-wf * th) * sc.dt;
+        float* o = out + k * 12;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            o[2 * c] += ph0 * jv[c];
+            o[2 * c + 1] += ph1 * jv[c];
+            o[6 + 2 * c] += pe0 * mv[c];
+            o[6 + 2 * c + 1] += pe1 * mv[c];
+        }
+    }
+}
+
+// cpu.rs:417-421: sum of E^2 + (376.73 H)^2 in f64, one partial per block.
+__global__ void k_energy(Geom g, const float* __restrict__ e, const float* __restrict__ h, double* __restrict__ partial) {
+    __shared__ double s[256];
+    double acc = 0.0;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (int c = 0; c < 3; ++c) {
+        const float* ec = e + c * g.cs;
+        const float* hc = h + c * g.cs;
+        for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < g.nn; q += stride) {
+            double x = double(ec[q]);
+            double y = double(hc[q]) * 376.73;
+            acc += x * x + y * y;
+        }
+    }
+    s[threadIdx.x] = acc;
+    __syncthreads();
+    for (int k = blockDim.x / 2; k > 0; k >>= 1) {
+        if (threadIdx.x < k) s[threadIdx.x] += s[threadIdx.x + k];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) partial[blockIdx.x] = s[0];
+}
+
+}  // namespace fg

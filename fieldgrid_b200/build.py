@@ -51,6 +51,8 @@ def build(force: bool = False, verbose: bool = False) -> str:
         if src.endswith(".cu"):
             cmd = [nvcc, "-ccbin", cxx, *ARCH, "-lineinfo", "-O3", "-std=c++17", "-c", src, "-o", obj,
                    "-Xcompiler", "-fPIC,-fopenmp,-ffp-contract=off", "-Xptxas", "-O3",
+                   # no a*b+c contraction: the kernels round like the reference's CPU path
+                   "--fmad=false",
                    "-I", os.path.join(ROOT, "include")]
             if verbose:
                 cmd += ["-Xptxas", "-v"]

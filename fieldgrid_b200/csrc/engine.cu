@@ -18,6 +18,9 @@
 #include "kernels.cuh"
 #include "stencil_fused.cuh"
 #include "stencil_separate.cuh"
+#include "stencil_tma.cuh"
+
+#include <cudaTypedefs.h>
 
 namespace fg {
 
@@ -68,7 +71,7 @@ struct Session {
     float *e = nullptr, *h = nullptr, *e2 = nullptr, *h2 = nullptr;
     float *psi = nullptr, *psi_h2 = nullptr;
     void* node_class = nullptr;
-    Coef* classes = nullptr;
+    DevCoef* classes = nullptr;
     AxisNode* axes = nullptr;
     unsigned* counter = nullptr;
     float* series = nullptr;
@@ -90,6 +93,11 @@ struct Session {
     float* debye_state = nullptr;
     float* debye_table = nullptr;
     double* partial = nullptr;
+    int* error = nullptr;           // set by a kernel whose bounded wait ran out
+    TmaPlan tma;                    // the TMA-fed fused step, when it applies
+    uint8_t* local_ids = nullptr;   // per node: index into its block region's coefficient table
+    float* tables = nullptr;        // per block region: LOCAL_CLASSES x (ca[3], cb[3])
+    bool local = false;
     // counts
     int n_sources = 0, n_inductors = 0, n_ports = 0, n_wires = 0, n_sheets = 0, n_debye = 0, n_patches = 0;
     int plane_k = 0;
@@ -123,6 +131,162 @@ T* carve(char*& cur, size_t count) {
 }
 
 size_t carve_size(size_t bytes) { return std::max<size_t>((bytes + 255) & ~size_t(255), 256); }
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link against libcuda).
+PFN_cuTensorMapEncodeTiled_v12000 encode_tiled() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (!fn) {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }
+    return fn;
+}
+
+bool encode(CUtensorMap* m, CUtensorMapDataType dt, void* base, int rank, const cuuint64_t* dims,
+            const cuuint64_t* strides, const cuuint32_t* box, std::string& why) {
+    auto fn = encode_tiled();
+    if (!fn) { why = "cuTensorMapEncodeTiled is unavailable"; return false; }
+    cuuint32_t es[5] = {1, 1, 1, 1, 1};
+    CUresult r = fn(m, dt, cuuint32_t(rank), base, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                    CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) { why = "cuTensorMapEncodeTiled failed (" + std::to_string(int(r)) + ")"; return false; }
+    return true;
+}
+
+constexpr int TMA_TJ = 7, TMA_TK = 64, TMA_STAGES = 3, TMA_SEGMAX = 64;
+
+template <typename CID, bool LOCAL = false>
+using TmaL = TmaLayout<TMA_TJ, TMA_TK, CID, TMA_STAGES, TMA_SEGMAX, LOCAL>;
+template <typename CID, bool LOCAL = false>
+constexpr auto tma_kernel = k_tma_step<TMA_TJ, TMA_TK, CID, TMA_STAGES, TMA_SEGMAX, LOCAL>;
+
+// tiles along k: a node count of 64t + 1 gives t tiles, the last owning the extra column
+inline int tma_ktiles(int n2) { return (n2 > TMA_TK && n2 % TMA_TK == 1) ? (n2 - 1) / TMA_TK : (n2 + TMA_TK - 1) / TMA_TK; }
+
+// x-planes per block: enough segments for several waves of 3 blocks per SM, at most TMA_SEGMAX.
+int tma_seg(const Geom& g) {
+    const long long tiles = (long long)tma_ktiles(g.n2) * ((g.n1 + TMA_TJ - 1) / TMA_TJ);
+    int seg = TMA_SEGMAX;
+    while (seg > 8 && tiles * ((g.n0 + seg - 1) / seg) < 148 * 3 * 6) seg /= 2;
+    return seg;
+}
+
+// Per block region of the TMA step (a TJ x TK tile over one x-segment): the distinct node classes
+// it holds, renumbered from 0, and each node's index into that short list. ok = false when a
+// region holds more than LOCAL_CLASSES classes.
+struct LocalClasses {
+    std::vector<uint8_t> ids;    // device node layout (pitch p2)
+    std::vector<float> tables;   // regions x LOCAL_CLASSES x 6
+    bool ok = true;
+};
+
+LocalClasses build_local(const HostSim& sim, const Geom& g, int seg) {
+    LocalClasses out;
+    const int kt = tma_ktiles(g.n2), jt = (g.n1 + TMA_TJ - 1) / TMA_TJ, st = (g.n0 + seg - 1) / seg;
+    const long long regions = (long long)kt * jt * st;
+    out.ids.assign(size_t(g.n0) * g.n1 * g.p2, 0);
+    out.tables.assign(size_t(regions) * LOCAL_CLASSES * 6, 0.f);
+    bool over = false;
+    const size_t n1 = g.n1, n2 = g.n2;
+#pragma omp parallel for schedule(dynamic, 8) reduction(|| : over)
+    for (long long r = 0; r < regions; ++r) {
+        if (over) continue;
+        const int bx = int(r % kt), by = int((r / kt) % jt), bz = int(r / ((long long)kt * jt));
+        const int k0 = bx * TMA_TK, j0 = by * TMA_TJ, i0 = bz * seg, i1 = std::min(i0 + seg, g.n0);
+        int kend = std::min(k0 + TMA_TK, g.n2);
+        if (bx == kt - 1 && k0 + TMA_TK == g.n2 - 1) kend = g.n2;  // the owned right-edge column
+        const int jend = std::min(j0 + TMA_TJ, g.n1);
+        uint32_t keys[512];
+        uint16_t vals[512];
+        std::fill(keys, keys + 512, 0xffffffffu);
+        int count = 0;
+        float* tab = out.tables.data() + size_t(r) * LOCAL_CLASSES * 6;
+        for (int i = i0; i < i1 && !over; ++i)
+            for (int j = j0; j < jend && !over; ++j)
+                for (int k = k0; k < kend; ++k) {
+                    const uint32_t gid = sim.node_class[(size_t(i) * n1 + j) * n2 + k];
+                    uint32_t h = (gid * 2654435761u) & 511u;
+                    while (keys[h] != 0xffffffffu && keys[h] != gid) h = (h + 1) & 511u;
+                    if (keys[h] == 0xffffffffu) {
+                        if (count == LOCAL_CLASSES) { over = true; break; }
+                        keys[h] = gid;
+                        vals[h] = uint16_t(count);
+                        const Coef& cf = sim.classes[gid];
+                        for (int c = 0; c < 3; ++c) { tab[count * 6 + c] = cf.ca[c]; tab[count * 6 + 3 + c] = cf.cb[c]; }
+                        ++count;
+                    }
+                    out.ids[(size_t(i) * n1 + j) * g.p2 + k] = uint8_t(vals[h]);
+                }
+    }
+    out.ok = !over;
+    return out;
+}
+
+// Builds the tensor maps of the TMA step: E and H of both buffer sets, and the class ids.
+void plan_tma(Session& s) {
+    TmaPlan& t = s.tma;
+    t.ok = false;
+    const Geom& g = s.geom;
+    if (!s.fused) { t.why = "separate step"; return; }
+    if (const char* v = std::getenv("FIELDGRID_NO_TMA"); v && v[0] == '1') { t.why = "disabled by FIELDGRID_NO_TMA"; return; }
+    int dev = 0, major = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev);
+    if (major < 10) { t.why = "needs sm_100"; return; }
+    if (g.n2 < 2 || g.n1 < 2) { t.why = "grid too thin"; return; }
+    t.tj = TMA_TJ;
+    t.tk = TMA_TK;
+    const cuuint64_t dims[4] = {cuuint64_t(g.n2), cuuint64_t(g.n1), cuuint64_t(g.n0), 3};
+    const cuuint64_t strides[3] = {cuuint64_t(g.p2) * 4, cuuint64_t(g.n1) * g.p2 * 4, cuuint64_t(g.cs) * 4};
+    const cuuint32_t box_e[4] = {cuuint32_t(TmaL<float>::EW), cuuint32_t(TmaL<float>::ER), 1, 3};
+    const cuuint32_t box_h[4] = {cuuint32_t(TmaL<float>::HW), cuuint32_t(TmaL<float>::HR), 1, 3};
+    float* es[2] = {s.e, s.e2};
+    float* hs[2] = {s.h, s.h2};
+    for (int q = 0; q < 2; ++q) {
+        if (!encode(&t.e[q], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, es[q], 4, dims, strides, box_e, t.why)) return;
+        if (!encode(&t.h[q], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, hs[q], 4, dims, strides, box_h, t.why)) return;
+    }
+    const int b = s.local ? 1 : s.cid_bytes;
+    const CUtensorMapDataType dt = b == 1 ? CU_TENSOR_MAP_DATA_TYPE_UINT8
+                                 : (b == 2 ? CU_TENSOR_MAP_DATA_TYPE_UINT16 : CU_TENSOR_MAP_DATA_TYPE_UINT32);
+    const cuuint64_t cdims[3] = {cuuint64_t(g.n2), cuuint64_t(g.n1), cuuint64_t(g.n0)};
+    const cuuint64_t cstr[2] = {cuuint64_t(g.p2) * b, cuuint64_t(g.n1) * g.p2 * b};
+    const cuuint32_t cbox[3] = {cuuint32_t(TmaL<float>::CW), cuuint32_t(TmaL<float>::CR), 1};
+    if (!encode(&t.c, dt, s.local ? (void*)s.local_ids : s.node_class, 3, cdims, cstr, cbox, t.why)) return;
+    t.smem = s.local ? TmaL<uint8_t, true>::TOTAL
+                     : (b == 1 ? TmaL<uint8_t>::TOTAL : (b == 2 ? TmaL<uint16_t>::TOTAL : TmaL<uint32_t>::TOTAL));
+    cudaError_t ce;
+    if (s.local) ce = cudaFuncSetAttribute(tma_kernel<uint8_t, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, t.smem);
+    else if (b == 1) ce = cudaFuncSetAttribute(tma_kernel<uint8_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, t.smem);
+    else if (b == 2) ce = cudaFuncSetAttribute(tma_kernel<uint16_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, t.smem);
+    else ce = cudaFuncSetAttribute(tma_kernel<uint32_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, t.smem);
+    if (ce != cudaSuccess) { t.why = std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(ce); return; }
+    t.seg = tma_seg(g);
+    t.ok = true;
+}
+
+int launch_tma(Session& s, int parity, float* e_out, float* h_out, const float* psi_h_in, float* psi_h_out) {
+    const Geom& g = s.geom;
+    const TmaPlan& t = s.tma;
+    const int kt = tma_ktiles(g.n2);
+    TmaArgs a{g, s.classes, e_out, h_out, s.psi, psi_h_in, psi_h_out, s.sc.k_mu, t.seg, kt,
+              (g.n1 + TMA_TJ - 1) / TMA_TJ, s.tables, s.counter, s.error};
+    dim3 grd(kt, (g.n1 + TMA_TJ - 1) / TMA_TJ, (g.n0 + t.seg - 1) / t.seg);
+    dim3 blk(TMA_CONSUMERS + 32);
+    if (s.local) {
+        tma_kernel<uint8_t, true><<<grd, blk, t.smem, s.stream>>>(t.e[parity], t.h[parity], t.c, a);
+        return cudaPeekAtLastError() == cudaSuccess ? 0 : 1;
+    }
+    switch (s.cid_bytes) {
+        case 1: tma_kernel<uint8_t><<<grd, blk, t.smem, s.stream>>>(t.e[parity], t.h[parity], t.c, a); break;
+        case 2: tma_kernel<uint16_t><<<grd, blk, t.smem, s.stream>>>(t.e[parity], t.h[parity], t.c, a); break;
+        default: tma_kernel<uint32_t><<<grd, blk, t.smem, s.stream>>>(t.e[parity], t.h[parity], t.c, a); break;
+    }
+    return cudaPeekAtLastError() == cudaSuccess ? 0 : 1;
+}
 
 // One time step. `parity` selects the ping-pong direction of the fused step (input = parity 0
 // buffers on even steps). The separate step updates in place.
@@ -159,9 +323,11 @@ int enqueue_step(Session& s, int parity, std::string& err) {
             k_wire_h<<<(s.n_wires + 127) / 128, 128, 0, st>>>(s.wires, s.n_wires, e_in, h_in);
         }
         mark("fused_step");
-        int rc = launch_fused(s.shape, s.cid_bytes, g, s.node_class, s.classes, e_in, h_in, e_out, h_out, s.psi,
-                              parity ? s.psi_h2 : s.psi, parity ? s.psi : s.psi_h2, s.sc.k_mu, s.counter,
-                              s.n_wires > 0, st);
+        int rc = s.tma.ok
+                     ? launch_tma(s, parity, e_out, h_out, parity ? s.psi_h2 : s.psi, parity ? s.psi : s.psi_h2)
+                     : launch_fused(s.shape, s.cid_bytes, g, s.node_class, s.classes, e_in, h_in, e_out, h_out, s.psi,
+                                    parity ? s.psi_h2 : s.psi, parity ? s.psi : s.psi_h2, s.sc.k_mu, s.counter,
+                                    s.n_wires > 0, st);
         if (rc) { err = "fused step launch failed"; return FG_ERR_CUDA; }
         if (s.n_sheets) {
             mark("sheet_pre");
@@ -239,9 +405,13 @@ int session_new(Gpu* gpu, const HostSim& sim, const RunSpec& rs, Session** out, 
     g.n0 = int(n0); g.n1 = int(n1); g.n2 = int(n2);
     g.pml = int(sim.pml);
     g.nn = (long long)nn;
-    g.cs = (long long)((nn + 31) & ~size_t(31));
+    g.p2 = int((n2 + 31) & ~size_t(31));
+    const size_t nnp = n0 * n1 * size_t(g.p2);   // device nodes, rows padded to the pitch
+    g.cs = (long long)((nnp + 31) & ~size_t(31));
     const long long cs = g.cs;
-    auto fidx = [&](uint64_t key) { return (long long)(key / nn) * cs + (long long)(key % nn); };
+    // reference node id (i*n1 + j)*n2 + k -> device node id (i*n1 + j)*p2 + k
+    auto dev = [&](uint64_t id) { return (long long)(id / n2) * g.p2 + (long long)(id % n2); };
+    auto fidx = [&](uint64_t key) { return (long long)(key / nn) * cs + dev(key % nn); };
 
     // psi slabs (run.rs:214-225)
     long long psi_total = 0;
@@ -264,9 +434,9 @@ int session_new(Gpu* gpu, const HostSim& sim, const RunSpec& rs, Session** out, 
 
     // sparse lists (pack, run.rs:243-340)
     std::vector<DevSource> src;
-    for (auto& q : sim.port_src[rs.driven]) src.push_back(DevSource{(long long)q.comp * cs + (long long)q.id, q.src});
+    for (auto& q : sim.port_src[rs.driven]) src.push_back(DevSource{(long long)q.comp * cs + dev(q.id), q.src});
     std::vector<DevInductor> ind;
-    for (auto& q : sim.inductors) ind.push_back(DevInductor{(long long)q.comp * cs + (long long)q.id, q.ke, q.ki, 0.f});
+    for (auto& q : sim.inductors) ind.push_back(DevInductor{(long long)q.comp * cs + dev(q.id), q.ke, q.ki, 0.f});
     std::vector<DevWire> wires;
     for (auto& w : sim.wires) {
         DevWire d;
@@ -279,9 +449,9 @@ int session_new(Gpu* gpu, const HostSim& sim, const RunSpec& rs, Session** out, 
         if (q.comp == 2 || q.id % n2 == 0) continue;
         long long hc = q.comp == 0 ? 1 : 0;
         DevSheet d{};
-        d.f = (long long)q.comp * cs + (long long)q.id;
-        d.ha = hc * cs + (long long)q.id;
-        d.hb = hc * cs + (long long)q.id - 1;
+        d.f = (long long)q.comp * cs + dev(q.id);
+        d.ha = hc * cs + dev(q.id);
+        d.hb = hc * cs + dev(q.id) - 1;
         d.len = float(q.len);
         d.c = float(q.c);
         d.r = float(q.r);
@@ -295,7 +465,7 @@ int session_new(Gpu* gpu, const HostSim& sim, const RunSpec& rs, Session** out, 
     std::vector<long long> debye_f;
     std::vector<float> debye_dd;
     for (auto& q : sim.debye_edges) {
-        debye_f.push_back((long long)q.comp * cs + (long long)q.id);
+        debye_f.push_back((long long)q.comp * cs + dev(q.id));
         debye_dd.push_back(float(q.dd));
     }
     std::vector<float> debye_table{float(sim.poles.size())};
@@ -316,7 +486,7 @@ int session_new(Gpu* gpu, const HostSim& sim, const RunSpec& rs, Session** out, 
         const double weight = polarity / double(p.columns.size());
         for (auto& col : p.columns)
             for (auto& e : col)
-                pedges.push_back(DevPortEdge{(long long)sim.idx(e.at[0], e.at[1], e.at[2]),
+                pedges.push_back(DevPortEdge{dev(sim.idx(e.at[0], e.at[1], e.at[2])),
                                              float(sim.ax[axis].d[e.at[axis]] * weight)});
         d.count = int(pedges.size()) - d.first;
         double height = 0.0;
@@ -344,14 +514,19 @@ int session_new(Gpu* gpu, const HostSim& sim, const RunSpec& rs, Session** out, 
                 const int comp = kc.second;
                 const size_t pc = comp == 0 ? id / (n1 * n2) : (comp == 1 ? (id / n2) % n1 : id % n2);
                 const double w = double(t) * sim.ax[comp].dd[pc];
-                loops.push_back(DevLoop{(long long)comp * cs + (long long)id, float(w * share)});
+                loops.push_back(DevLoop{(long long)comp * cs + dev(id), float(w * share)});
             }
         }
         d.loop_count = int(loops.size()) - d.loop_first;
         probes.push_back(d);
     }
-    for (auto& q : pedges)
-        if (float(q.id) >= float(1u << 24)) { err = "grid too large for f32 port indices"; return FG_ERR_PORT_INDEX; }
+    for (auto& p : sim.ports)  // run.rs:341-343, on the reference's node ids
+        for (auto& col : p.columns)
+            for (auto& e : col)
+                if (float(sim.idx(e.at[0], e.at[1], e.at[2])) >= float(1u << 24)) {
+                    err = "grid too large for f32 port indices";
+                    return FG_ERR_PORT_INDEX;
+                }
 
     pulse_shape(rs.fc, s->t0, s->tau);
     StepConst& sc = s->sc;
@@ -378,10 +553,42 @@ int session_new(Gpu* gpu, const HostSim& sim, const RunSpec& rs, Session** out, 
     for (size_t q = 0; q < size_t(s->n_patches) * 13; ++q)
         if (q % 13 != 0 && rs.ntff[q] >= nn) { err = "an NTFF patch index is outside the grid"; return FG_ERR_INVALID; }
     s->series_len = uint64_t(sc.cap) * sc.ports * 2;
+    // per-step pulse and phase tables (host libm, f32, the reference's expressions)
+    std::vector<float> t_pulse(sc.cap), t_dft(size_t(sc.cap) * sc.nf * 4), t_far(size_t(sc.cap) * sc.nf * 4);
+    {
+        const float dt = sc.dt, t0 = sc.t0, tau = sc.tau, w0 = sc.w0;
+        const int nf = sc.nf;
+        const float* om = sc.omega;
+#pragma omp parallel for schedule(static)
+        for (long long n = 0; n < (long long)sc.cap; ++n) {
+            const float t = (float(n) + 0.5f) * dt;
+            const float x = (t - t0) / tau;
+            t_pulse[n] = std::exp(-x * x) * std::cos(w0 * (t - t0));
+            const float te = (float(n) + 1.0f) * dt, th = (float(n) + 0.5f) * dt;
+            for (int k = 0; k < nf; ++k) {
+                float* d = &t_dft[(size_t(n) * nf + k) * 4];
+                d[0] = std::cos(om[k] * te) * dt;
+                d[1] = -std::sin(om[k] * te) * dt;
+                d[2] = std::cos(om[k] * th) * dt;
+                d[3] = -std::sin(om[k] * th) * dt;
+                float* f = &t_far[(size_t(n) * nf + k) * 4];
+                f[0] = std::cos(-om[k] * te) * dt;
+                f[1] = std::sin(-om[k] * te) * dt;
+                f[2] = std::cos(-om[k] * th) * dt;
+                f[3] = std::sin(-om[k] * th) * dt;
+            }
+        }
+    }
     const size_t states = sim.sheet_states;
     const size_t nr_nc = sim.sheet_table.size() >= 2 ? size_t(sim.sheet_table[0]) + 2 * size_t(sim.sheet_table[1]) : 0;
     (void)states;
 
+    // per-region class tables for the TMA step (fused runs on sm_100)
+    LocalClasses lc;
+    if (s->fused && !(std::getenv("FIELDGRID_NO_TMA") && std::getenv("FIELDGRID_NO_TMA")[0] == '1')) {
+        lc = build_local(sim, g, tma_seg(g));
+        s->local = lc.ok;
+    }
     // size the arena
     const size_t fields = size_t(3 * cs);
     size_t need = 0;
@@ -389,8 +596,8 @@ int session_new(Gpu* gpu, const HostSim& sim, const RunSpec& rs, Session** out, 
     need += carve_size(fields * 4) * 2 * field_sets;
     need += carve_size(size_t(std::max<long long>(psi_total, 1)) * 4);
     if (s->fused) need += carve_size(size_t(std::max<long long>(psi_h, 1)) * 4);
-    need += carve_size(nn * size_t(s->cid_bytes));
-    need += carve_size(ncls * sizeof(Coef));
+    need += carve_size(nnp * size_t(s->cid_bytes));
+    need += carve_size(ncls * sizeof(DevCoef));
     need += carve_size((n0 + n1 + n2) * sizeof(AxisNode));
     need += carve_size(64);
     need += carve_size(std::max<uint64_t>(s->series_len, 1) * 4);
@@ -410,7 +617,11 @@ int session_new(Gpu* gpu, const HostSim& sim, const RunSpec& rs, Session** out, 
     need += carve_size(std::max<size_t>(debye_f.size(), 1) * 4) * 2;
     need += carve_size(std::max<size_t>(debye_f.size() * sim.poles.size(), 1) * 4);
     need += carve_size(debye_table.size() * 4);
+    need += carve_size(std::max<size_t>(t_pulse.size(), 1) * 4);
+    need += carve_size(std::max<size_t>(t_dft.size(), 1) * 4) * 2;
     need += carve_size(ENERGY_BLOCKS * 8);
+    need += carve_size(64);
+    if (s->local) need += carve_size(lc.ids.size()) + carve_size(lc.tables.size() * 4);
     size_t free_b = 0, total_b = 0;
     FG_CUDA(cudaMemGetInfo(&free_b, &total_b));
     if (need + (size_t(256) << 20) > free_b) {
@@ -430,8 +641,8 @@ int session_new(Gpu* gpu, const HostSim& sim, const RunSpec& rs, Session** out, 
         float* hb = carve<float>(cur, size_t(std::max<long long>(psi_h, 1)));
         s->psi_h2 = hb - g.psi_off[9];
     }
-    s->node_class = carve<char>(cur, nn * size_t(s->cid_bytes));
-    s->classes = carve<Coef>(cur, ncls);
+    s->node_class = carve<char>(cur, nnp * size_t(s->cid_bytes));
+    s->classes = carve<DevCoef>(cur, ncls);
     s->axes = carve<AxisNode>(cur, n0 + n1 + n2);
     s->counter = carve<unsigned>(cur, 16);
     s->series = carve<float>(cur, std::max<uint64_t>(s->series_len, 1));
@@ -452,44 +663,70 @@ int session_new(Gpu* gpu, const HostSim& sim, const RunSpec& rs, Session** out, 
     s->debye_old = carve<float>(cur, std::max<size_t>(debye_f.size(), 1));
     s->debye_state = carve<float>(cur, std::max<size_t>(debye_f.size() * sim.poles.size(), 1));
     s->debye_table = carve<float>(cur, debye_table.size());
+    float* d_pulse = carve<float>(cur, std::max<size_t>(t_pulse.size(), 1));
+    float* d_dft = carve<float>(cur, std::max<size_t>(t_dft.size(), 1));
+    float* d_far = carve<float>(cur, std::max<size_t>(t_far.size(), 1));
+    sc.pulse = d_pulse;
+    sc.dft = d_dft;
+    sc.far = d_far;
     s->partial = carve<double>(cur, ENERGY_BLOCKS);
+    s->error = carve<int>(cur, 16);
+    if (s->local) {
+        s->local_ids = carve<uint8_t>(cur, lc.ids.size());
+        s->tables = carve<float>(cur, lc.tables.size());
+    }
     if (size_t(cur - s->arena) > need) { err = "internal: arena overflow"; return FG_ERR_INVALID; }
 
     cudaStream_t st = s->stream;
     FG_CUDA(cudaMemsetAsync(s->arena, 0, need, st));
-    // node classes, narrowed on the host in parallel
+    // node classes, narrowed and laid out with the row pitch on the host in parallel
     {
-        std::vector<uint8_t> narrow(nn * size_t(s->cid_bytes));
+        std::vector<uint8_t> narrow(nnp * size_t(s->cid_bytes), 0);
         const uint32_t* src_c = sim.node_class.data();
-        if (s->cid_bytes == 1) {
+        const long long rows = (long long)(n0 * n1);
+        const int cb = s->cid_bytes, p2 = g.p2;
 #pragma omp parallel for schedule(static)
-            for (long long q = 0; q < (long long)nn; ++q) narrow[q] = uint8_t(src_c[q]);
-        } else if (s->cid_bytes == 2) {
-            uint16_t* d = reinterpret_cast<uint16_t*>(narrow.data());
-#pragma omp parallel for schedule(static)
-            for (long long q = 0; q < (long long)nn; ++q) d[q] = uint16_t(src_c[q]);
-        } else {
-            std::memcpy(narrow.data(), src_c, nn * 4);
+        for (long long r = 0; r < rows; ++r) {
+            const uint32_t* in = src_c + r * (long long)n2;
+            if (cb == 1) {
+                uint8_t* d = narrow.data() + r * p2;
+                for (size_t k = 0; k < n2; ++k) d[k] = uint8_t(in[k]);
+            } else if (cb == 2) {
+                uint16_t* d = reinterpret_cast<uint16_t*>(narrow.data()) + r * p2;
+                for (size_t k = 0; k < n2; ++k) d[k] = uint16_t(in[k]);
+            } else {
+                uint32_t* d = reinterpret_cast<uint32_t*>(narrow.data()) + r * p2;
+                std::memcpy(d, in, n2 * 4);
+            }
         }
         FG_CUDA(cudaMemcpyAsync(s->node_class, narrow.data(), narrow.size(), cudaMemcpyHostToDevice, st));
         s->h2d_bytes += narrow.size();
         FG_CUDA(cudaStreamSynchronize(st));
     }
-    FG_CUDA(cudaMemcpyAsync(s->classes, sim.classes.data(), ncls * sizeof(Coef), cudaMemcpyHostToDevice, st));
+    std::vector<DevCoef> dcls(ncls);
+    for (size_t q = 0; q < ncls; ++q) {
+        for (int c = 0; c < 3; ++c) { dcls[q].ca[c] = sim.classes[q].ca[c]; dcls[q].cb[c] = sim.classes[q].cb[c]; }
+        dcls[q].pad0 = dcls[q].pad1 = 0.f;
+    }
+    FG_CUDA(cudaMemcpyAsync(s->classes, dcls.data(), ncls * sizeof(DevCoef), cudaMemcpyHostToDevice, st));
+    FG_CUDA(cudaStreamSynchronize(st));
     std::vector<AxisNode> axes;
     for (int a = 0; a < 3; ++a) axes.insert(axes.end(), sim.ax[a].node.begin(), sim.ax[a].node.end());
     FG_CUDA(cudaMemcpyAsync(s->axes, axes.data(), axes.size() * sizeof(AxisNode), cudaMemcpyHostToDevice, st));
     g.ax[0] = s->axes;
     g.ax[1] = s->axes + n0;
     g.ax[2] = s->axes + n0 + n1;
-    s->h2d_bytes += ncls * sizeof(Coef) + axes.size() * sizeof(AxisNode);
+    s->h2d_bytes += ncls * sizeof(DevCoef) + axes.size() * sizeof(AxisNode);
     auto up = [&](void* dst, const void* srcp, size_t bytes) -> int {
         s->h2d_bytes += bytes;
         if (bytes) FG_CUDA(cudaMemcpyAsync(dst, srcp, bytes, cudaMemcpyHostToDevice, st));
         return FG_OK;
     };
     int rc = FG_OK;
-    rc |= up(s->patch, rs.ntff.data(), rs.ntff.size() * 4);
+    std::vector<uint32_t> patch_dev(rs.ntff.size());
+    for (size_t q = 0; q < rs.ntff.size(); ++q) patch_dev[q] = q % 13 == 0 ? rs.ntff[q] : uint32_t(dev(rs.ntff[q]));
+    if (!rs.ntff.empty() && 3ull * uint64_t(cs) >= (1ull << 32)) { err = "the NTFF box needs 64-bit indices on this grid"; return FG_ERR_UNSUPPORTED; }
+    rc |= up(s->patch, patch_dev.data(), patch_dev.size() * 4);
     rc |= up(s->sources, src.data(), src.size() * sizeof(DevSource));
     rc |= up(s->inductors, ind.data(), ind.size() * sizeof(DevInductor));
     rc |= up(s->probes, probes.data(), probes.size() * sizeof(DevProbe));
@@ -501,11 +738,24 @@ int session_new(Gpu* gpu, const HostSim& sim, const RunSpec& rs, Session** out, 
     rc |= up(s->debye_f, debye_f.data(), debye_f.size() * 8);
     rc |= up(s->debye_dd, debye_dd.data(), debye_dd.size() * 4);
     rc |= up(s->debye_table, debye_table.data(), debye_table.size() * 4);
+    rc |= up(d_pulse, t_pulse.data(), t_pulse.size() * 4);
+    if (s->local) {
+        rc |= up(s->local_ids, lc.ids.data(), lc.ids.size());
+        rc |= up(s->tables, lc.tables.data(), lc.tables.size() * 4);
+    }
+    rc |= up(d_dft, t_dft.data(), t_dft.size() * 4);
+    rc |= up(d_far, t_far.data(), t_far.size() * 4);
     if (rc) return FG_ERR_CUDA;
     FG_CUDA(cudaStreamSynchronize(st));
 
     s->shape = choose_shape(g, s->cid_bytes, s->n_wires > 0);
-    s->variant = s->fused ? fused_name(s->shape) : std::string("separate H+E, 64x4 threads");
+    plan_tma(*s);
+    if (s->tma.ok)
+        s->variant = "TMA fused march, tile " + std::to_string(s->tma.tj) + "x" + std::to_string(s->tma.tk) + ", " +
+                     std::to_string(s->tma.seg) + " planes per block, " + std::to_string(TMA_STAGES) + " stages, " +
+                     (s->local ? "per-block class tables" : "global class table");
+    else
+        s->variant = s->fused ? fused_name(s->shape) + " (" + s->tma.why + ")" : std::string("separate H+E, 64x4 threads");
     s->launches = count_launches(*s);
     // graphs: a block of even length (the fused step alternates buffers), a pair and singles
     s->graph_steps = 32;
@@ -578,6 +828,12 @@ int session_energy(Session* s, double* out, std::string& err) {
     FG_CUDA(cudaMemcpyAsync(part.data(), s->partial, ENERGY_BLOCKS * 8, cudaMemcpyDeviceToHost, s->stream));
     s->d2h_bytes += ENERGY_BLOCKS * 8;
     FG_CUDA(cudaStreamSynchronize(s->stream));
+    int flag = 0;
+    FG_CUDA(cudaMemcpy(&flag, s->error, sizeof(int), cudaMemcpyDeviceToHost));
+    if (flag) {
+        err = "a bounded wait in the fused step ran out (code " + std::to_string(flag) + ")";
+        return FG_ERR_CUDA;
+    }
     double sum = 0.0;
     for (double v : part) sum += v;
     *out = sum;
@@ -607,7 +863,10 @@ int session_read(Session* s, const std::string& which, float* dst, uint64_t len,
         const float* src = which == "e" ? e : h;
         const uint64_t nn = uint64_t(s->geom.nn);
         if (3 * nn > len) { err = "destination too small for " + which; return FG_ERR_INVALID; }
-        for (int c = 0; c < 3; ++c) FG_CUDA(cudaMemcpy(dst + c * nn, src + c * s->geom.cs, nn * 4, cudaMemcpyDeviceToHost));
+        const Geom& g = s->geom;
+        for (int c = 0; c < 3; ++c)
+            FG_CUDA(cudaMemcpy2D(dst + c * nn, size_t(g.n2) * 4, src + c * g.cs, size_t(g.p2) * 4, size_t(g.n2) * 4,
+                                 size_t(g.n0) * g.n1, cudaMemcpyDeviceToHost));
         s->d2h_bytes += 3 * nn * 4;
         return FG_OK;
     }

@@ -11,15 +11,26 @@
 
 namespace fg {
 
-// Node geometry shared by every kernel. Fields are component-major with component stride `cs`
-// (>= nn, padded to 32 floats) and node id (i*n1 + j)*n2 + k.
+// Node geometry shared by every kernel. On the device a row of n2 nodes is stored with pitch p2
+// (n2 rounded up to 32, so rows start 128-byte aligned and TMA strides are legal): the device
+// node index is (i*n1 + j)*p2 + k. Fields are component-major with component stride cs
+// (>= n0*n1*p2). The psi slabs keep the reference's unpadded layout (sim.rs:659-665).
 struct Geom {
     int n0, n1, n2;
+    int p2;
     int pml;
-    long long nn;
+    long long nn;               // real nodes n0*n1*n2
     long long cs;
     const AxisNode* ax[3];
     long long psi_off[18];  // offsets of the 12 psi slabs: [field*9 + comp*3 + axis], field 0 = E, 1 = H
+};
+
+// A node's three (ca, cb) pairs as the kernels read them: 32 bytes, two 16-byte loads.
+struct __align__(16) DevCoef {
+    float ca[3];
+    float pad0;
+    float cb[3];
+    float pad1;
 };
 
 struct DevSheet {           // pack() sheet record (run.rs:259-289), named
@@ -42,6 +53,11 @@ struct StepConst {          // per-run scalars (run.rs:433-464 Params)
     float omega[4];
     unsigned cap;
     int ports;
+    // Per-step tables formed on the host with the same f32 libm calls as the reference's CPU path
+    // (cpu.rs:262-265, :344-353, :370-405), for steps below `cap`:
+    const float* pulse;     // [cap]             pulse((n + 1/2) dt)
+    const float* dft;       // [cap][nf][4]      cos(w te) dt, -sin(w te) dt, cos(w th) dt, -sin(w th) dt
+    const float* far;       // [cap][nf][4]      cos(-w te) dt, sin(-w te) dt, cos(-w th) dt, sin(-w th) dt
 };
 
 __device__ __forceinline__ long long psi_at(const Geom& g, int a, int i, int j, int k, int s) {
@@ -140,7 +156,7 @@ __global__ void k_debye_pre(const long long* __restrict__ f, int count, const fl
 template <typename CID>
 __global__ void k_debye_post(const long long* __restrict__ f, const float* __restrict__ dd, int count,
                              const float* __restrict__ eold_saved, const float* __restrict__ eold_field,
-                             const CID* __restrict__ node_class, const Coef* __restrict__ classes, long long cs,
+                             const CID* __restrict__ node_class, const DevCoef* __restrict__ classes, long long cs,
                              const float* __restrict__ table, float* __restrict__ state, float* __restrict__ e) {
     int q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= count) return;
@@ -173,8 +189,7 @@ __device__ __forceinline__ float pulse_at(const StepConst& sc, float t) {
 __global__ void k_lumped(const DevSource* __restrict__ src, int ns, DevInductor* __restrict__ ind, int ni,
                          StepConst sc, const unsigned* __restrict__ counter, float* __restrict__ e) {
     const unsigned n = step_index(counter);
-    const float t = (float(n) + 0.5f) * sc.dt;
-    const float p = pulse_at(sc, t);
+    const float p = n < sc.cap ? sc.pulse[n] : pulse_at(sc, (float(n) + 0.5f) * sc.dt);
     for (int q = threadIdx.x; q < ns; q += blockDim.x) {
         DevSource s = src[q];
         e[s.f] -= s.src * p;
@@ -230,13 +245,19 @@ __global__ void k_field_dft(Geom g, int plane_k, StepConst sc, const unsigned* _
     if (q >= (long long)g.n0 * g.n1) return;
     const unsigned n = step_index(counter);
     const float te = (float(n) + 1.0f) * sc.dt, th = (float(n) + 0.5f) * sc.dt;
-    const long long id = q * g.n2 + plane_k;
+    const long long id = q * g.p2 + plane_k;
     const float f[5] = {e[id], e[g.cs + id], e[2 * g.cs + id], h[id], h[g.cs + id]};
     float* out = acc + q * sc.nf * 10;
     for (int k = 0; k < sc.nf; ++k) {
         const float w = sc.omega[k];
-        const float ce0 = cosf(w * te) * sc.dt, ce1 = -sinf(w * te) * sc.dt;
-        const float ch0 = cosf(w * th) * sc.dt, ch1 = -sinf(w * th) * sc.dt;
+        float ce0, ce1, ch0, ch1;
+        if (n < sc.cap) {
+            const float* t = sc.dft + ((long long)n * sc.nf + k) * 4;
+            ce0 = t[0]; ce1 = t[1]; ch0 = t[2]; ch1 = t[3];
+        } else {
+            ce0 = cosf(w * te) * sc.dt; ce1 = -sinf(w * te) * sc.dt;
+            ch0 = cosf(w * th) * sc.dt; ch1 = -sinf(w * th) * sc.dt;
+        }
 #pragma unroll
         for (int c = 0; c < 5; ++c) {
             const float p0 = c >= 3 ? ch0 : ce0, p1 = c >= 3 ? ch1 : ce1;
@@ -272,8 +293,14 @@ __global__ void k_ntff(const unsigned* __restrict__ pidx, int patches, long long
     float* out = acc + (long long)g * sc.nf * 12;
     for (int k = 0; k < sc.nf; ++k) {
         const float wf = sc.omega[k];
-        const float pe0 = cosf(-wf * te) * sc.dt, pe1 = sinf(-wf * te) * sc.dt;
-        const float ph0 = cosf(-wf * th) * sc.dt, ph1 = sinf(-wf * th) * sc.dt;
+        float pe0, pe1, ph0, ph1;
+        if (n < sc.cap) {
+            const float* t = sc.far + ((long long)n * sc.nf + k) * 4;
+            pe0 = t[0]; pe1 = t[1]; ph0 = t[2]; ph1 = t[3];
+        } else {
+            pe0 = cosf(-wf * te) * sc.dt; pe1 = sinf(-wf * te) * sc.dt;
+            ph0 = cosf(-wf * th) * sc.dt; ph1 = sinf(-wf * th) * sc.dt;
+        }
         float* o = out + k * 12;
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
@@ -285,7 +312,8 @@ __global__ void k_ntff(const unsigned* __restrict__ pidx, int patches, long long
     }
 }
 
-// cpu.rs:417-421: sum of E^2 + (376.73 H)^2 in f64, one partial per block.
+// cpu.rs:417-421: sum of E^2 + (376.73 H)^2 in f64, one partial per block. Row padding and the
+// component tail hold zeros and add nothing.
 __global__ void k_energy(Geom g, const float* __restrict__ e, const float* __restrict__ h, double* __restrict__ partial) {
     __shared__ double s[256];
     double acc = 0.0;
@@ -293,7 +321,7 @@ __global__ void k_energy(Geom g, const float* __restrict__ e, const float* __res
     for (int c = 0; c < 3; ++c) {
         const float* ec = e + c * g.cs;
         const float* hc = h + c * g.cs;
-        for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < g.nn; q += stride) {
+        for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < g.cs; q += stride) {
             double x = double(ec[q]);
             double y = double(hc[q]) * 376.73;
             acc += x * x + y * y;

@@ -28,7 +28,7 @@ struct FusedShape {
 struct FusedArgs {
     Geom g;
     const void* node_class;
-    const Coef* classes;
+    const DevCoef* classes;
     const float* __restrict__ e_in;
     const float* __restrict__ h_in;
     float* __restrict__ e_out;
@@ -45,7 +45,7 @@ __device__ __forceinline__ int dim_of(const Geom& g) { return A == 0 ? g.n0 : (A
 
 template <int A>
 __device__ __forceinline__ long long stride_of(const Geom& g) {
-    return A == 0 ? (long long)g.n1 * g.n2 : (A == 1 ? (long long)g.n2 : 1ll);
+    return A == 0 ? (long long)g.n1 * g.p2 : (A == 1 ? (long long)g.p2 : 1ll);
 }
 
 // New H_C at node (i, j, k) from the step's inputs (cpu.rs:65-102). `own` nodes also write psi.
@@ -54,7 +54,7 @@ __device__ __forceinline__ float h_new(const FusedArgs& a, int i, int j, int k, 
     constexpr int U = (C + 1) % 3, V = (C + 2) % 3;
     const Geom& g = a.g;
     const int p[3] = {i, j, k};
-    const long long id = ((long long)i * g.n1 + j) * g.n2 + k;
+    const long long id = ((long long)i * g.n1 + j) * g.p2 + k;
     const float hin = a.h_in[C * g.cs + id];
     if (p[U] + 1 >= dim_of<U>(g) || p[V] + 1 >= dim_of<V>(g)) return hin;
     const float e_v = a.e_in[V * g.cs + id];
@@ -136,7 +136,7 @@ __global__ void __launch_bounds__(TK* TJ) k_fused_step(FusedArgs a, int seg) {
         const int o = i & 1;
         float hx = 0.f, hy = 0.f, hz = 0.f;
         if (live) {
-            const long long id = ((long long)i * g.n1 + j) * g.n2 + k;
+            const long long id = ((long long)i * g.n1 + j) * g.p2 + k;
             hx = h_new<0>(a, i, j, k, true);
             hy = h_new<1>(a, i, j, k, true);
             hz = h_new<2>(a, i, j, k, true);
@@ -158,9 +158,9 @@ __global__ void __launch_bounds__(TK* TJ) k_fused_step(FusedArgs a, int seg) {
         }
         __syncthreads();
         if (live) {
-            const long long id = ((long long)i * g.n1 + j) * g.n2 + k;
+            const long long id = ((long long)i * g.n1 + j) * g.p2 + k;
             const int p[3] = {i, j, k};
-            const Coef cf = a.classes[cls[id]];
+            const DevCoef cf = a.classes[cls[id]];
             const float hx_j = hs[o][0][lj][lk + 1];
             const float hz_j = hs[o][2][lj][lk + 1];
             const float hx_k = hs[o][0][lj + 1][lk];
@@ -192,7 +192,7 @@ inline std::string fused_name(const FusedShape& s) {
            " planes per block";
 }
 
-inline int launch_fused(const FusedShape& s, int cid_bytes, const Geom& g, const void* node_class, const Coef* classes,
+inline int launch_fused(const FusedShape& s, int cid_bytes, const Geom& g, const void* node_class, const DevCoef* classes,
                         const float* e_in, const float* h_in, float* e_out, float* h_out, float* psi_e,
                         const float* psi_h_in, float* psi_h_out, float k_mu, unsigned* counter, bool /*wires*/,
                         cudaStream_t st) {

@@ -46,7 +46,7 @@ __device__ __forceinline__ void h_update_one(const Geom& g, const int p[3], long
 // cb == 0 (cpu.rs:125-162)
 template <int C>
 __device__ __forceinline__ void e_update_one(const Geom& g, const int p[3], long long id, const long long st[3],
-                                             const Coef& cf, const float* __restrict__ h, float* __restrict__ e,
+                                             const DevCoef& cf, const float* __restrict__ h, float* __restrict__ e,
                                              float* __restrict__ psi) {
     constexpr int U = (C + 1) % 3, V = (C + 2) % 3;
     const float cb = cf.cb[C];
@@ -87,8 +87,8 @@ __global__ void __launch_bounds__(256) k_update_h(Geom g, const float* __restric
     const int i = blockIdx.z;
     if (k >= g.n2 || j >= g.n1) return;
     const int p[3] = {i, j, k};
-    const long long st[3] = {(long long)g.n1 * g.n2, g.n2, 1};
-    const long long id = ((long long)i * g.n1 + j) * g.n2 + k;
+    const long long st[3] = {(long long)g.n1 * g.p2, g.p2, 1};
+    const long long id = ((long long)i * g.n1 + j) * g.p2 + k;
     h_update_one<0>(g, p, id, st, e, h, psi, k_mu);
     h_update_one<1>(g, p, id, st, e, h, psi, k_mu);
     h_update_one<2>(g, p, id, st, e, h, psi, k_mu);
@@ -96,16 +96,16 @@ __global__ void __launch_bounds__(256) k_update_h(Geom g, const float* __restric
 
 template <typename CID>
 __global__ void __launch_bounds__(256) k_update_e(Geom g, const CID* __restrict__ node_class,
-                                                  const Coef* __restrict__ classes, const float* __restrict__ h,
+                                                  const DevCoef* __restrict__ classes, const float* __restrict__ h,
                                                   float* __restrict__ e, float* __restrict__ psi) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
     const int i = blockIdx.z;
     if (k >= g.n2 || j >= g.n1) return;
     const int p[3] = {i, j, k};
-    const long long st[3] = {(long long)g.n1 * g.n2, g.n2, 1};
-    const long long id = ((long long)i * g.n1 + j) * g.n2 + k;
-    const Coef cf = classes[node_class[id]];
+    const long long st[3] = {(long long)g.n1 * g.p2, g.p2, 1};
+    const long long id = ((long long)i * g.n1 + j) * g.p2 + k;
+    const DevCoef cf = classes[node_class[id]];
     e_update_one<0>(g, p, id, st, cf, h, e, psi);
     e_update_one<1>(g, p, id, st, cf, h, e, psi);
     e_update_one<2>(g, p, id, st, cf, h, e, psi);

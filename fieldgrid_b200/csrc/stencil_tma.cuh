@@ -1,0 +1,510 @@
+// The fused E+H step fed by the Tensor Memory Accelerator: the engine's main stencil on the B200.
+//
+// A block owns a TJ x TK tile of (j, k) columns and marches along x over a segment of planes.
+// One producer warp streams, per plane p, three boxes into a ring of shared-memory stages with
+// cp.async.bulk.tensor (4-D maps over (k, j, i, component)):
+//   E(p)     rows j0-1 .. j0+TJ,   columns k0-4 .. k0+TK+3 (all 3 components)
+//   H_in(p)  rows j0-1 .. j0+TJ-1, columns k0-4 .. k0+TK-1 (all 3 components)
+//   class(p) rows j0   .. j0+TJ-1, columns k0   .. k0+TK-1 (the node class ids)
+// Box origins in k are rounded down to 16 bytes; rows or planes outside the grid arrive as zeros.
+// Eight consumer warps then, per plane i:
+//   1. form the new H on the tile and on its j-1 row and k-1 column (the halo the E update needs;
+//      halo points are recomputed, read-only) from the E(i), E(i+1) and H_in(i) boxes, into a
+//      triple-buffered H tile; owned points go to the output buffer;
+//   2. after one barrier, form the new E of the tile from the H tile of plane i and of plane i-1.
+// Each node's E and H are read from DRAM once and written once per step (48 B) plus its class id;
+// the halo reads hit L2. The CPML psi recursions run only on tiles/planes inside the absorbing
+// layer (a block-uniform test), with the E slabs in place and the H slabs ping-ponged like the
+// fields. Mbarrier waits are bounded by the global timer: a wait that runs out raises the error
+// word and the block leaves without starting new work.
+#pragma once
+
+#include <cuda.h>
+
+#include <string>
+
+#include "kernels.cuh"
+
+namespace fg {
+
+namespace tma {
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return uint32_t(__cvta_generic_to_shared(p)); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+__device__ __forceinline__ uint64_t global_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Waits for the phase of the given parity to complete; false after `limit_ns` without it.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint64_t limit_ns) {
+    if (mbar_try_wait(bar, parity)) return true;
+    const uint64_t t0 = global_ns();
+    while (!mbar_try_wait(bar, parity))
+        if (global_ns() - t0 > limit_ns) return false;
+    return true;
+}
+
+__device__ __forceinline__ void load_4d(void* dst, const CUtensorMap* map, uint64_t* bar, int x, int y, int z, int w) {
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%3, %4, %5, %6}], [%2];" ::"r"(smem_u32(dst)),
+        "l"(map), "r"(smem_u32(bar)), "r"(x), "r"(y), "r"(z), "r"(w)
+        : "memory");
+}
+
+__device__ __forceinline__ void load_3d(void* dst, const CUtensorMap* map, uint64_t* bar, int x, int y, int z) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%3, %4, %5}], [%2];" ::"r"(smem_u32(dst)),
+        "l"(map), "r"(smem_u32(bar)), "r"(x), "r"(y), "r"(z)
+        : "memory");
+}
+
+// Consumer-only barrier (named barrier 1) that also ORs a flag across the consumers.
+__device__ __forceinline__ bool consumers_sync_or(bool flag, int count) {
+    int out;
+    asm volatile(
+        "{\n\t.reg .pred p, q;\n\t"
+        "setp.ne.s32 p, %1, 0;\n\t"
+        "barrier.cta.red.or.pred q, 1, %2, p;\n\t"
+        "selp.s32 %0, 1, 0, q;\n\t}"
+        : "=r"(out)
+        : "r"(int(flag)), "r"(count)
+        : "memory");
+    return out != 0;
+}
+
+constexpr uint64_t WAIT_LIMIT_NS = 2000000000ull;  // 2 s: far beyond any legitimate copy
+
+}  // namespace tma
+
+// Shared-memory layout of one block (tile TJ x TK, TJ + 1 consumer warps' worth of rows).
+// With LOCAL, class ids are 8-bit indices into a per-block table of at most LOCAL_CLASSES
+// (ca[3], cb[3]) records that the block keeps in shared memory.
+constexpr int LOCAL_CLASSES = 256;
+
+template <int TJ, int TK, typename CID, int STAGES, int SEGMAX, bool LOCAL = false>
+struct TmaLayout {
+    static constexpr int EW = TK + 8, ER = TJ + 2;   // E box: columns k0-4 .. k0+TK+3, rows j0-1 .. j0+TJ
+    static constexpr int HW = TK + 8, HR = TJ + 1;   // H box: columns k0-4 .. k0+TK+3, rows j0-1 .. j0+TJ-1
+    static constexpr int CW = TK + 16, CR = TJ;      // class box: columns k0 .. k0+TK+15, rows j0 .. j0+TJ-1
+    static constexpr int NW = TK + 4, NR = TJ + 1;   // new-H tile: column k at k-k0+2, row j at j-j0+1
+    static constexpr int E_BYTES = 3 * ER * EW * 4;
+    static constexpr int H_BYTES = 3 * HR * HW * 4;
+    static constexpr int C_BYTES = CR * CW * int(sizeof(CID));
+    __host__ __device__ static constexpr int al(int b) { return (b + 127) & ~127; }
+    static constexpr int STAGE = al(E_BYTES) + al(H_BYTES) + al(C_BYTES);
+    static constexpr int TX = E_BYTES + H_BYTES + C_BYTES;  // bytes one stage's copies deliver
+    static constexpr int HN = al(3 * NR * NW * 4);
+    static constexpr int NAX = (TJ + 2) + (TK + 4) + (SEGMAX + 2);
+    static constexpr int AX = al(NAX * int(sizeof(AxisNode)));
+    static constexpr int BARS = al(2 * STAGES * 8);
+    static constexpr int LT = LOCAL ? al(LOCAL_CLASSES * 6 * 4) : 0;  // the block's coefficient table
+    static constexpr int TOTAL = STAGES * STAGE + 2 * HN + AX + BARS + LT + 128;
+};
+
+struct TmaArgs {
+    Geom g;
+    const DevCoef* classes;
+    float* __restrict__ e_out;
+    float* __restrict__ h_out;
+    float* __restrict__ psi_e;           // E slabs, in place
+    const float* __restrict__ psi_h_in;  // H slabs of the step's input set
+    float* __restrict__ psi_h_out;
+    float k_mu;
+    int seg;
+    int ktiles;                          // tiles along k (the last may own one extra column)
+    int jtiles;
+    const float* tables;                 // LOCAL: per block region, LOCAL_CLASSES x (ca[3], cb[3])
+    unsigned* counter;
+    int* error;
+};
+
+// H_C at one point with CPML; writes psi only for owned points (cpu.rs:65-102).
+template <int C>
+__device__ __forceinline__ float h_point(const TmaArgs& a, float hin, float ev, float eu, const AxisNode& axu,
+                                         const AxisNode& axv, int i, int j, int k, bool own) {
+    constexpr int U = (C + 1) % 3, V = (C + 2) % 3;
+    const Geom& g = a.g;
+    float t1 = ev * axu.inv_d;
+    float t2 = eu * axv.inv_d;
+    if (axu.slot_h >= 0) {
+        const long long q = g.psi_off[9 + C * 3 + U] + psi_at(g, U, i, j, k, axu.slot_h);
+        const float r = axu.bh * a.psi_h_in[q] + axu.ch * ev * axu.raw_inv_d;
+        if (own) a.psi_h_out[q] = r;
+        t1 += r;
+    }
+    if (axv.slot_h >= 0) {
+        const long long q = g.psi_off[9 + C * 3 + V] + psi_at(g, V, i, j, k, axv.slot_h);
+        const float r = axv.bh * a.psi_h_in[q] + axv.ch * eu * axv.raw_inv_d;
+        if (own) a.psi_h_out[q] = r;
+        t2 += r;
+    }
+    return hin - a.k_mu * (t1 - t2);
+}
+
+// E_C at an owned point with CPML (cpu.rs:125-162).
+template <int C>
+__device__ __forceinline__ float e_point(const TmaArgs& a, float e_own, float ca, float cb, float hv, float hu,
+                                         const AxisNode& axu, const AxisNode& axv, int i, int j, int k) {
+    constexpr int U = (C + 1) % 3, V = (C + 2) % 3;
+    const Geom& g = a.g;
+    float t1 = hv * axu.inv_dd;
+    float t2 = hu * axv.inv_dd;
+    if (axu.slot_e >= 0) {
+        const long long q = g.psi_off[C * 3 + U] + psi_at(g, U, i, j, k, axu.slot_e);
+        const float r = axu.be * a.psi_e[q] + axu.ce * hv * axu.raw_inv_dd;
+        a.psi_e[q] = r;
+        t1 += r;
+    }
+    if (axv.slot_e >= 0) {
+        const long long q = g.psi_off[C * 3 + V] + psi_at(g, V, i, j, k, axv.slot_e);
+        const float r = axv.be * a.psi_e[q] + axv.ce * hu * axv.raw_inv_dd;
+        a.psi_e[q] = r;
+        t2 += r;
+    }
+    return ca * e_own + cb * (t1 - t2);
+}
+
+// The E values around one point that its H update needs (own, +j, +k, +i neighbours).
+struct ENb {
+    float x, y, z;        // own
+    float z_jp, x_jp;     // Ez, Ex at j+1
+    float y_kp, x_kp;     // Ey, Ex at k+1
+    float z_ip, y_ip;     // Ez, Ey at i+1
+};
+
+struct PtAxes {           // the axis factors of one point
+    const AxisNode* aj;
+    const AxisNode* ak;
+    bool jn, kn, pml;     // j+1 / k+1 inside the grid; j or k inside the absorbing layer
+};
+
+// New H at one point (the update of cpu.rs:48-107); `pml` selects the CPML form.
+__device__ __forceinline__ void h_node(const TmaArgs& a, const ENb& n, float& hx, float& hy, float& hz,
+                                       const PtAxes& q, const AxisNode& ai, bool in, bool pml, int i, int j, int k,
+                                       bool own) {
+    if (!pml) {
+        const float idj = q.aj->inv_d, idk = q.ak->inv_d, idi = ai.inv_d;
+        if (q.jn && q.kn) hx = hx - a.k_mu * ((n.z_jp - n.z) * idj - (n.y_kp - n.y) * idk);
+        if (q.kn && in) hy = hy - a.k_mu * ((n.x_kp - n.x) * idk - (n.z_ip - n.z) * idi);
+        if (in && q.jn) hz = hz - a.k_mu * ((n.y_ip - n.y) * idi - (n.x_jp - n.x) * idj);
+    } else {
+        const AxisNode aj = *q.aj, ak = *q.ak;
+        if (q.jn && q.kn) hx = h_point<0>(a, hx, n.z_jp - n.z, n.y_kp - n.y, aj, ak, i, j, k, own);
+        if (q.kn && in) hy = h_point<1>(a, hy, n.x_kp - n.x, n.z_ip - n.z, ak, ai, i, j, k, own);
+        if (in && q.jn) hz = h_point<2>(a, hz, n.y_ip - n.y, n.x_jp - n.x, ai, aj, i, j, k, own);
+    }
+}
+
+// New E at one owned point; h*_jm / h*_km are the new H at j-1 / k-1, py / pz the H of plane i-1.
+struct CoefRef {          // three ca then three cb
+    float ca[3], cb[3];
+};
+
+__device__ __forceinline__ void e_node(const TmaArgs& a, const CoefRef& cf, float& ex, float& ey, float& ez,
+                                       float hx, float hy, float hz, float hz_jm, float hx_jm, float hy_km,
+                                       float hx_km, float py, float pz, const PtAxes& q, const AxisNode& ai, bool pml,
+                                       int i, int j, int k) {
+    if (!pml) {
+        const float iddj = q.aj->inv_dd, iddk = q.ak->inv_dd, iddi = ai.inv_dd;
+        if (cf.cb[0] != 0.0f && j > 0 && k > 0) ex = cf.ca[0] * ex + cf.cb[0] * ((hz - hz_jm) * iddj - (hy - hy_km) * iddk);
+        if (cf.cb[1] != 0.0f && k > 0 && i > 0) ey = cf.ca[1] * ey + cf.cb[1] * ((hx - hx_km) * iddk - (hz - pz) * iddi);
+        if (cf.cb[2] != 0.0f && i > 0 && j > 0) ez = cf.ca[2] * ez + cf.cb[2] * ((hy - py) * iddi - (hx - hx_jm) * iddj);
+    } else {
+        const AxisNode aj = *q.aj, ak = *q.ak;
+        if (cf.cb[0] != 0.0f && j > 0 && k > 0) ex = e_point<0>(a, ex, cf.ca[0], cf.cb[0], hz - hz_jm, hy - hy_km, aj, ak, i, j, k);
+        if (cf.cb[1] != 0.0f && k > 0 && i > 0) ey = e_point<1>(a, ey, cf.ca[1], cf.cb[1], hx - hx_km, hz - pz, ak, ai, i, j, k);
+        if (cf.cb[2] != 0.0f && i > 0 && j > 0) ez = e_point<2>(a, ez, cf.ca[2], cf.cb[2], hy - py, hx - hx_jm, ai, aj, i, j, k);
+    }
+}
+
+constexpr int TMA_CONSUMERS = 256;
+
+// Tile TJ = 7 rows x TK = 64 columns; consumer warp w computes row j0 + w - 1 (warp 0: the halo
+// row j0 - 1), each lane a pair of columns k0 + 2 lane, +1. Warp 0 lanes 0..TJ-1 also take the
+// halo column k0 - 1, lanes TJ..2TJ-1 the column k0 + TK when the tile owns it (a grid whose
+// node count along k is 64t + 1).
+// The coefficients of class `id`: from the block's shared table or from the global table.
+template <bool LOCAL>
+__device__ __forceinline__ CoefRef coef_of(const TmaArgs& a, const float* lt, unsigned id) {
+    CoefRef c;
+    if constexpr (LOCAL) {
+        const float* t = lt + id * 6;
+#pragma unroll
+        for (int q = 0; q < 3; ++q) { c.ca[q] = t[q]; c.cb[q] = t[3 + q]; }
+    } else {
+        const DevCoef d = a.classes[id];
+#pragma unroll
+        for (int q = 0; q < 3; ++q) { c.ca[q] = d.ca[q]; c.cb[q] = d.cb[q]; }
+    }
+    return c;
+}
+
+template <int TJ, int TK, typename CID, int STAGES, int SEGMAX, bool LOCAL>
+__global__ void __launch_bounds__(TMA_CONSUMERS + 32, 3)
+    k_tma_step(const __grid_constant__ CUtensorMap map_e, const __grid_constant__ CUtensorMap map_h,
+               const __grid_constant__ CUtensorMap map_c, TmaArgs a) {
+    static_assert(TJ + 1 == TMA_CONSUMERS / 32 && TK == 64, "one warp per row, one column pair per lane");
+    using L = TmaLayout<TJ, TK, CID, STAGES, SEGMAX, LOCAL>;
+    static_assert(!LOCAL || sizeof(CID) == 1, "local class ids are 8-bit");
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    unsigned char* base = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
+    unsigned char* stages = base;
+    float* hn_all = reinterpret_cast<float*>(base + STAGES * L::STAGE);
+    AxisNode* axj = reinterpret_cast<AxisNode*>(base + STAGES * L::STAGE + 2 * L::HN);  // rows j0-1 .. j0+TJ
+    AxisNode* axk = axj + (TJ + 2);                                                    // cols k0-1 .. k0+TK+2
+    AxisNode* axi = axk + (TK + 4);                                                    // planes p_first .. i1
+    uint64_t* full = reinterpret_cast<uint64_t*>(base + STAGES * L::STAGE + 2 * L::HN + L::AX);
+    uint64_t* empty = full + STAGES;
+    float* lt = reinterpret_cast<float*>(base + STAGES * L::STAGE + 2 * L::HN + L::AX + L::BARS);
+
+    const Geom& g = a.g;
+    const int tid = threadIdx.x;
+    const int k0 = blockIdx.x * TK, j0 = blockIdx.y * TJ;
+    const int i0 = blockIdx.z * a.seg;
+    const int i1 = min(i0 + a.seg, g.n0);
+    const int p_first = i0 > 0 ? i0 - 1 : 0;   // plane i0-1 supplies H(i0-1) for the first E update
+    const int p_last = i1;                     // E(i1) for the last H update (zeros past the grid)
+    const bool redge = int(blockIdx.x) == a.ktiles - 1 && k0 + TK == g.n2 - 1;
+    if ((blockIdx.x | blockIdx.y | blockIdx.z | tid) == 0) *a.counter += 1u;
+
+    if (tid == 0) {
+        for (int s = 0; s < STAGES; ++s) {
+            tma::mbar_init(&full[s], 1);
+            tma::mbar_init(&empty[s], TMA_CONSUMERS);
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    for (int q = tid; q < L::NAX; q += blockDim.x) {
+        AxisNode v;
+        if (q < TJ + 2) v = g.ax[1][min(max(j0 - 1 + q, 0), g.n1 - 1)];
+        else if (q < TJ + 2 + TK + 4) v = g.ax[2][min(max(k0 - 1 + (q - TJ - 2), 0), g.n2 - 1)];
+        else v = g.ax[0][min(p_first + (q - TJ - 2 - TK - 4), g.n0 - 1)];
+        axj[q] = v;
+    }
+    if constexpr (LOCAL) {
+        const long long region = ((long long)blockIdx.z * a.jtiles + blockIdx.y) * a.ktiles + blockIdx.x;
+        const float* src = a.tables + region * (LOCAL_CLASSES * 6);
+        for (int q = tid; q < LOCAL_CLASSES * 6; q += blockDim.x) lt[q] = src[q];
+    }
+    __syncthreads();
+
+    if (tid >= TMA_CONSUMERS) {
+        // producer warp: one lane issues the copies
+        if (tid != TMA_CONSUMERS) return;
+        for (int p = p_first; p <= p_last; ++p) {
+            const int u = p - p_first, s = u % STAGES, n = u / STAGES;
+            if (!tma::mbar_wait(&empty[s], uint32_t((n & 1) ^ 1), tma::WAIT_LIMIT_NS)) {
+                atomicExch(a.error, 1);
+                for (int q = max(p_first, p - STAGES); q < p; ++q) {
+                    const int uq = q - p_first;
+                    tma::mbar_wait(&full[uq % STAGES], uint32_t((uq / STAGES) & 1), tma::WAIT_LIMIT_NS);
+                }
+                return;
+            }
+            unsigned char* st = stages + s * L::STAGE;
+            tma::mbar_expect_tx(&full[s], L::TX);
+            tma::load_4d(st, &map_e, &full[s], k0 - 4, j0 - 1, p, 0);
+            tma::load_4d(st + L::al(L::E_BYTES), &map_h, &full[s], k0 - 4, j0 - 1, p, 0);
+            tma::load_3d(st + L::al(L::E_BYTES) + L::al(L::H_BYTES), &map_c, &full[s], k0, j0, p);
+        }
+        return;
+    }
+
+    // ---- consumers
+    constexpr int EC = L::ER * L::EW, HC = L::HR * L::HW, NC = L::NR * L::NW;
+    const int w = tid >> 5, lane = tid & 31;
+    const int r = w - 1;              // tile row of this warp's pair (-1: the halo row)
+    const int c = 2 * lane;           // first column of the pair
+    const int jj = j0 + r, kk = k0 + c;
+    const bool row_live = jj >= 0 && jj < g.n1;
+    const bool live0 = row_live && kk < g.n2, live1 = row_live && kk + 1 < g.n2;
+    const bool own_row = r >= 0;
+    const AxisNode* rj = axj + (r + 1);
+    PtAxes q0{rj, axk + (c + 1), jj + 1 < g.n1, kk + 1 < g.n2, false};
+    PtAxes q1{rj, axk + (c + 2), jj + 1 < g.n1, kk + 2 < g.n2, false};
+    const bool pml_j = g.pml > 0 && (rj->slot_e >= 0 || rj->slot_h >= 0);
+    q0.pml = pml_j || (g.pml > 0 && (q0.ak->slot_e >= 0 || q0.ak->slot_h >= 0));
+    q1.pml = pml_j || (g.pml > 0 && (q1.ak->slot_e >= 0 || q1.ak->slot_h >= 0));
+    const int eo = (r + 1) * L::EW + c + 4, ho = (r + 1) * L::HW + c + 4, no = (r + 1) * L::NW + c + 2;
+    const unsigned goff = unsigned(max(jj, 0)) * unsigned(g.p2) + unsigned(kk);
+    // warp 0 extras: the k-1 halo column (lanes 0..TJ-1), the owned right-edge column (lanes
+    // TJ..2TJ-1) and that column's j-1 halo point (lane 2TJ)
+    const int xr = lane < TJ ? lane : (lane < 2 * TJ ? lane - TJ : -1);  // row of the extra point
+    const int xc = lane < TJ ? -1 : TK;                                   // column of the extra point
+    const bool xtra = w == 0 && ((lane < TJ && k0 > 0) || (lane >= TJ && lane <= 2 * TJ && redge)) &&
+                      j0 + xr >= 0 && j0 + xr < g.n1;
+    const bool xown = xtra && lane >= TJ && lane < 2 * TJ;                // the right-edge points are owned
+    const int xj = j0 + xr, xk = k0 + xc;
+    PtAxes qx{axj + (xr + 1), axk + (xc + 1), xj + 1 < g.n1, xk + 1 < g.n2, false};
+    qx.pml = g.pml > 0 && (qx.aj->slot_e >= 0 || qx.aj->slot_h >= 0 || qx.ak->slot_e >= 0 || qx.ak->slot_h >= 0);
+    const int xeo = (xr + 1) * L::EW + xc + 4, xho = (xr + 1) * L::HW + xc + 4, xno = (xr + 1) * L::NW + xc + 2;
+    const unsigned xgoff = unsigned(min(xj, g.n1 - 1)) * unsigned(g.p2) + unsigned(max(xk, 0));
+
+    float py0 = 0.f, pz0 = 0.f, py1 = 0.f, pz1 = 0.f, pyx = 0.f, pzx = 0.f;  // H of plane i-1
+    bool bad = false;
+    for (int p = p_first; p < i1; ++p) {
+        const int u = p - p_first;
+        const int s = u % STAGES, s1 = (u + 1) % STAGES;
+        const bool pre = p < i0;  // the plane before the segment: H only, nothing written
+        if (!tma::mbar_wait(&full[s], uint32_t((u / STAGES) & 1), tma::WAIT_LIMIT_NS)) bad = true;
+        if (!tma::mbar_wait(&full[s1], uint32_t(((u + 1) / STAGES) & 1), tma::WAIT_LIMIT_NS)) bad = true;
+        const float* E = reinterpret_cast<const float*>(stages + s * L::STAGE);
+        const float* E1 = reinterpret_cast<const float*>(stages + s1 * L::STAGE);
+        const float* H = reinterpret_cast<const float*>(stages + s * L::STAGE + L::al(L::E_BYTES));
+        const CID* CL = reinterpret_cast<const CID*>(stages + s * L::STAGE + L::al(L::E_BYTES) + L::al(L::H_BYTES));
+        float* hn = hn_all + (u & 1) * (L::HN / 4);
+        const int i = p;
+        const AxisNode& ai = axi[u];
+        const bool pml_i = g.pml > 0 && (ai.slot_e >= 0 || ai.slot_h >= 0);
+        const bool in = i + 1 < g.n0;
+        const long long plane = (long long)i * g.n1 * g.p2;
+        const bool own = own_row && !pre;
+
+        // 1. new H: the pair (two columns), and warp 0's extra point
+        ENb nb0, nb1;
+        float hx0 = 0.f, hy0 = 0.f, hz0 = 0.f, hx1 = 0.f, hy1 = 0.f, hz1 = 0.f;
+        if (live0) {
+            const float2 x = *reinterpret_cast<const float2*>(E + eo);
+            const float2 y = *reinterpret_cast<const float2*>(E + EC + eo);
+            const float2 z = *reinterpret_cast<const float2*>(E + 2 * EC + eo);
+            const float2 zj = *reinterpret_cast<const float2*>(E + 2 * EC + eo + L::EW);
+            const float2 xj = *reinterpret_cast<const float2*>(E + eo + L::EW);
+            const float2 zi = *reinterpret_cast<const float2*>(E1 + 2 * EC + eo);
+            const float2 yi = *reinterpret_cast<const float2*>(E1 + EC + eo);
+            const float y2 = E[EC + eo + 2], x2 = E[eo + 2];
+            nb0 = ENb{x.x, y.x, z.x, zj.x, xj.x, y.y, x.y, zi.x, yi.x};
+            nb1 = ENb{x.y, y.y, z.y, zj.y, xj.y, y2, x2, zi.y, yi.y};
+            const float2 hx = *reinterpret_cast<const float2*>(H + ho);
+            const float2 hy = *reinterpret_cast<const float2*>(H + HC + ho);
+            const float2 hz = *reinterpret_cast<const float2*>(H + 2 * HC + ho);
+            hx0 = hx.x; hy0 = hy.x; hz0 = hz.x;
+            hx1 = hx.y; hy1 = hy.y; hz1 = hz.y;
+            h_node(a, nb0, hx0, hy0, hz0, q0, ai, in, q0.pml || pml_i, i, jj, kk, own);
+            if (live1) h_node(a, nb1, hx1, hy1, hz1, q1, ai, in, q1.pml || pml_i, i, jj, kk + 1, own);
+            *reinterpret_cast<float2*>(hn + no) = make_float2(hx0, hx1);
+            *reinterpret_cast<float2*>(hn + NC + no) = make_float2(hy0, hy1);
+            *reinterpret_cast<float2*>(hn + 2 * NC + no) = make_float2(hz0, hz1);
+            if (own) {
+                // a dead second column is padding and stays zero
+                float* o = a.h_out + plane + goff;
+                *reinterpret_cast<float2*>(o) = make_float2(hx0, live1 ? hx1 : 0.f);
+                *reinterpret_cast<float2*>(o + g.cs) = make_float2(hy0, live1 ? hy1 : 0.f);
+                *reinterpret_cast<float2*>(o + 2 * g.cs) = make_float2(hz0, live1 ? hz1 : 0.f);
+            }
+        }
+        ENb nx;
+        float hxx = 0.f, hyx = 0.f, hzx = 0.f;
+        if (xtra) {
+            const float* e0 = E + xeo;
+            nx = ENb{e0[0], e0[EC], e0[2 * EC], e0[2 * EC + L::EW], e0[L::EW], e0[EC + 1], e0[1], E1[2 * EC + xeo],
+                     E1[EC + xeo]};
+            hxx = H[xho];
+            hyx = H[HC + xho];
+            hzx = H[2 * HC + xho];
+            const bool xo = xown && !pre;
+            h_node(a, nx, hxx, hyx, hzx, qx, ai, in, qx.pml || pml_i, i, xj, xk, xo);
+            hn[xno] = hxx;
+            hn[NC + xno] = hyx;
+            hn[2 * NC + xno] = hzx;
+            if (xo) {
+                float* o = a.h_out + plane + xgoff;
+                o[0] = hxx;
+                o[g.cs] = hyx;
+                o[2 * g.cs] = hzx;
+            }
+        }
+        if (tma::consumers_sync_or(bad, TMA_CONSUMERS)) {
+            if (tid == 0) atomicExch(a.error, 2);
+            return;
+        }
+
+        // 2. new E on the owned points
+        if (!pre) {
+            if (own_row && live0) {
+                // the pair's two class ids in one aligned load (c is even)
+                unsigned id0, id1;
+                if constexpr (sizeof(CID) == 1) {
+                    const unsigned v = *reinterpret_cast<const uint16_t*>(CL + r * L::CW + c);
+                    id0 = v & 0xffu;
+                    id1 = v >> 8;
+                } else if constexpr (sizeof(CID) == 2) {
+                    const unsigned v = *reinterpret_cast<const uint32_t*>(CL + r * L::CW + c);
+                    id0 = v & 0xffffu;
+                    id1 = v >> 16;
+                } else {
+                    id0 = CL[r * L::CW + c];
+                    id1 = CL[r * L::CW + c + 1];
+                }
+                const CoefRef cf0 = coef_of<LOCAL>(a, lt, id0);
+                const float2 hzj = *reinterpret_cast<const float2*>(hn + 2 * NC + no - L::NW);
+                const float2 hxj = *reinterpret_cast<const float2*>(hn + no - L::NW);
+                const float hyk = hn[NC + no - 1], hxk = hn[no - 1];
+                float ex0 = nb0.x, ey0 = nb0.y, ez0 = nb0.z;
+                e_node(a, cf0, ex0, ey0, ez0, hx0, hy0, hz0, hzj.x, hxj.x, hyk, hxk, py0, pz0, q0, ai, q0.pml || pml_i, i, jj, kk);
+                float ex1 = 0.f, ey1 = 0.f, ez1 = 0.f;
+                if (live1) {
+                    const CoefRef cf1 = coef_of<LOCAL>(a, lt, id1);
+                    ex1 = nb1.x; ey1 = nb1.y; ez1 = nb1.z;
+                    e_node(a, cf1, ex1, ey1, ez1, hx1, hy1, hz1, hzj.y, hxj.y, hy0, hx0, py1, pz1, q1, ai, q1.pml || pml_i, i, jj, kk + 1);
+                }
+                float* o = a.e_out + plane + goff;
+                *reinterpret_cast<float2*>(o) = make_float2(ex0, ex1);
+                *reinterpret_cast<float2*>(o + g.cs) = make_float2(ey0, ey1);
+                *reinterpret_cast<float2*>(o + 2 * g.cs) = make_float2(ez0, ez1);
+            }
+            if (xown) {
+                const CoefRef cf = coef_of<LOCAL>(a, lt, CL[xr * L::CW + xc]);
+                float ex = nx.x, ey = nx.y, ez = nx.z;
+                e_node(a, cf, ex, ey, ez, hxx, hyx, hzx, hn[2 * NC + xno - L::NW], hn[xno - L::NW], hn[NC + xno - 1],
+                       hn[xno - 1], pyx, pzx, qx, ai, qx.pml || pml_i, i, xj, xk);
+                float* o = a.e_out + plane + xgoff;
+                o[0] = ex;
+                o[g.cs] = ey;
+                o[2 * g.cs] = ez;
+            }
+        }
+        py0 = hy0; pz0 = hz0; py1 = hy1; pz1 = hz1; pyx = hyx; pzx = hzx;
+        tma::mbar_arrive(&empty[s]);
+    }
+    // the last plane's stage (E(i1)) was waited on by the final iteration; nothing is in flight
+}
+
+// Host side ---------------------------------------------------------------------------------
+
+struct TmaPlan {
+    CUtensorMap e[2], h[2], c;   // per input parity
+    int tj = 8, tk = 64, seg = 64;
+    int smem = 0;
+    bool ok = false;
+    std::string why;
+};
+
+}  // namespace fg

@@ -229,7 +229,24 @@ def test_the_pipelines_are_the_cuda_kernels(gpu):
     sc = W.dielectric_box(16, pml=3, steps=4)
     sim = fdtd.Sim.try_new(*sc.args())
     s = fdtd.Session(gpu, sim, 0, sc.pulse, sc.extras)
-    assert "fused" in s.variant
+    assert "fused" in s.variant and "TMA" in s.variant, s.variant
     assert s.launches_per_step >= 2
     assert s.stream != 0
     s.close()
+
+
+def test_the_tma_step_and_the_direct_march_agree_bit_for_bit(gpu, monkeypatch):
+    """The TMA-fed fused step and the direct-load fused march do the same arithmetic."""
+    sc = W.spheres(72, pml=6, count=16, rmin=3, rmax=14, steps=120, fused=True)
+    sim = fdtd.Sim.try_new(*sc.args())
+    s = fdtd.Session(gpu, sim, 0, sc.pulse, sc.extras)
+    assert s.variant.startswith("TMA"), s.variant
+    s.close()
+    a = fdtd.run(gpu, sim, 0, sc.pulse, sc.extras, keep_fields=True)
+    monkeypatch.setenv("FIELDGRID_NO_TMA", "1")
+    s = fdtd.Session(gpu, sim, 0, sc.pulse, sc.extras)
+    assert not s.variant.startswith("TMA"), s.variant
+    s.close()
+    b = fdtd.run(gpu, sim, 0, sc.pulse, sc.extras, keep_fields=True)
+    for name in ("e", "h", "series"):
+        assert np.array_equal(getattr(a, name), getattr(b, name)), name

@@ -150,18 +150,56 @@ bool encode(CUtensorMap* m, CUtensorMapDataType dt, void* base, int rank, const 
     auto fn = encode_tiled();
     if (!fn) { why = "cuTensorMapEncodeTiled is unavailable"; return false; }
     cuuint32_t es[5] = {1, 1, 1, 1, 1};
+    CUtensorMapL2promotion promo = CU_TENSOR_MAP_L2_PROMOTION_L2_256B;
+    if (const char* v = std::getenv("FIELDGRID_TMA_L2PROMO")) {
+        const int b = std::atoi(v);
+        promo = b == 0 ? CU_TENSOR_MAP_L2_PROMOTION_NONE
+              : b == 64 ? CU_TENSOR_MAP_L2_PROMOTION_L2_64B
+              : b == 128 ? CU_TENSOR_MAP_L2_PROMOTION_L2_128B : CU_TENSOR_MAP_L2_PROMOTION_L2_256B;
+    }
     CUresult r = fn(m, dt, cuuint32_t(rank), base, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                    CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+                    CU_TENSOR_MAP_SWIZZLE_NONE, promo, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) { why = "cuTensorMapEncodeTiled failed (" + std::to_string(int(r)) + ")"; return false; }
     return true;
 }
 
 constexpr int TMA_TJ = 7, TMA_TK = 64, TMA_STAGES = 3, TMA_SEGMAX = 64;
 
+// Kernel shapes the step can run with: stages of the copy ring and the blocks per SM the register
+// budget is cut for. Shape 0 is the default; the others are tried by the tuner.
+struct TmaShape {
+    int stages, minb;
+};
+constexpr TmaShape TMA_SHAPES[] = {{4, 2}, {3, 3}, {2, 3}};
+constexpr int TMA_NSHAPES = 3;
+
+template <typename CID, bool LOCAL, int ST>
+using TmaLS = TmaLayout<TMA_TJ, TMA_TK, CID, ST, TMA_SEGMAX, LOCAL>;
 template <typename CID, bool LOCAL = false>
-using TmaL = TmaLayout<TMA_TJ, TMA_TK, CID, TMA_STAGES, TMA_SEGMAX, LOCAL>;
-template <typename CID, bool LOCAL = false>
-constexpr auto tma_kernel = k_tma_step<TMA_TJ, TMA_TK, CID, TMA_STAGES, TMA_SEGMAX, LOCAL>;
+using TmaL = TmaLS<CID, LOCAL, TMA_STAGES>;
+template <typename CID, bool LOCAL, int SHAPE>
+constexpr auto tma_kernel_s =
+    k_tma_step<TMA_TJ, TMA_TK, CID, TMA_SHAPES[SHAPE].stages, TMA_SEGMAX, LOCAL, TMA_SHAPES[SHAPE].minb>;
+
+template <typename CID, bool LOCAL, int SHAPE>
+int tma_smem_s() { return TmaLS<CID, LOCAL, TMA_SHAPES[SHAPE].stages>::TOTAL; }
+
+// Calls f(kernel, smem bytes) with the instantiation for (class-id width, local tables, shape).
+template <typename F>
+bool with_tma_kernel(int cid_bytes, bool local, int shape, F&& f) {
+    auto go = [&](auto sh) {
+        constexpr int S = decltype(sh)::value;
+        if (local) return f(tma_kernel_s<uint8_t, true, S>, tma_smem_s<uint8_t, true, S>());
+        if (cid_bytes == 1) return f(tma_kernel_s<uint8_t, false, S>, tma_smem_s<uint8_t, false, S>());
+        if (cid_bytes == 2) return f(tma_kernel_s<uint16_t, false, S>, tma_smem_s<uint16_t, false, S>());
+        return f(tma_kernel_s<uint32_t, false, S>, tma_smem_s<uint32_t, false, S>());
+    };
+    switch (shape) {
+        case 0: return go(std::integral_constant<int, 0>{});
+        case 1: return go(std::integral_constant<int, 1>{});
+        default: return go(std::integral_constant<int, 2>{});
+    }
+}
 
 // tiles along k: a node count of 64t + 1 gives t tiles, the last owning the extra column
 inline int tma_ktiles(int n2) { return (n2 > TMA_TK && n2 % TMA_TK == 1) ? (n2 - 1) / TMA_TK : (n2 + TMA_TK - 1) / TMA_TK; }
@@ -239,6 +277,8 @@ void plan_tma(Session& s) {
     if (g.n2 < 2 || g.n1 < 2) { t.why = "grid too thin"; return; }
     t.tj = TMA_TJ;
     t.tk = TMA_TK;
+    t.shape = 0;
+    if (const char* v = std::getenv("FIELDGRID_TMA_SHAPE")) t.shape = std::min(std::max(std::atoi(v), 0), TMA_NSHAPES - 1);
     const cuuint64_t dims[4] = {cuuint64_t(g.n2), cuuint64_t(g.n1), cuuint64_t(g.n0), 3};
     const cuuint64_t strides[3] = {cuuint64_t(g.p2) * 4, cuuint64_t(g.n1) * g.p2 * 4, cuuint64_t(g.cs) * 4};
     const cuuint32_t box_e[4] = {cuuint32_t(TmaL<float>::EW), cuuint32_t(TmaL<float>::ER), 1, 3};
@@ -256,13 +296,13 @@ void plan_tma(Session& s) {
     const cuuint64_t cstr[2] = {cuuint64_t(g.p2) * b, cuuint64_t(g.n1) * g.p2 * b};
     const cuuint32_t cbox[3] = {cuuint32_t(TmaL<float>::CW), cuuint32_t(TmaL<float>::CR), 1};
     if (!encode(&t.c, dt, s.local ? (void*)s.local_ids : s.node_class, 3, cdims, cstr, cbox, t.why)) return;
-    t.smem = s.local ? TmaL<uint8_t, true>::TOTAL
-                     : (b == 1 ? TmaL<uint8_t>::TOTAL : (b == 2 ? TmaL<uint16_t>::TOTAL : TmaL<uint32_t>::TOTAL));
-    cudaError_t ce;
-    if (s.local) ce = cudaFuncSetAttribute(tma_kernel<uint8_t, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, t.smem);
-    else if (b == 1) ce = cudaFuncSetAttribute(tma_kernel<uint8_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, t.smem);
-    else if (b == 2) ce = cudaFuncSetAttribute(tma_kernel<uint16_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, t.smem);
-    else ce = cudaFuncSetAttribute(tma_kernel<uint32_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, t.smem);
+    cudaError_t ce = cudaSuccess;
+    for (int sh = 0; sh < TMA_NSHAPES && ce == cudaSuccess; ++sh)
+        with_tma_kernel(b, s.local, sh, [&](auto kern, int smem) {
+            ce = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+            if (sh == t.shape) t.smem = smem;
+            return true;
+        });
     if (ce != cudaSuccess) { t.why = std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(ce); return; }
     t.seg = tma_seg(g);
     t.ok = true;
@@ -276,15 +316,10 @@ int launch_tma(Session& s, int parity, float* e_out, float* h_out, const float* 
               (g.n1 + TMA_TJ - 1) / TMA_TJ, s.tables, s.counter, s.error};
     dim3 grd(kt, (g.n1 + TMA_TJ - 1) / TMA_TJ, (g.n0 + t.seg - 1) / t.seg);
     dim3 blk(TMA_CONSUMERS + 32);
-    if (s.local) {
-        tma_kernel<uint8_t, true><<<grd, blk, t.smem, s.stream>>>(t.e[parity], t.h[parity], t.c, a);
-        return cudaPeekAtLastError() == cudaSuccess ? 0 : 1;
-    }
-    switch (s.cid_bytes) {
-        case 1: tma_kernel<uint8_t><<<grd, blk, t.smem, s.stream>>>(t.e[parity], t.h[parity], t.c, a); break;
-        case 2: tma_kernel<uint16_t><<<grd, blk, t.smem, s.stream>>>(t.e[parity], t.h[parity], t.c, a); break;
-        default: tma_kernel<uint32_t><<<grd, blk, t.smem, s.stream>>>(t.e[parity], t.h[parity], t.c, a); break;
-    }
+    with_tma_kernel(s.cid_bytes, s.local, t.shape, [&](auto kern, int smem) {
+        kern<<<grd, blk, smem, s.stream>>>(t.e[parity], t.h[parity], t.c, a);
+        return true;
+    });
     return cudaPeekAtLastError() == cudaSuccess ? 0 : 1;
 }
 
@@ -752,7 +787,9 @@ int session_new(Gpu* gpu, const HostSim& sim, const RunSpec& rs, Session** out, 
     plan_tma(*s);
     if (s->tma.ok)
         s->variant = "TMA fused march, tile " + std::to_string(s->tma.tj) + "x" + std::to_string(s->tma.tk) + ", " +
-                     std::to_string(s->tma.seg) + " planes per block, " + std::to_string(TMA_STAGES) + " stages, " +
+                     std::to_string(s->tma.seg) + " planes per block, " +
+                     std::to_string(TMA_SHAPES[s->tma.shape].stages) + " stages, " +
+                     std::to_string(TMA_SHAPES[s->tma.shape].minb) + " blocks/SM, " +
                      (s->local ? "per-block class tables" : "global class table");
     else
         s->variant = s->fused ? fused_name(s->shape) + " (" + s->tma.why + ")" : std::string("separate H+E, 64x4 threads");

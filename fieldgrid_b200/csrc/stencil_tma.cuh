@@ -206,43 +206,126 @@ struct PtAxes {           // the axis factors of one point
     bool jn, kn, pml;     // j+1 / k+1 inside the grid; j or k inside the absorbing layer
 };
 
-// New H at one point (the update of cpu.rs:48-107); `pml` selects the CPML form.
-__device__ __forceinline__ void h_node(const TmaArgs& a, const ENb& n, float& hx, float& hy, float& hz,
-                                       const PtAxes& q, const AxisNode& ai, bool in, bool pml, int i, int j, int k,
-                                       bool own) {
-    if (!pml) {
-        const float idj = q.aj->inv_d, idk = q.ak->inv_d, idi = ai.inv_d;
-        if (q.jn && q.kn) hx = hx - a.k_mu * ((n.z_jp - n.z) * idj - (n.y_kp - n.y) * idk);
-        if (q.kn && in) hy = hy - a.k_mu * ((n.x_kp - n.x) * idk - (n.z_ip - n.z) * idi);
-        if (in && q.jn) hz = hz - a.k_mu * ((n.y_ip - n.y) * idi - (n.x_jp - n.x) * idj);
-    } else {
-        const AxisNode aj = *q.aj, ak = *q.ak;
-        if (q.jn && q.kn) hx = h_point<0>(a, hx, n.z_jp - n.z, n.y_kp - n.y, aj, ak, i, j, k, own);
-        if (q.kn && in) hy = h_point<1>(a, hy, n.x_kp - n.x, n.z_ip - n.z, ak, ai, i, j, k, own);
-        if (in && q.jn) hz = h_point<2>(a, hz, n.y_ip - n.y, n.x_jp - n.x, ai, aj, i, j, k, own);
-    }
+// The plane-dependent parts of the psi offsets (psi_idx, sim.rs:659-665) at plane i: the x slab
+// (slot*n1 + j)*n2 + k splits into slot*n1*n2 + (j*n2 + k), the y slab (i*2pml + slot)*n2 + k
+// into i*2pml*n2 + (slot*n2 + k), the z slab (i*n1 + j)*2pml + slot into i*n1*2pml + (j*2pml +
+// slot); the bracketed parts are 32-bit and formed per point.
+struct PsiPlane {
+    long long bie, bih, bj, bk;
+};
+
+__device__ __forceinline__ PsiPlane psi_plane(const Geom& g, int i, const AxisNode& ai) {
+    const long long w = 2 * g.pml, nn12 = (long long)g.n1 * g.n2;
+    return PsiPlane{(long long)ai.slot_e * nn12, (long long)ai.slot_h * nn12, (long long)i * w * g.n2,
+                    (long long)i * g.n1 * w};
 }
 
-// New E at one owned point; h*_jm / h*_km are the new H at j-1 / k-1, py / pz the H of plane i-1.
+// Offset inside slab (field F: 0 = E, 1 = H; derivative axis A) of point (j, k) whose slot along
+// A is `slot`.
+template <int F>
+__device__ __forceinline__ long long psi_off_of(const Geom& g, const PsiPlane& b, int A, int j, int k, int slot) {
+    if (A == 0) return (F ? b.bih : b.bie) + (j * g.n2 + k);
+    if (A == 1) return b.bj + (slot * g.n2 + k);
+    return b.bk + (j * 2 * g.pml + slot);
+}
+
 struct CoefRef {          // three ca then three cb
     float ca[3], cb[3];
 };
 
+// New H at one point (the update of cpu.rs:48-107). Every lane runs the same arithmetic; a
+// point inside the CPML (`pml`) additionally gathers its psi entries, updates them and adds them
+// to t1/t2 where the reference does, so only that block diverges.
+__device__ __forceinline__ void h_node(const TmaArgs& a, const ENb& n, float& hx, float& hy, float& hz,
+                                       const PtAxes& q, const AxisNode& ai, const PsiPlane& pp, bool in, bool pml,
+                                       int i, int j, int k, bool own) {
+    const AxisNode* ax[3] = {&ai, q.aj, q.ak};            // by axis 0 (i), 1 (j), 2 (k)
+    const float d[3][2] = {{n.z_jp - n.z, n.y_kp - n.y}, {n.x_kp - n.x, n.z_ip - n.z}, {n.y_ip - n.y, n.x_jp - n.x}};
+    const bool run[3] = {q.jn && q.kn, q.kn && in, in && q.jn};
+    float t[3][2];
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+        for (int u = 0; u < 2; ++u) t[c][u] = d[c][u] * ax[(c + 1 + u) % 3]->inv_d;
+    if (pml) {
+        const Geom& g = a.g;
+        long long qi[3][2];
+        float pv[3][2];
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+#pragma unroll
+            for (int u = 0; u < 2; ++u) {
+                const int A = (c + 1 + u) % 3;
+                const int sl = ax[A]->slot_h;
+                qi[c][u] = sl >= 0 ? g.psi_off[9 + c * 3 + A] + psi_off_of<1>(g, pp, A, j, k, sl) : 0;
+            }
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+#pragma unroll
+            for (int u = 0; u < 2; ++u) pv[c][u] = a.psi_h_in[qi[c][u]];
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+#pragma unroll
+            for (int u = 0; u < 2; ++u) {
+                const AxisNode& an = *ax[(c + 1 + u) % 3];
+                if (run[c] && an.slot_h >= 0) {
+                    const float r = an.bh * pv[c][u] + an.ch * d[c][u] * an.raw_inv_d;
+                    if (own) a.psi_h_out[qi[c][u]] = r;
+                    t[c][u] += r;
+                }
+            }
+    }
+    if (run[0]) hx = hx - a.k_mu * (t[0][0] - t[0][1]);
+    if (run[1]) hy = hy - a.k_mu * (t[1][0] - t[1][1]);
+    if (run[2]) hz = hz - a.k_mu * (t[2][0] - t[2][1]);
+}
+
+// New E at one owned point (cpu.rs:109-167); h*_jm / h*_km are the new H at j-1 / k-1, py / pz
+// the H of plane i-1. Same structure as h_node: the psi block is the only divergent part.
 __device__ __forceinline__ void e_node(const TmaArgs& a, const CoefRef& cf, float& ex, float& ey, float& ez,
                                        float hx, float hy, float hz, float hz_jm, float hx_jm, float hy_km,
-                                       float hx_km, float py, float pz, const PtAxes& q, const AxisNode& ai, bool pml,
-                                       int i, int j, int k) {
-    if (!pml) {
-        const float iddj = q.aj->inv_dd, iddk = q.ak->inv_dd, iddi = ai.inv_dd;
-        if (cf.cb[0] != 0.0f && j > 0 && k > 0) ex = cf.ca[0] * ex + cf.cb[0] * ((hz - hz_jm) * iddj - (hy - hy_km) * iddk);
-        if (cf.cb[1] != 0.0f && k > 0 && i > 0) ey = cf.ca[1] * ey + cf.cb[1] * ((hx - hx_km) * iddk - (hz - pz) * iddi);
-        if (cf.cb[2] != 0.0f && i > 0 && j > 0) ez = cf.ca[2] * ez + cf.cb[2] * ((hy - py) * iddi - (hx - hx_jm) * iddj);
-    } else {
-        const AxisNode aj = *q.aj, ak = *q.ak;
-        if (cf.cb[0] != 0.0f && j > 0 && k > 0) ex = e_point<0>(a, ex, cf.ca[0], cf.cb[0], hz - hz_jm, hy - hy_km, aj, ak, i, j, k);
-        if (cf.cb[1] != 0.0f && k > 0 && i > 0) ey = e_point<1>(a, ey, cf.ca[1], cf.cb[1], hx - hx_km, hz - pz, ak, ai, i, j, k);
-        if (cf.cb[2] != 0.0f && i > 0 && j > 0) ez = e_point<2>(a, ez, cf.ca[2], cf.cb[2], hy - py, hx - hx_jm, ai, aj, i, j, k);
+                                       float hx_km, float py, float pz, const PtAxes& q, const AxisNode& ai,
+                                       const PsiPlane& pp, bool pml, int i, int j, int k) {
+    const AxisNode* ax[3] = {&ai, q.aj, q.ak};
+    const float d[3][2] = {{hz - hz_jm, hy - hy_km}, {hx - hx_km, hz - pz}, {hy - py, hx - hx_jm}};
+    const bool run[3] = {cf.cb[0] != 0.0f && j > 0 && k > 0, cf.cb[1] != 0.0f && k > 0 && i > 0,
+                         cf.cb[2] != 0.0f && i > 0 && j > 0};
+    float t[3][2];
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+        for (int u = 0; u < 2; ++u) t[c][u] = d[c][u] * ax[(c + 1 + u) % 3]->inv_dd;
+    if (pml) {
+        const Geom& g = a.g;
+        long long qi[3][2];
+        float pv[3][2];
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+#pragma unroll
+            for (int u = 0; u < 2; ++u) {
+                const int A = (c + 1 + u) % 3;
+                const int sl = ax[A]->slot_e;
+                qi[c][u] = (sl >= 0 && run[c]) ? g.psi_off[c * 3 + A] + psi_off_of<0>(g, pp, A, j, k, sl) : 0;
+            }
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+#pragma unroll
+            for (int u = 0; u < 2; ++u) pv[c][u] = a.psi_e[qi[c][u]];
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+#pragma unroll
+            for (int u = 0; u < 2; ++u) {
+                const AxisNode& an = *ax[(c + 1 + u) % 3];
+                if (run[c] && an.slot_e >= 0) {
+                    const float r = an.be * pv[c][u] + an.ce * d[c][u] * an.raw_inv_dd;
+                    a.psi_e[qi[c][u]] = r;
+                    t[c][u] += r;
+                }
+            }
     }
+    if (run[0]) ex = cf.ca[0] * ex + cf.cb[0] * (t[0][0] - t[0][1]);
+    if (run[1]) ey = cf.ca[1] * ey + cf.cb[1] * (t[1][0] - t[1][1]);
+    if (run[2]) ez = cf.ca[2] * ez + cf.cb[2] * (t[2][0] - t[2][1]);
 }
 
 constexpr int TMA_CONSUMERS = 256;
@@ -267,8 +350,8 @@ __device__ __forceinline__ CoefRef coef_of(const TmaArgs& a, const float* lt, un
     return c;
 }
 
-template <int TJ, int TK, typename CID, int STAGES, int SEGMAX, bool LOCAL>
-__global__ void __launch_bounds__(TMA_CONSUMERS + 32, 3)
+template <int TJ, int TK, typename CID, int STAGES, int SEGMAX, bool LOCAL, int MINB>
+__global__ void __launch_bounds__(TMA_CONSUMERS + 32, MINB)
     k_tma_step(const __grid_constant__ CUtensorMap map_e, const __grid_constant__ CUtensorMap map_h,
                const __grid_constant__ CUtensorMap map_c, TmaArgs a) {
     static_assert(TJ + 1 == TMA_CONSUMERS / 32 && TK == 64, "one warp per row, one column pair per lane");
@@ -387,6 +470,7 @@ __global__ void __launch_bounds__(TMA_CONSUMERS + 32, 3)
         const bool in = i + 1 < g.n0;
         const long long plane = (long long)i * g.n1 * g.p2;
         const bool own = own_row && !pre;
+        const PsiPlane pp = psi_plane(g, i, ai);
 
         // 1. new H: the pair (two columns), and warp 0's extra point
         ENb nb0, nb1;
@@ -407,8 +491,8 @@ __global__ void __launch_bounds__(TMA_CONSUMERS + 32, 3)
             const float2 hz = *reinterpret_cast<const float2*>(H + 2 * HC + ho);
             hx0 = hx.x; hy0 = hy.x; hz0 = hz.x;
             hx1 = hx.y; hy1 = hy.y; hz1 = hz.y;
-            h_node(a, nb0, hx0, hy0, hz0, q0, ai, in, q0.pml || pml_i, i, jj, kk, own);
-            if (live1) h_node(a, nb1, hx1, hy1, hz1, q1, ai, in, q1.pml || pml_i, i, jj, kk + 1, own);
+            h_node(a, nb0, hx0, hy0, hz0, q0, ai, pp, in, q0.pml || pml_i, i, jj, kk, own);
+            if (live1) h_node(a, nb1, hx1, hy1, hz1, q1, ai, pp, in, q1.pml || pml_i, i, jj, kk + 1, own);
             *reinterpret_cast<float2*>(hn + no) = make_float2(hx0, hx1);
             *reinterpret_cast<float2*>(hn + NC + no) = make_float2(hy0, hy1);
             *reinterpret_cast<float2*>(hn + 2 * NC + no) = make_float2(hz0, hz1);
@@ -430,7 +514,7 @@ __global__ void __launch_bounds__(TMA_CONSUMERS + 32, 3)
             hyx = H[HC + xho];
             hzx = H[2 * HC + xho];
             const bool xo = xown && !pre;
-            h_node(a, nx, hxx, hyx, hzx, qx, ai, in, qx.pml || pml_i, i, xj, xk, xo);
+            h_node(a, nx, hxx, hyx, hzx, qx, ai, pp, in, qx.pml || pml_i, i, xj, xk, xo);
             hn[xno] = hxx;
             hn[NC + xno] = hyx;
             hn[2 * NC + xno] = hzx;
@@ -468,12 +552,12 @@ __global__ void __launch_bounds__(TMA_CONSUMERS + 32, 3)
                 const float2 hxj = *reinterpret_cast<const float2*>(hn + no - L::NW);
                 const float hyk = hn[NC + no - 1], hxk = hn[no - 1];
                 float ex0 = nb0.x, ey0 = nb0.y, ez0 = nb0.z;
-                e_node(a, cf0, ex0, ey0, ez0, hx0, hy0, hz0, hzj.x, hxj.x, hyk, hxk, py0, pz0, q0, ai, q0.pml || pml_i, i, jj, kk);
+                e_node(a, cf0, ex0, ey0, ez0, hx0, hy0, hz0, hzj.x, hxj.x, hyk, hxk, py0, pz0, q0, ai, pp, q0.pml || pml_i, i, jj, kk);
                 float ex1 = 0.f, ey1 = 0.f, ez1 = 0.f;
                 if (live1) {
                     const CoefRef cf1 = coef_of<LOCAL>(a, lt, id1);
                     ex1 = nb1.x; ey1 = nb1.y; ez1 = nb1.z;
-                    e_node(a, cf1, ex1, ey1, ez1, hx1, hy1, hz1, hzj.y, hxj.y, hy0, hx0, py1, pz1, q1, ai, q1.pml || pml_i, i, jj, kk + 1);
+                    e_node(a, cf1, ex1, ey1, ez1, hx1, hy1, hz1, hzj.y, hxj.y, hy0, hx0, py1, pz1, q1, ai, pp, q1.pml || pml_i, i, jj, kk + 1);
                 }
                 float* o = a.e_out + plane + goff;
                 *reinterpret_cast<float2*>(o) = make_float2(ex0, ex1);
@@ -484,7 +568,7 @@ __global__ void __launch_bounds__(TMA_CONSUMERS + 32, 3)
                 const CoefRef cf = coef_of<LOCAL>(a, lt, CL[xr * L::CW + xc]);
                 float ex = nx.x, ey = nx.y, ez = nx.z;
                 e_node(a, cf, ex, ey, ez, hxx, hyx, hzx, hn[2 * NC + xno - L::NW], hn[xno - L::NW], hn[NC + xno - 1],
-                       hn[xno - 1], pyx, pzx, qx, ai, qx.pml || pml_i, i, xj, xk);
+                       hn[xno - 1], pyx, pzx, qx, ai, pp, qx.pml || pml_i, i, xj, xk);
                 float* o = a.e_out + plane + xgoff;
                 o[0] = ex;
                 o[g.cs] = ey;
@@ -502,6 +586,7 @@ __global__ void __launch_bounds__(TMA_CONSUMERS + 32, 3)
 struct TmaPlan {
     CUtensorMap e[2], h[2], c;   // per input parity
     int tj = 8, tk = 64, seg = 64;
+    int shape = 0;               // index into the engine's kernel shapes
     int smem = 0;
     bool ok = false;
     std::string why;

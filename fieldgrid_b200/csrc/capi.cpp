@@ -48,6 +48,11 @@ struct Far {
 
 }  // namespace
 
+namespace fg {
+// lets other translation units of the library report through fg_last_error
+void set_last_error(const std::string& msg) { g_last_error = msg; }
+}  // namespace fg
+
 struct fg_gpu { Gpu* g; };
 struct fg_sim { HostSim* s; };
 struct fg_session { Session* s; };

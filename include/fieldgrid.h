@@ -223,6 +223,24 @@ int fg_session_kernel_times(fg_session* s, uint64_t steps, char* names, double* 
 const char* fg_session_variant(const fg_session* s);
 void fg_session_free(fg_session* s);
 
+/* ---- field energy without device allocation --------------------------------------------
+ * No counterpart in the reference. For callers that cannot allocate device memory when they need
+ * the energy of a field (e.g. an operator callback running while a host framework's caching
+ * allocator owns the device memory, or a loop that must avoid the device-wide synchronisation of
+ * cudaMalloc/cudaFree): sum over q < n of e[q]^2 + (376.73 h[q])^2 in f64 (the quantity of
+ * cpu.rs:417-421), written to *out. e, h and out are device pointers owned by the caller; the
+ * call allocates nothing. Its per-block partial sums live in one fixed array of
+ * FG_ENERGY_NOALLOC_MAX_BLOCKS doubles (32 KB) per device, held from the library's load until
+ * process exit; each block covers FG_ENERGY_NOALLOC_CHUNK elements, so n is limited to
+ * FG_ENERGY_NOALLOC_MAX_BLOCKS * FG_ENERGY_NOALLOC_CHUNK (2^32) and larger n is refused with
+ * FG_ERR_INVALID. The first call on a device looks up that array's device address (make it before
+ * any stream capture). Every call uses the same array: calls that overlap on the GPU (different
+ * streams, or host threads on one device) race; calls ordered on one stream are safe. Work is
+ * enqueued on `stream` (NULL = the default stream); read *out after that stream is synchronised. */
+#define FG_ENERGY_NOALLOC_MAX_BLOCKS 4096
+#define FG_ENERGY_NOALLOC_CHUNK (1u << 20)
+int fg_energy_noalloc(const float* e, const float* h, uint64_t n, double* out, void* stream);
+
 /* ---- near-to-far field (ntff.rs) -------------------------------------------------------- */
 /* patches(sim, inset).gpu (ntff.rs:11-59): 13 u32 per patch. Call with dst == NULL to get the
  * count of patches in *count, then again with a buffer of 13*count u32 (and pos/area of

@@ -96,13 +96,14 @@ struct Session {
     int* error = nullptr;           // set by a kernel whose bounded wait ran out
     TmaPlan tma;                    // the TMA-fed fused step, when it applies
     uint8_t* local_ids = nullptr;   // per node: index into its block region's coefficient table
+    int4* tma_blocks = nullptr;     // the TMA step's blocks: clean ones first, then the layer ones
     float* tables = nullptr;        // per block region: LOCAL_CLASSES x (ca[3], cb[3])
     bool local = false;
     // counts
     int n_sources = 0, n_inductors = 0, n_ports = 0, n_wires = 0, n_sheets = 0, n_debye = 0, n_patches = 0;
     int plane_k = 0;
     uint64_t plane_len = 0, ntff_len = 0, series_len = 0;
-    long long psi_total = 0;
+    long long psi_total = 0, psi_hbase = 0;
     double t0 = 0, tau = 0;
     uint64_t steps = 0;
     uint64_t launches = 0;
@@ -173,32 +174,37 @@ struct TmaShape {
 constexpr TmaShape TMA_SHAPES[] = {{4, 2}, {3, 3}, {2, 3}};
 constexpr int TMA_NSHAPES = 3;
 
-template <typename CID, bool LOCAL, int ST>
-using TmaLS = TmaLayout<TMA_TJ, TMA_TK, CID, ST, TMA_SEGMAX, LOCAL>;
+template <typename CID, bool LOCAL, int ST, bool PML = true>
+using TmaLS = TmaLayout<TMA_TJ, TMA_TK, CID, ST, TMA_SEGMAX, LOCAL, PML>;
 template <typename CID, bool LOCAL = false>
 using TmaL = TmaLS<CID, LOCAL, TMA_STAGES>;
-template <typename CID, bool LOCAL, int SHAPE>
+template <typename CID, bool LOCAL, int SHAPE, bool PML>
 constexpr auto tma_kernel_s =
-    k_tma_step<TMA_TJ, TMA_TK, CID, TMA_SHAPES[SHAPE].stages, TMA_SEGMAX, LOCAL, TMA_SHAPES[SHAPE].minb>;
+    k_tma_step<TMA_TJ, TMA_TK, CID, TMA_SHAPES[SHAPE].stages, TMA_SEGMAX, LOCAL, TMA_SHAPES[SHAPE].minb, PML>;
 
-template <typename CID, bool LOCAL, int SHAPE>
-int tma_smem_s() { return TmaLS<CID, LOCAL, TMA_SHAPES[SHAPE].stages>::TOTAL; }
+template <typename CID, bool LOCAL, int SHAPE, bool PML>
+int tma_smem_s() { return TmaLS<CID, LOCAL, TMA_SHAPES[SHAPE].stages, PML>::TOTAL; }
 
-// Calls f(kernel, smem bytes) with the instantiation for (class-id width, local tables, shape).
+// Calls f(kernel, smem bytes) with the instantiation for (class-id width, local tables, shape,
+// clean or layer blocks).
 template <typename F>
-bool with_tma_kernel(int cid_bytes, bool local, int shape, F&& f) {
-    auto go = [&](auto sh) {
+bool with_tma_kernel(int cid_bytes, bool local, int shape, bool pml, F&& f) {
+    auto go = [&](auto sh, auto pm) {
         constexpr int S = decltype(sh)::value;
-        if (local) return f(tma_kernel_s<uint8_t, true, S>, tma_smem_s<uint8_t, true, S>());
-        if (cid_bytes == 1) return f(tma_kernel_s<uint8_t, false, S>, tma_smem_s<uint8_t, false, S>());
-        if (cid_bytes == 2) return f(tma_kernel_s<uint16_t, false, S>, tma_smem_s<uint16_t, false, S>());
-        return f(tma_kernel_s<uint32_t, false, S>, tma_smem_s<uint32_t, false, S>());
+        constexpr bool P = decltype(pm)::value;
+        if (local) return f(tma_kernel_s<uint8_t, true, S, P>, tma_smem_s<uint8_t, true, S, P>());
+        if (cid_bytes == 1) return f(tma_kernel_s<uint8_t, false, S, P>, tma_smem_s<uint8_t, false, S, P>());
+        if (cid_bytes == 2) return f(tma_kernel_s<uint16_t, false, S, P>, tma_smem_s<uint16_t, false, S, P>());
+        return f(tma_kernel_s<uint32_t, false, S, P>, tma_smem_s<uint32_t, false, S, P>());
     };
-    switch (shape) {
-        case 0: return go(std::integral_constant<int, 0>{});
-        case 1: return go(std::integral_constant<int, 1>{});
-        default: return go(std::integral_constant<int, 2>{});
-    }
+    auto by_shape = [&](auto pm) {
+        switch (shape) {
+            case 0: return go(std::integral_constant<int, 0>{}, pm);
+            case 1: return go(std::integral_constant<int, 1>{}, pm);
+            default: return go(std::integral_constant<int, 2>{}, pm);
+        }
+    };
+    return pml ? by_shape(std::true_type{}) : by_shape(std::false_type{});
 }
 
 // tiles along k: a node count of 64t + 1 gives t tiles, the last owning the extra column
@@ -212,7 +218,71 @@ int tma_seg(const Geom& g) {
     return seg;
 }
 
-// Per block region of the TMA step (a TJ x TK tile over one x-segment): the distinct node classes
+// The blocks of the TMA step, (k0, j0, i0, i1) each: a TJ x TK tile over one x-segment. The x
+// range is cut where the CPML begins, so that "clean" blocks (listed first) have no plane, row or
+// column with a live psi slot anywhere in their tile, halo row, halo column or halo plane; they
+// run the kernel without psi code. The rest run the layer kernel.
+struct TmaBlocks {
+    std::vector<int4> list;
+    int clean = 0;
+    int seg = 0;     // planes per clean block (at most)
+};
+
+TmaBlocks plan_tma_blocks(const HostSim& sim, const Geom& g) {
+    auto hot = [&](int a, int i) {
+        const AxisNode& n = sim.ax[a].node[size_t(i)];
+        return n.slot_e >= 0 || n.slot_h >= 0;
+    };
+    // x: clean planes [xa, xb), chosen so no plane of [xa - 1, xb) is hot
+    int lead = 0;
+    while (lead < g.n0 && hot(0, lead)) ++lead;
+    int trail = g.n0;
+    while (trail > lead && hot(0, trail - 1)) --trail;
+    int xa = lead > 0 ? lead + 1 : 0, xb = trail;
+    bool inner = xa < xb;
+    for (int p = std::max(xa - 1, 0); inner && p < xb; ++p) inner = !hot(0, p);
+    TmaBlocks out;
+    out.seg = tma_seg(g);
+    std::vector<int2> segs;
+    std::vector<char> seg_clean;
+    auto chunk = [&](int lo, int hi, int len, bool clean) {
+        if (hi <= lo) return;
+        const int n = (hi - lo + len - 1) / len;
+        for (int q = 0; q < n; ++q) {
+            segs.push_back(make_int2(lo + int((long long)(hi - lo) * q / n), lo + int((long long)(hi - lo) * (q + 1) / n)));
+            seg_clean.push_back(clean);
+        }
+    };
+    if (inner) {
+        chunk(0, xa, TMA_SEGMAX, false);
+        chunk(xa, xb, out.seg, true);
+        chunk(xb, g.n0, TMA_SEGMAX, false);
+    } else {
+        chunk(0, g.n0, out.seg, false);
+    }
+    // tiles: clean when no row of j0-1 .. j0+TJ-1 and no column of k0-1 .. k0+TK is hot
+    const int kt = tma_ktiles(g.n2), jt = (g.n1 + TMA_TJ - 1) / TMA_TJ;
+    std::vector<char> kcl(size_t(kt), 1), jcl(size_t(jt), 1);
+    for (int bx = 0; bx < kt; ++bx)
+        for (int k = std::max(bx * TMA_TK - 1, 0); k <= std::min(bx * TMA_TK + TMA_TK, g.n2 - 1); ++k)
+            if (hot(2, k)) kcl[size_t(bx)] = 0;
+    for (int by = 0; by < jt; ++by)
+        for (int j = std::max(by * TMA_TJ - 1, 0); j <= std::min(by * TMA_TJ + TMA_TJ - 1, g.n1 - 1); ++j)
+            if (hot(1, j)) jcl[size_t(by)] = 0;
+    std::vector<int4> layer;
+    for (size_t q = 0; q < segs.size(); ++q)
+        for (int by = 0; by < jt; ++by)
+            for (int bx = 0; bx < kt; ++bx) {
+                const int4 b = make_int4(bx * TMA_TK, by * TMA_TJ, segs[q].x, segs[q].y);
+                if (seg_clean[q] && jcl[size_t(by)] && kcl[size_t(bx)]) out.list.push_back(b);
+                else layer.push_back(b);
+            }
+    out.clean = int(out.list.size());
+    out.list.insert(out.list.end(), layer.begin(), layer.end());
+    return out;
+}
+
+// Per block of the TMA step (a TJ x TK tile over one x-segment): the distinct node classes
 // it holds, renumbered from 0, and each node's index into that short list. ok = false when a
 // region holds more than LOCAL_CLASSES classes.
 struct LocalClasses {
@@ -221,10 +291,9 @@ struct LocalClasses {
     bool ok = true;
 };
 
-LocalClasses build_local(const HostSim& sim, const Geom& g, int seg) {
+LocalClasses build_local(const HostSim& sim, const Geom& g, const std::vector<int4>& blocks) {
     LocalClasses out;
-    const int kt = tma_ktiles(g.n2), jt = (g.n1 + TMA_TJ - 1) / TMA_TJ, st = (g.n0 + seg - 1) / seg;
-    const long long regions = (long long)kt * jt * st;
+    const long long regions = (long long)blocks.size();
     out.ids.assign(size_t(g.n0) * g.n1 * g.p2, 0);
     out.tables.assign(size_t(regions) * LOCAL_CLASSES * 6, 0.f);
     bool over = false;
@@ -232,10 +301,10 @@ LocalClasses build_local(const HostSim& sim, const Geom& g, int seg) {
 #pragma omp parallel for schedule(dynamic, 8) reduction(|| : over)
     for (long long r = 0; r < regions; ++r) {
         if (over) continue;
-        const int bx = int(r % kt), by = int((r / kt) % jt), bz = int(r / ((long long)kt * jt));
-        const int k0 = bx * TMA_TK, j0 = by * TMA_TJ, i0 = bz * seg, i1 = std::min(i0 + seg, g.n0);
+        const int4 b = blocks[size_t(r)];
+        const int k0 = b.x, j0 = b.y, i0 = b.z, i1 = b.w;
         int kend = std::min(k0 + TMA_TK, g.n2);
-        if (bx == kt - 1 && k0 + TMA_TK == g.n2 - 1) kend = g.n2;  // the owned right-edge column
+        if (k0 + TMA_TK == g.n2 - 1) kend = g.n2;  // the owned right-edge column
         const int jend = std::min(j0 + TMA_TJ, g.n1);
         uint32_t keys[512];
         uint16_t vals[512];
@@ -296,30 +365,55 @@ void plan_tma(Session& s) {
     const cuuint64_t cstr[2] = {cuuint64_t(g.p2) * b, cuuint64_t(g.n1) * g.p2 * b};
     const cuuint32_t cbox[3] = {cuuint32_t(TmaL<float>::CW), cuuint32_t(TmaL<float>::CR), 1};
     if (!encode(&t.c, dt, s.local ? (void*)s.local_ids : s.node_class, 3, cdims, cstr, cbox, t.why)) return;
+    // z-slab psi: (slot, j, i, component) over each field's two adjacent z slabs
+    t.pz = g.pml > 0 && g.pw <= TmaL<float>::PZW;
+    if (t.pz) {
+        const long long zlen = g.psi_off[1 * 3 + 2] - g.psi_off[0 * 3 + 2];  // slab stride, 128-byte multiple
+        const cuuint64_t zd[4] = {cuuint64_t(g.pw), cuuint64_t(g.n1), cuuint64_t(g.n0), 2};
+        const cuuint64_t zs[3] = {cuuint64_t(g.pw) * 4, cuuint64_t(g.n1) * g.pw * 4, cuuint64_t(zlen) * 4};
+        const cuuint32_t zb[4] = {cuuint32_t(g.pw), cuuint32_t(TMA_TJ + 1), 1, 2};
+        if (!encode(&t.pze, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, s.psi + g.psi_off[0 * 3 + 2], 4, zd, zs, zb, t.why)) return;
+        float* hsets[2] = {s.psi, s.psi_h2};  // the H slabs read by a step whose input set is 0 / 1
+        for (int q = 0; q < 2; ++q)
+            if (!encode(&t.pzh[q], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, hsets[q] + g.psi_off[9 + 0 * 3 + 2], 4, zd, zs, zb,
+                        t.why))
+                return;
+    }
     cudaError_t ce = cudaSuccess;
     for (int sh = 0; sh < TMA_NSHAPES && ce == cudaSuccess; ++sh)
-        with_tma_kernel(b, s.local, sh, [&](auto kern, int smem) {
-            ce = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-            if (sh == t.shape) t.smem = smem;
-            return true;
-        });
+        for (int pm = 0; pm < 2 && ce == cudaSuccess; ++pm)
+            with_tma_kernel(b, s.local, sh, pm != 0, [&](auto kern, int smem) {
+                ce = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+                if (sh == t.shape) t.smem = std::max(t.smem, smem);
+                return true;
+            });
     if (ce != cudaSuccess) { t.why = std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(ce); return; }
-    t.seg = tma_seg(g);
+    if (!s.tma_blocks) { t.why = "no block list"; return; }
     t.ok = true;
 }
 
 int launch_tma(Session& s, int parity, float* e_out, float* h_out, const float* psi_h_in, float* psi_h_out) {
     const Geom& g = s.geom;
     const TmaPlan& t = s.tma;
-    const int kt = tma_ktiles(g.n2);
-    TmaArgs a{g, s.classes, e_out, h_out, s.psi, psi_h_in, psi_h_out, s.sc.k_mu, t.seg, kt,
-              (g.n1 + TMA_TJ - 1) / TMA_TJ, s.tables, s.counter, s.error};
-    dim3 grd(kt, (g.n1 + TMA_TJ - 1) / TMA_TJ, (g.n0 + t.seg - 1) / t.seg);
-    dim3 blk(TMA_CONSUMERS + 32);
-    with_tma_kernel(s.cid_bytes, s.local, t.shape, [&](auto kern, int smem) {
-        kern<<<grd, blk, smem, s.stream>>>(t.e[parity], t.h[parity], t.c, a);
-        return true;
-    });
+    TmaArgs a{g, s.classes, e_out, h_out, s.psi, psi_h_in, psi_h_out, s.sc.k_mu, int(t.pz), s.tma_blocks, 0, 1,
+              s.tables, s.counter, s.error};
+    const dim3 blk(TMA_CONSUMERS + 32);
+    // the clean blocks, then the layer blocks (without staged z boxes the last two maps are never read)
+    const CUtensorMap& pze = t.pz ? t.pze : t.c;
+    const CUtensorMap& pzh = t.pz ? t.pzh[parity] : t.c;
+    if (t.n_clean > 0)
+        with_tma_kernel(s.cid_bytes, s.local, t.shape, false, [&](auto kern, int smem) {
+            kern<<<unsigned(t.n_clean), blk, smem, s.stream>>>(t.e[parity], t.h[parity], t.c, pze, pzh, a);
+            return true;
+        });
+    if (t.n_layer > 0) {
+        a.block0 = t.n_clean;
+        a.bump = t.n_clean == 0;
+        with_tma_kernel(s.cid_bytes, s.local, t.shape, true, [&](auto kern, int smem) {
+            kern<<<unsigned(t.n_layer), blk, smem, s.stream>>>(t.e[parity], t.h[parity], t.c, pze, pzh, a);
+            return true;
+        });
+    }
     return cudaPeekAtLastError() == cudaSuccess ? 0 : 1;
 }
 
@@ -399,6 +493,7 @@ int enqueue_step(Session& s, int parity, std::string& err) {
 
 uint64_t count_launches(const Session& s) {
     uint64_t n = 1;  // the field update (fused) or H update (separate)
+    if (s.tma.ok && s.tma.n_clean > 0 && s.tma.n_layer > 0) n++;  // clean and layer blocks of the TMA step
     if (!s.fused) n += 1 + (s.n_debye ? 1 : 0);
     if (s.n_wires) n++;
     if (s.n_sheets) n += 2;
@@ -448,20 +543,27 @@ int session_new(Gpu* gpu, const HostSim& sim, const RunSpec& rs, Session** out, 
     auto dev = [&](uint64_t id) { return (long long)(id / n2) * g.p2 + (long long)(id % n2); };
     auto fidx = [&](uint64_t key) { return (long long)(key / nn) * cs + dev(key % nn); };
 
-    // psi slabs (run.rs:214-225)
-    long long psi_total = 0;
-    for (int e = 0; e < 2; ++e)
-        for (int c = 0; c < 3; ++c)
-            for (int a = 0; a < 3; ++a) {
-                g.psi_off[e * 9 + c * 3 + a] = psi_total;
-                if (a != c && sim.pml > 0) {
-                    size_t m[3] = {n0, n1, n2};
-                    m[a] = 2 * sim.pml;
-                    psi_total += (long long)(m[0] * m[1] * m[2]);
-                }
+    // psi slabs (run.rs:214-225): the 12 (field, component, axis) slabs of the reference, E
+    // first, then H; per field the two z slabs (components 0 and 1, derivative along k) first and
+    // adjacent, each slab 128-byte aligned, z-slab rows padded to pw slots
+    g.pw = int((2 * sim.pml + 3) & ~size_t(3));
+    long long psi_total = 0, psi_hbase = 0;
+    for (int e = 0; e < 2; ++e) {
+        if (e == 1) psi_hbase = psi_total;
+        static const int order[6][2] = {{0, 2}, {1, 2}, {0, 1}, {1, 0}, {2, 0}, {2, 1}};  // (comp, axis)
+        for (int c = 0; c < 3; ++c) g.psi_off[e * 9 + c * 3 + c] = psi_total;  // unused (axis == comp)
+        for (const auto& ca : order) {
+            g.psi_off[e * 9 + ca[0] * 3 + ca[1]] = psi_total;
+            if (sim.pml > 0) {
+                size_t m[3] = {n0, n1, n2};
+                m[ca[1]] = ca[1] == 2 ? size_t(g.pw) : 2 * sim.pml;
+                psi_total += (long long)((m[0] * m[1] * m[2] + 31) & ~size_t(31));
             }
+        }
+    }
     s->psi_total = psi_total;
-    const long long psi_h = psi_total - g.psi_off[9];  // the H slabs, ping-ponged in the fused step
+    s->psi_hbase = psi_hbase;
+    const long long psi_h = psi_total - psi_hbase;  // the H slabs, ping-ponged in the fused step
 
     // class ids narrowed to the smallest width that holds them
     const size_t ncls = sim.classes.size();
@@ -620,8 +722,10 @@ int session_new(Gpu* gpu, const HostSim& sim, const RunSpec& rs, Session** out, 
 
     // per-region class tables for the TMA step (fused runs on sm_100)
     LocalClasses lc;
+    TmaBlocks tb;
     if (s->fused && !(std::getenv("FIELDGRID_NO_TMA") && std::getenv("FIELDGRID_NO_TMA")[0] == '1')) {
-        lc = build_local(sim, g, tma_seg(g));
+        tb = plan_tma_blocks(sim, g);
+        lc = build_local(sim, g, tb.list);
         s->local = lc.ok;
     }
     // size the arena
@@ -657,6 +761,7 @@ int session_new(Gpu* gpu, const HostSim& sim, const RunSpec& rs, Session** out, 
     need += carve_size(ENERGY_BLOCKS * 8);
     need += carve_size(64);
     if (s->local) need += carve_size(lc.ids.size()) + carve_size(lc.tables.size() * 4);
+    need += carve_size(tb.list.size() * sizeof(int4));
     size_t free_b = 0, total_b = 0;
     FG_CUDA(cudaMemGetInfo(&free_b, &total_b));
     if (need + (size_t(256) << 20) > free_b) {
@@ -672,9 +777,9 @@ int session_new(Gpu* gpu, const HostSim& sim, const RunSpec& rs, Session** out, 
     if (s->fused) { s->e2 = carve<float>(cur, fields); s->h2 = carve<float>(cur, fields); }
     s->psi = carve<float>(cur, size_t(std::max<long long>(psi_total, 1)));
     if (s->fused) {
-        // the H slabs of the second set live at psi_h2 - psi_off[9] so the same offsets apply
+        // the H slabs of the second set live at psi_h2 + psi_hbase so the same offsets apply
         float* hb = carve<float>(cur, size_t(std::max<long long>(psi_h, 1)));
-        s->psi_h2 = hb - g.psi_off[9];
+        s->psi_h2 = hb - psi_hbase;
     }
     s->node_class = carve<char>(cur, nnp * size_t(s->cid_bytes));
     s->classes = carve<DevCoef>(cur, ncls);
@@ -710,6 +815,10 @@ int session_new(Gpu* gpu, const HostSim& sim, const RunSpec& rs, Session** out, 
         s->local_ids = carve<uint8_t>(cur, lc.ids.size());
         s->tables = carve<float>(cur, lc.tables.size());
     }
+    if (!tb.list.empty()) s->tma_blocks = carve<int4>(cur, tb.list.size());
+    s->tma.n_clean = tb.clean;
+    s->tma.n_layer = int(tb.list.size()) - tb.clean;
+    s->tma.seg = tb.seg;
     if (size_t(cur - s->arena) > need) { err = "internal: arena overflow"; return FG_ERR_INVALID; }
 
     cudaStream_t st = s->stream;
@@ -778,6 +887,7 @@ int session_new(Gpu* gpu, const HostSim& sim, const RunSpec& rs, Session** out, 
         rc |= up(s->local_ids, lc.ids.data(), lc.ids.size());
         rc |= up(s->tables, lc.tables.data(), lc.tables.size() * 4);
     }
+    if (!tb.list.empty()) rc |= up(s->tma_blocks, tb.list.data(), tb.list.size() * sizeof(int4));
     rc |= up(d_dft, t_dft.data(), t_dft.size() * 4);
     rc |= up(d_far, t_far.data(), t_far.size() * 4);
     if (rc) return FG_ERR_CUDA;
@@ -787,7 +897,8 @@ int session_new(Gpu* gpu, const HostSim& sim, const RunSpec& rs, Session** out, 
     plan_tma(*s);
     if (s->tma.ok)
         s->variant = "TMA fused march, tile " + std::to_string(s->tma.tj) + "x" + std::to_string(s->tma.tk) + ", " +
-                     std::to_string(s->tma.seg) + " planes per block, " +
+                     std::to_string(s->tma.seg) + " planes per block, " + std::to_string(s->tma.n_clean) +
+                     " clean + " + std::to_string(s->tma.n_layer) + " layer blocks, " +
                      std::to_string(TMA_SHAPES[s->tma.shape].stages) + " stages, " +
                      std::to_string(TMA_SHAPES[s->tma.shape].minb) + " blocks/SM, " +
                      (s->local ? "per-block class tables" : "global class table");

@@ -14,11 +14,15 @@ namespace fg {
 // Node geometry shared by every kernel. On the device a row of n2 nodes is stored with pitch p2
 // (n2 rounded up to 32, so rows start 128-byte aligned and TMA strides are legal): the device
 // node index is (i*n1 + j)*p2 + k. Fields are component-major with component stride cs
-// (>= n0*n1*p2). The psi slabs keep the reference's unpadded layout (sim.rs:659-665).
+// (>= n0*n1*p2). The psi slabs follow the reference's layout (sim.rs:659-665), except that a
+// z slab (derivative along k) pads its rows of 2 pml slots to pw, a multiple of 4, so its rows
+// are whole 16-byte units for the TMA; slabs start 128-byte aligned, and each field's two z
+// slabs sit next to each other (one box brings both components).
 struct Geom {
     int n0, n1, n2;
     int p2;
     int pml;
+    int pw;                     // z-slab row pitch: 2 pml rounded up to 4
     long long nn;               // real nodes n0*n1*n2
     long long cs;
     const AxisNode* ax[3];
@@ -61,10 +65,9 @@ struct StepConst {          // per-run scalars (run.rs:433-464 Params)
 };
 
 __device__ __forceinline__ long long psi_at(const Geom& g, int a, int i, int j, int k, int s) {
-    const int w = 2 * g.pml;
     if (a == 0) return ((long long)s * g.n1 + j) * g.n2 + k;
-    if (a == 1) return ((long long)i * w + s) * g.n2 + k;
-    return ((long long)i * g.n1 + j) * w + s;
+    if (a == 1) return ((long long)i * (2 * g.pml) + s) * g.n2 + k;
+    return ((long long)i * g.n1 + j) * g.pw + s;
 }
 
 // The step index n of the running step: the first kernel of step n raised the counter to n + 1.

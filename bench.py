@@ -256,7 +256,10 @@ def main():
     classes = sim.coef_classes()
     debye_edges = sim.count("debye_edges")
     s.close()
-    dom_name, dom_ms = max(kt.items(), key=lambda x: x[1])
+    # the field update of a step: the march over the clean box plus the CPML shell kernels (or the
+    # separate H and E kernels); its time is what the 48 B/node roofline is measured against
+    field_parts = [k for k in ("fused_step", "shell_h", "shell_e", "update_h", "update_e") if k in kt]
+    dom_name, dom_ms = "field_update", sum(kt[k] for k in field_parts)
     peak, peak_src = measured_peaks()
     achieved = BYTES_PER_NODE * nn / (dom_ms / 1e3) / 1e9
     total_kt = sum(kt.values())
@@ -301,6 +304,7 @@ def main():
             "hbm_fraction_of_algorithmic": BYTES_PER_NODE * value * 1e6 / world / 1e9 / peak,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": traffic_for(dom_name, sc.name), "kernel": dom_name,
+                         "kernels": field_parts,
                          "bytes_per_launch": BYTES_PER_NODE * nn, "kernel_ms": dom_ms, "peak_source": peak_src},
             "kernel_ms": {k: round(v, 5) for k, v in kt.items()},
             "kernel_share": {k: round(v / total_kt, 4) for k, v in kt.items()},

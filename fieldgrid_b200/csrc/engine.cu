@@ -18,6 +18,7 @@
 #include "kernels.cuh"
 #include "stencil_fused.cuh"
 #include "stencil_separate.cuh"
+#include "stencil_shell.cuh"
 #include "stencil_tma.cuh"
 
 #include <cudaTypedefs.h>
@@ -96,7 +97,10 @@ struct Session {
     int* error = nullptr;           // set by a kernel whose bounded wait ran out
     TmaPlan tma;                    // the TMA-fed fused step, when it applies
     uint8_t* local_ids = nullptr;   // per node: index into its block region's coefficient table
-    int4* tma_blocks = nullptr;     // the TMA step's blocks: clean ones first, then the layer ones
+    int4* tma_blocks = nullptr;     // the TMA march's blocks over the clean box
+    std::vector<int4> tma_plan_blocks;  // the same list on the host
+    int clean_lo[3] = {0, 0, 0}, clean_hi[3] = {0, 0, 0};
+    ShellBoxes shell{};             // the CPML shell around the clean box
     float* tables = nullptr;        // per block region: LOCAL_CLASSES x (ca[3], cb[3])
     bool local = false;
     // counts
@@ -174,111 +178,115 @@ struct TmaShape {
 constexpr TmaShape TMA_SHAPES[] = {{4, 2}, {3, 3}, {2, 3}};
 constexpr int TMA_NSHAPES = 3;
 
-template <typename CID, bool LOCAL, int ST, bool PML = true>
-using TmaLS = TmaLayout<TMA_TJ, TMA_TK, CID, ST, TMA_SEGMAX, LOCAL, PML>;
+template <typename CID, bool LOCAL, int ST>
+using TmaLS = TmaLayout<TMA_TJ, TMA_TK, CID, ST, TMA_SEGMAX, LOCAL>;
 template <typename CID, bool LOCAL = false>
 using TmaL = TmaLS<CID, LOCAL, TMA_STAGES>;
-template <typename CID, bool LOCAL, int SHAPE, bool PML>
+template <typename CID, bool LOCAL, int SHAPE>
 constexpr auto tma_kernel_s =
-    k_tma_step<TMA_TJ, TMA_TK, CID, TMA_SHAPES[SHAPE].stages, TMA_SEGMAX, LOCAL, TMA_SHAPES[SHAPE].minb, PML>;
+    k_tma_step<TMA_TJ, TMA_TK, CID, TMA_SHAPES[SHAPE].stages, TMA_SEGMAX, LOCAL, TMA_SHAPES[SHAPE].minb>;
 
-template <typename CID, bool LOCAL, int SHAPE, bool PML>
-int tma_smem_s() { return TmaLS<CID, LOCAL, TMA_SHAPES[SHAPE].stages, PML>::TOTAL; }
+template <typename CID, bool LOCAL, int SHAPE>
+int tma_smem_s() { return TmaLS<CID, LOCAL, TMA_SHAPES[SHAPE].stages>::TOTAL; }
 
-// Calls f(kernel, smem bytes) with the instantiation for (class-id width, local tables, shape,
-// clean or layer blocks).
+// Calls f(kernel, smem bytes) with the instantiation for (class-id width, local tables, shape).
 template <typename F>
-bool with_tma_kernel(int cid_bytes, bool local, int shape, bool pml, F&& f) {
-    auto go = [&](auto sh, auto pm) {
+bool with_tma_kernel(int cid_bytes, bool local, int shape, F&& f) {
+    auto go = [&](auto sh) {
         constexpr int S = decltype(sh)::value;
-        constexpr bool P = decltype(pm)::value;
-        if (local) return f(tma_kernel_s<uint8_t, true, S, P>, tma_smem_s<uint8_t, true, S, P>());
-        if (cid_bytes == 1) return f(tma_kernel_s<uint8_t, false, S, P>, tma_smem_s<uint8_t, false, S, P>());
-        if (cid_bytes == 2) return f(tma_kernel_s<uint16_t, false, S, P>, tma_smem_s<uint16_t, false, S, P>());
-        return f(tma_kernel_s<uint32_t, false, S, P>, tma_smem_s<uint32_t, false, S, P>());
+        if (local) return f(tma_kernel_s<uint8_t, true, S>, tma_smem_s<uint8_t, true, S>());
+        if (cid_bytes == 1) return f(tma_kernel_s<uint8_t, false, S>, tma_smem_s<uint8_t, false, S>());
+        if (cid_bytes == 2) return f(tma_kernel_s<uint16_t, false, S>, tma_smem_s<uint16_t, false, S>());
+        return f(tma_kernel_s<uint32_t, false, S>, tma_smem_s<uint32_t, false, S>());
     };
-    auto by_shape = [&](auto pm) {
-        switch (shape) {
-            case 0: return go(std::integral_constant<int, 0>{}, pm);
-            case 1: return go(std::integral_constant<int, 1>{}, pm);
-            default: return go(std::integral_constant<int, 2>{}, pm);
-        }
-    };
-    return pml ? by_shape(std::true_type{}) : by_shape(std::false_type{});
+    switch (shape) {
+        case 0: return go(std::integral_constant<int, 0>{});
+        case 1: return go(std::integral_constant<int, 1>{});
+        default: return go(std::integral_constant<int, 2>{});
+    }
 }
 
-// tiles along k: a node count of 64t + 1 gives t tiles, the last owning the extra column
-inline int tma_ktiles(int n2) { return (n2 > TMA_TK && n2 % TMA_TK == 1) ? (n2 - 1) / TMA_TK : (n2 + TMA_TK - 1) / TMA_TK; }
-
-// x-planes per block: enough segments for several waves of 3 blocks per SM, at most TMA_SEGMAX.
-int tma_seg(const Geom& g) {
-    const long long tiles = (long long)tma_ktiles(g.n2) * ((g.n1 + TMA_TJ - 1) / TMA_TJ);
-    int seg = TMA_SEGMAX;
-    while (seg > 8 && tiles * ((g.n0 + seg - 1) / seg) < 148 * 3 * 6) seg /= 2;
-    return seg;
+// Tiles along k over [za, zb): when the range reaches n2 and spans 64t + 1 nodes, t tiles, the
+// last owning the extra column.
+inline int tma_ktiles(int za, int zb, int n2) {
+    const int w = zb - za;
+    return (zb == n2 && w > TMA_TK && w % TMA_TK == 1) ? (w - 1) / TMA_TK : (w + TMA_TK - 1) / TMA_TK;
 }
 
-// The blocks of the TMA step, (k0, j0, i0, i1) each: a TJ x TK tile over one x-segment. The x
-// range is cut where the CPML begins, so that "clean" blocks (listed first) have no plane, row or
-// column with a live psi slot anywhere in their tile, halo row, halo column or halo plane; they
-// run the kernel without psi code. The rest run the layer kernel.
-struct TmaBlocks {
-    std::vector<int4> list;
-    int clean = 0;
-    int seg = 0;     // planes per clean block (at most)
+// The fused TMA march covers the clean box [lo, hi): no node the march computes there (its tiles
+// and their halo row, column and plane) has a live CPML slot, so the march carries no psi term.
+// The box starts one node past the low layer, so the halo stays outside it, and along k on a
+// 16-node boundary (the TMA boxes start at k0 - 4 floats and at k0 class ids, and a box origin
+// must sit on 16 bytes, whatever the id width); along k its width is even unless it reaches n2,
+// so column pairs are owned whole. The shell around it (the layer and a one-node ring) goes to
+// the shell kernels. Blocks are (k0, j0, i0, i1): a TJ x TK tile over one x-segment.
+struct CleanPlan {
+    std::vector<int4> blocks;
+    int seg = 0;                 // planes per block (at most)
+    int lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
+    ShellBoxes shell{};
+    bool ok = false;
 };
 
-TmaBlocks plan_tma_blocks(const HostSim& sim, const Geom& g) {
-    auto hot = [&](int a, int i) {
-        const AxisNode& n = sim.ax[a].node[size_t(i)];
-        return n.slot_e >= 0 || n.slot_h >= 0;
-    };
-    // x: clean planes [xa, xb), chosen so no plane of [xa - 1, xb) is hot
+// [a, b) along one axis such that no node of [a - 1, b) has a live slot; false when empty.
+bool clean_range(const Axis& ax, int n, int& a, int& b) {
+    auto hot = [&](int i) { return ax.node[size_t(i)].slot_e >= 0 || ax.node[size_t(i)].slot_h >= 0; };
     int lead = 0;
-    while (lead < g.n0 && hot(0, lead)) ++lead;
-    int trail = g.n0;
-    while (trail > lead && hot(0, trail - 1)) --trail;
-    int xa = lead > 0 ? lead + 1 : 0, xb = trail;
-    bool inner = xa < xb;
-    for (int p = std::max(xa - 1, 0); inner && p < xb; ++p) inner = !hot(0, p);
-    TmaBlocks out;
-    out.seg = tma_seg(g);
-    std::vector<int2> segs;
-    std::vector<char> seg_clean;
-    auto chunk = [&](int lo, int hi, int len, bool clean) {
-        if (hi <= lo) return;
-        const int n = (hi - lo + len - 1) / len;
-        for (int q = 0; q < n; ++q) {
-            segs.push_back(make_int2(lo + int((long long)(hi - lo) * q / n), lo + int((long long)(hi - lo) * (q + 1) / n)));
-            seg_clean.push_back(clean);
-        }
-    };
-    if (inner) {
-        chunk(0, xa, TMA_SEGMAX, false);
-        chunk(xa, xb, out.seg, true);
-        chunk(xb, g.n0, TMA_SEGMAX, false);
-    } else {
-        chunk(0, g.n0, out.seg, false);
-    }
-    // tiles: clean when no row of j0-1 .. j0+TJ-1 and no column of k0-1 .. k0+TK is hot
-    const int kt = tma_ktiles(g.n2), jt = (g.n1 + TMA_TJ - 1) / TMA_TJ;
-    std::vector<char> kcl(size_t(kt), 1), jcl(size_t(jt), 1);
-    for (int bx = 0; bx < kt; ++bx)
-        for (int k = std::max(bx * TMA_TK - 1, 0); k <= std::min(bx * TMA_TK + TMA_TK, g.n2 - 1); ++k)
-            if (hot(2, k)) kcl[size_t(bx)] = 0;
-    for (int by = 0; by < jt; ++by)
-        for (int j = std::max(by * TMA_TJ - 1, 0); j <= std::min(by * TMA_TJ + TMA_TJ - 1, g.n1 - 1); ++j)
-            if (hot(1, j)) jcl[size_t(by)] = 0;
-    std::vector<int4> layer;
-    for (size_t q = 0; q < segs.size(); ++q)
+    while (lead < n && hot(lead)) ++lead;
+    int trail = n;
+    while (trail > lead && hot(trail - 1)) --trail;
+    a = lead > 0 ? lead + 1 : 0;
+    b = trail;
+    for (int i = std::max(a - 1, 0); i < b; ++i)
+        if (hot(i)) return false;
+    return a < b;
+}
+
+CleanPlan plan_clean(const HostSim& sim, const Geom& g) {
+    CleanPlan out;
+    const int n[3] = {g.n0, g.n1, g.n2};
+    for (int a = 0; a < 3; ++a)
+        if (!clean_range(sim.ax[a], n[a], out.lo[a], out.hi[a])) return out;
+    out.lo[2] = (out.lo[2] + 15) & ~15;   // k0 is the class-id box origin: 16 bytes of 8-bit ids
+    if (out.hi[2] < g.n2) out.hi[2] = out.lo[2] + ((out.hi[2] - out.lo[2]) & ~1);
+    if (out.lo[2] >= out.hi[2]) return out;
+    const int kt = tma_ktiles(out.lo[2], out.hi[2], g.n2);
+    const int jt = (out.hi[1] - out.lo[1] + TMA_TJ - 1) / TMA_TJ;
+    const int xw = out.hi[0] - out.lo[0];
+    // x-planes per block: enough blocks for several waves of 3 blocks per SM, at most TMA_SEGMAX
+    int seg = TMA_SEGMAX;
+    while (seg > 8 && (long long)kt * jt * ((xw + seg - 1) / seg) < 148 * 3 * 6) seg /= 2;
+    out.seg = seg;
+    const int ns = (xw + seg - 1) / seg;
+    for (int q = 0; q < ns; ++q) {
+        const int i0 = out.lo[0] + int((long long)xw * q / ns), i1 = out.lo[0] + int((long long)xw * (q + 1) / ns);
         for (int by = 0; by < jt; ++by)
-            for (int bx = 0; bx < kt; ++bx) {
-                const int4 b = make_int4(bx * TMA_TK, by * TMA_TJ, segs[q].x, segs[q].y);
-                if (seg_clean[q] && jcl[size_t(by)] && kcl[size_t(bx)]) out.list.push_back(b);
-                else layer.push_back(b);
-            }
-    out.clean = int(out.list.size());
-    out.list.insert(out.list.end(), layer.begin(), layer.end());
+            for (int bx = 0; bx < kt; ++bx)
+                out.blocks.push_back(make_int4(out.lo[2] + bx * TMA_TK, out.lo[1] + by * TMA_TJ, i0, i1));
+    }
+    // the shell: up to six boxes around the clean box
+    ShellBoxes& sb = out.shell;
+    sb.n = 0;
+    auto add = [&](int l0, int h0, int l1, int h1, int l2, int h2) {
+        if (l0 >= h0 || l1 >= h1 || l2 >= h2) return;
+        const int q = sb.n++;
+        sb.lo[q][0] = l0; sb.hi[q][0] = h0;
+        sb.lo[q][1] = l1; sb.hi[q][1] = h1;
+        sb.lo[q][2] = l2; sb.hi[q][2] = h2;
+    };
+    const int *lo = out.lo, *hi = out.hi;
+    add(0, lo[0], 0, g.n1, 0, g.n2);
+    add(hi[0], g.n0, 0, g.n1, 0, g.n2);
+    add(lo[0], hi[0], 0, lo[1], 0, g.n2);
+    add(lo[0], hi[0], hi[1], g.n1, 0, g.n2);
+    add(lo[0], hi[0], lo[1], hi[1], 0, lo[2]);
+    add(lo[0], hi[0], lo[1], hi[1], hi[2], g.n2);
+    sb.start[0] = 0;
+    for (int q = 0; q < sb.n; ++q)
+        sb.start[q + 1] = sb.start[q] + (long long)(sb.hi[q][0] - sb.lo[q][0]) * (sb.hi[q][1] - sb.lo[q][1]) *
+                                             (sb.hi[q][2] - sb.lo[q][2]);
+    for (int q = sb.n; q < 6; ++q) sb.start[q + 1] = sb.start[sb.n];
+    out.ok = true;
     return out;
 }
 
@@ -291,7 +299,8 @@ struct LocalClasses {
     bool ok = true;
 };
 
-LocalClasses build_local(const HostSim& sim, const Geom& g, const std::vector<int4>& blocks) {
+LocalClasses build_local(const HostSim& sim, const Geom& g, const CleanPlan& cp) {
+    const std::vector<int4>& blocks = cp.blocks;
     LocalClasses out;
     const long long regions = (long long)blocks.size();
     out.ids.assign(size_t(g.n0) * g.n1 * g.p2, 0);
@@ -303,9 +312,9 @@ LocalClasses build_local(const HostSim& sim, const Geom& g, const std::vector<in
         if (over) continue;
         const int4 b = blocks[size_t(r)];
         const int k0 = b.x, j0 = b.y, i0 = b.z, i1 = b.w;
-        int kend = std::min(k0 + TMA_TK, g.n2);
-        if (k0 + TMA_TK == g.n2 - 1) kend = g.n2;  // the owned right-edge column
-        const int jend = std::min(j0 + TMA_TJ, g.n1);
+        int kend = std::min(k0 + TMA_TK, cp.hi[2]);
+        if (cp.hi[2] == g.n2 && k0 + TMA_TK == g.n2 - 1) kend = g.n2;  // the owned right-edge column
+        const int jend = std::min(j0 + TMA_TJ, cp.hi[1]);
         uint32_t keys[512];
         uint16_t vals[512];
         std::fill(keys, keys + 512, 0xffffffffu);
@@ -365,55 +374,29 @@ void plan_tma(Session& s) {
     const cuuint64_t cstr[2] = {cuuint64_t(g.p2) * b, cuuint64_t(g.n1) * g.p2 * b};
     const cuuint32_t cbox[3] = {cuuint32_t(TmaL<float>::CW), cuuint32_t(TmaL<float>::CR), 1};
     if (!encode(&t.c, dt, s.local ? (void*)s.local_ids : s.node_class, 3, cdims, cstr, cbox, t.why)) return;
-    // z-slab psi: (slot, j, i, component) over each field's two adjacent z slabs
-    t.pz = g.pml > 0 && g.pw <= TmaL<float>::PZW;
-    if (t.pz) {
-        const long long zlen = g.psi_off[1 * 3 + 2] - g.psi_off[0 * 3 + 2];  // slab stride, 128-byte multiple
-        const cuuint64_t zd[4] = {cuuint64_t(g.pw), cuuint64_t(g.n1), cuuint64_t(g.n0), 2};
-        const cuuint64_t zs[3] = {cuuint64_t(g.pw) * 4, cuuint64_t(g.n1) * g.pw * 4, cuuint64_t(zlen) * 4};
-        const cuuint32_t zb[4] = {cuuint32_t(g.pw), cuuint32_t(TMA_TJ + 1), 1, 2};
-        if (!encode(&t.pze, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, s.psi + g.psi_off[0 * 3 + 2], 4, zd, zs, zb, t.why)) return;
-        float* hsets[2] = {s.psi, s.psi_h2};  // the H slabs read by a step whose input set is 0 / 1
-        for (int q = 0; q < 2; ++q)
-            if (!encode(&t.pzh[q], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, hsets[q] + g.psi_off[9 + 0 * 3 + 2], 4, zd, zs, zb,
-                        t.why))
-                return;
-    }
     cudaError_t ce = cudaSuccess;
     for (int sh = 0; sh < TMA_NSHAPES && ce == cudaSuccess; ++sh)
-        for (int pm = 0; pm < 2 && ce == cudaSuccess; ++pm)
-            with_tma_kernel(b, s.local, sh, pm != 0, [&](auto kern, int smem) {
-                ce = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-                if (sh == t.shape) t.smem = std::max(t.smem, smem);
-                return true;
-            });
+        with_tma_kernel(b, s.local, sh, [&](auto kern, int smem) {
+            ce = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+            if (sh == t.shape) t.smem = smem;
+            return true;
+        });
     if (ce != cudaSuccess) { t.why = std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(ce); return; }
     if (!s.tma_blocks) { t.why = "no block list"; return; }
+    // every TMA box origin along k must sit on 16 bytes: k0 - 4 floats and k0 ids of up to 4 bytes
+    for (const int4& bk : s.tma_plan_blocks)
+        if (bk.x % 16 != 0) { t.why = "internal: unaligned tile origin"; return; }
     t.ok = true;
 }
 
-int launch_tma(Session& s, int parity, float* e_out, float* h_out, const float* psi_h_in, float* psi_h_out) {
-    const Geom& g = s.geom;
+int launch_tma(Session& s, int parity, float* e_out, float* h_out) {
     const TmaPlan& t = s.tma;
-    TmaArgs a{g, s.classes, e_out, h_out, s.psi, psi_h_in, psi_h_out, s.sc.k_mu, int(t.pz), s.tma_blocks, 0, 1,
-              s.tables, s.counter, s.error};
-    const dim3 blk(TMA_CONSUMERS + 32);
-    // the clean blocks, then the layer blocks (without staged z boxes the last two maps are never read)
-    const CUtensorMap& pze = t.pz ? t.pze : t.c;
-    const CUtensorMap& pzh = t.pz ? t.pzh[parity] : t.c;
-    if (t.n_clean > 0)
-        with_tma_kernel(s.cid_bytes, s.local, t.shape, false, [&](auto kern, int smem) {
-            kern<<<unsigned(t.n_clean), blk, smem, s.stream>>>(t.e[parity], t.h[parity], t.c, pze, pzh, a);
-            return true;
-        });
-    if (t.n_layer > 0) {
-        a.block0 = t.n_clean;
-        a.bump = t.n_clean == 0;
-        with_tma_kernel(s.cid_bytes, s.local, t.shape, true, [&](auto kern, int smem) {
-            kern<<<unsigned(t.n_layer), blk, smem, s.stream>>>(t.e[parity], t.h[parity], t.c, pze, pzh, a);
-            return true;
-        });
-    }
+    TmaArgs a{s.geom, s.classes, e_out, h_out, s.sc.k_mu, s.clean_hi[1], s.clean_hi[2], s.tma_blocks, s.tables,
+              s.counter, s.error};
+    with_tma_kernel(s.cid_bytes, s.local, t.shape, [&](auto kern, int smem) {
+        kern<<<unsigned(t.blocks), TMA_CONSUMERS + 32, smem, s.stream>>>(t.e[parity], t.h[parity], t.c, a);
+        return true;
+    });
     return cudaPeekAtLastError() == cudaSuccess ? 0 : 1;
 }
 
@@ -453,11 +436,24 @@ int enqueue_step(Session& s, int parity, std::string& err) {
         }
         mark("fused_step");
         int rc = s.tma.ok
-                     ? launch_tma(s, parity, e_out, h_out, parity ? s.psi_h2 : s.psi, parity ? s.psi : s.psi_h2)
+                     ? launch_tma(s, parity, e_out, h_out)
                      : launch_fused(s.shape, s.cid_bytes, g, s.node_class, s.classes, e_in, h_in, e_out, h_out, s.psi,
                                     parity ? s.psi_h2 : s.psi, parity ? s.psi : s.psi_h2, s.sc.k_mu, s.counter,
                                     s.n_wires > 0, st);
         if (rc) { err = "fused step launch failed"; return FG_ERR_CUDA; }
+        if (s.tma.ok && s.shell.n > 0) {
+            // the CPML shell around the march's clean box
+            const unsigned gb = unsigned((s.shell.start[s.shell.n] + SHELL_THREADS - 1) / SHELL_THREADS);
+            mark("shell_h");
+            k_shell_h<<<gb, SHELL_THREADS, 0, st>>>(g, s.shell, e_in, h_in, h_out, parity ? s.psi_h2 : s.psi,
+                                                    parity ? s.psi : s.psi_h2, s.sc.k_mu);
+            mark("shell_e");
+            switch (s.cid_bytes) {
+                case 1: k_shell_e<uint8_t><<<gb, SHELL_THREADS, 0, st>>>(g, s.shell, (const uint8_t*)s.node_class, s.classes, h_out, e_in, e_out, s.psi); break;
+                case 2: k_shell_e<uint16_t><<<gb, SHELL_THREADS, 0, st>>>(g, s.shell, (const uint16_t*)s.node_class, s.classes, h_out, e_in, e_out, s.psi); break;
+                default: k_shell_e<uint32_t><<<gb, SHELL_THREADS, 0, st>>>(g, s.shell, (const uint32_t*)s.node_class, s.classes, h_out, e_in, e_out, s.psi); break;
+            }
+        }
         if (s.n_sheets) {
             mark("sheet_pre");
             k_sheet_pre<<<(s.n_sheets + 127) / 128, 128, 0, st>>>(s.sheets, s.n_sheets, e_in, h_out);
@@ -493,7 +489,7 @@ int enqueue_step(Session& s, int parity, std::string& err) {
 
 uint64_t count_launches(const Session& s) {
     uint64_t n = 1;  // the field update (fused) or H update (separate)
-    if (s.tma.ok && s.tma.n_clean > 0 && s.tma.n_layer > 0) n++;  // clean and layer blocks of the TMA step
+    if (s.tma.ok && s.shell.n > 0) n += 2;  // the CPML shell around the TMA march
     if (!s.fused) n += 1 + (s.n_debye ? 1 : 0);
     if (s.n_wires) n++;
     if (s.n_sheets) n += 2;
@@ -722,11 +718,13 @@ int session_new(Gpu* gpu, const HostSim& sim, const RunSpec& rs, Session** out, 
 
     // per-region class tables for the TMA step (fused runs on sm_100)
     LocalClasses lc;
-    TmaBlocks tb;
+    CleanPlan cp;
     if (s->fused && !(std::getenv("FIELDGRID_NO_TMA") && std::getenv("FIELDGRID_NO_TMA")[0] == '1')) {
-        tb = plan_tma_blocks(sim, g);
-        lc = build_local(sim, g, tb.list);
-        s->local = lc.ok;
+        cp = plan_clean(sim, g);
+        if (cp.ok) {
+            lc = build_local(sim, g, cp);
+            s->local = lc.ok;
+        }
     }
     // size the arena
     const size_t fields = size_t(3 * cs);
@@ -761,7 +759,7 @@ int session_new(Gpu* gpu, const HostSim& sim, const RunSpec& rs, Session** out, 
     need += carve_size(ENERGY_BLOCKS * 8);
     need += carve_size(64);
     if (s->local) need += carve_size(lc.ids.size()) + carve_size(lc.tables.size() * 4);
-    need += carve_size(tb.list.size() * sizeof(int4));
+    need += carve_size(cp.blocks.size() * sizeof(int4));
     size_t free_b = 0, total_b = 0;
     FG_CUDA(cudaMemGetInfo(&free_b, &total_b));
     if (need + (size_t(256) << 20) > free_b) {
@@ -815,10 +813,12 @@ int session_new(Gpu* gpu, const HostSim& sim, const RunSpec& rs, Session** out, 
         s->local_ids = carve<uint8_t>(cur, lc.ids.size());
         s->tables = carve<float>(cur, lc.tables.size());
     }
-    if (!tb.list.empty()) s->tma_blocks = carve<int4>(cur, tb.list.size());
-    s->tma.n_clean = tb.clean;
-    s->tma.n_layer = int(tb.list.size()) - tb.clean;
-    s->tma.seg = tb.seg;
+    if (!cp.blocks.empty()) s->tma_blocks = carve<int4>(cur, cp.blocks.size());
+    s->tma_plan_blocks = cp.blocks;
+    s->tma.blocks = int(cp.blocks.size());
+    s->tma.seg = cp.seg;
+    s->shell = cp.shell;
+    for (int q = 0; q < 3; ++q) { s->clean_lo[q] = cp.lo[q]; s->clean_hi[q] = cp.hi[q]; }
     if (size_t(cur - s->arena) > need) { err = "internal: arena overflow"; return FG_ERR_INVALID; }
 
     cudaStream_t st = s->stream;
@@ -887,7 +887,7 @@ int session_new(Gpu* gpu, const HostSim& sim, const RunSpec& rs, Session** out, 
         rc |= up(s->local_ids, lc.ids.data(), lc.ids.size());
         rc |= up(s->tables, lc.tables.data(), lc.tables.size() * 4);
     }
-    if (!tb.list.empty()) rc |= up(s->tma_blocks, tb.list.data(), tb.list.size() * sizeof(int4));
+    if (!cp.blocks.empty()) rc |= up(s->tma_blocks, cp.blocks.data(), cp.blocks.size() * sizeof(int4));
     rc |= up(d_dft, t_dft.data(), t_dft.size() * 4);
     rc |= up(d_far, t_far.data(), t_far.size() * 4);
     if (rc) return FG_ERR_CUDA;
@@ -897,8 +897,9 @@ int session_new(Gpu* gpu, const HostSim& sim, const RunSpec& rs, Session** out, 
     plan_tma(*s);
     if (s->tma.ok)
         s->variant = "TMA fused march, tile " + std::to_string(s->tma.tj) + "x" + std::to_string(s->tma.tk) + ", " +
-                     std::to_string(s->tma.seg) + " planes per block, " + std::to_string(s->tma.n_clean) +
-                     " clean + " + std::to_string(s->tma.n_layer) + " layer blocks, " +
+                     std::to_string(s->tma.seg) + " planes per block, " + std::to_string(s->tma.blocks) +
+                     " blocks on the clean box, CPML shell of " + std::to_string(s->shell.start[s->shell.n]) +
+                     " nodes, " +
                      std::to_string(TMA_SHAPES[s->tma.shape].stages) + " stages, " +
                      std::to_string(TMA_SHAPES[s->tma.shape].minb) + " blocks/SM, " +
                      (s->local ? "per-block class tables" : "global class table");

@@ -226,12 +226,18 @@ def test_stepping_in_odd_chunks_is_the_same_as_one_run(gpu, fused):
 
 
 def test_the_pipelines_are_the_cuda_kernels(gpu):
-    sc = W.dielectric_box(16, pml=3, steps=4)
+    # a grid with room for a clean box inside its CPML: the TMA march plus the two shell kernels
+    sc = W.dielectric_box(48, pml=6, steps=4)
     sim = fdtd.Sim.try_new(*sc.args())
     s = fdtd.Session(gpu, sim, 0, sc.pulse, sc.extras)
-    assert "fused" in s.variant and "TMA" in s.variant, s.variant
-    assert s.launches_per_step >= 2
+    assert "TMA" in s.variant and "CPML shell" in s.variant, s.variant
+    assert s.launches_per_step >= 4
     assert s.stream != 0
+    s.close()
+    # too small for a clean box: the direct-load fused march does the whole step
+    sc = W.dielectric_box(16, pml=3, steps=4)
+    s = fdtd.Session(gpu, fdtd.Sim.try_new(*sc.args()), 0, sc.pulse, sc.extras)
+    assert "fused" in s.variant and "TMA" not in s.variant, s.variant
     s.close()
 
 

@@ -100,7 +100,7 @@ struct Session {
     int4* tma_blocks = nullptr;     // the TMA march's blocks over the clean box
     std::vector<int4> tma_plan_blocks;  // the same list on the host
     int clean_lo[3] = {0, 0, 0}, clean_hi[3] = {0, 0, 0};
-    ShellBoxes shell{};             // the CPML shell around the clean box
+    ShellRows shell{};              // the CPML shell around the clean box
     float* tables = nullptr;        // per block region: LOCAL_CLASSES x (ca[3], cb[3])
     bool local = false;
     // counts
@@ -215,16 +215,18 @@ inline int tma_ktiles(int za, int zb, int n2) {
 
 // The fused TMA march covers the clean box [lo, hi): no node the march computes there (its tiles
 // and their halo row, column and plane) has a live CPML slot, so the march carries no psi term.
-// The box starts one node past the low layer, so the halo stays outside it, and along k on a
-// 16-node boundary (the TMA boxes start at k0 - 4 floats and at k0 class ids, and a box origin
-// must sit on 16 bytes, whatever the id width); along k its width is even unless it reaches n2,
-// so column pairs are owned whole. The shell around it (the layer and a one-node ring) goes to
+// The box starts one node past the low layer, so the halo stays outside it. Along k it starts on
+// an even node and ends on one unless it reaches n2, so column pairs are owned whole; the tiles
+// start at that node rounded down to 8 (a 32-byte sector: row writes of every tile but the first
+// fill whole sectors; the E and H boxes start at k0 - 4 floats, on 16 bytes; the class-id box at
+// k0 rounded down to 16 ids), and the first tile leaves its columns below the box unwritten. The shell around it (the layer and a one-node ring) goes to
 // the shell kernels. Blocks are (k0, j0, i0, i1): a TJ x TK tile over one x-segment.
 struct CleanPlan {
     std::vector<int4> blocks;
     int seg = 0;                 // planes per block (at most)
     int lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
-    ShellBoxes shell{};
+    int kbase = 0;               // the tile grid's origin along k: lo[2] rounded down to 8 nodes
+    ShellRows shell{};
     bool ok = false;
 };
 
@@ -247,10 +249,11 @@ CleanPlan plan_clean(const HostSim& sim, const Geom& g) {
     const int n[3] = {g.n0, g.n1, g.n2};
     for (int a = 0; a < 3; ++a)
         if (!clean_range(sim.ax[a], n[a], out.lo[a], out.hi[a])) return out;
-    out.lo[2] = (out.lo[2] + 15) & ~15;   // k0 is the class-id box origin: 16 bytes of 8-bit ids
+    out.lo[2] = (out.lo[2] + 1) & ~1;
     if (out.hi[2] < g.n2) out.hi[2] = out.lo[2] + ((out.hi[2] - out.lo[2]) & ~1);
     if (out.lo[2] >= out.hi[2]) return out;
-    const int kt = tma_ktiles(out.lo[2], out.hi[2], g.n2);
+    out.kbase = out.lo[2] & ~7;
+    const int kt = tma_ktiles(out.kbase, out.hi[2], g.n2);
     const int jt = (out.hi[1] - out.lo[1] + TMA_TJ - 1) / TMA_TJ;
     const int xw = out.hi[0] - out.lo[0];
     // x-planes per block: enough blocks for several waves of 3 blocks per SM, at most TMA_SEGMAX
@@ -262,30 +265,16 @@ CleanPlan plan_clean(const HostSim& sim, const Geom& g) {
         const int i0 = out.lo[0] + int((long long)xw * q / ns), i1 = out.lo[0] + int((long long)xw * (q + 1) / ns);
         for (int by = 0; by < jt; ++by)
             for (int bx = 0; bx < kt; ++bx)
-                out.blocks.push_back(make_int4(out.lo[2] + bx * TMA_TK, out.lo[1] + by * TMA_TJ, i0, i1));
+                out.blocks.push_back(make_int4(out.kbase + bx * TMA_TK, out.lo[1] + by * TMA_TJ, i0, i1));
     }
-    // the shell: up to six boxes around the clean box
-    ShellBoxes& sb = out.shell;
-    sb.n = 0;
-    auto add = [&](int l0, int h0, int l1, int h1, int l2, int h2) {
-        if (l0 >= h0 || l1 >= h1 || l2 >= h2) return;
-        const int q = sb.n++;
-        sb.lo[q][0] = l0; sb.hi[q][0] = h0;
-        sb.lo[q][1] = l1; sb.hi[q][1] = h1;
-        sb.lo[q][2] = l2; sb.hi[q][2] = h2;
-    };
-    const int *lo = out.lo, *hi = out.hi;
-    add(0, lo[0], 0, g.n1, 0, g.n2);
-    add(hi[0], g.n0, 0, g.n1, 0, g.n2);
-    add(lo[0], hi[0], 0, lo[1], 0, g.n2);
-    add(lo[0], hi[0], hi[1], g.n1, 0, g.n2);
-    add(lo[0], hi[0], lo[1], hi[1], 0, lo[2]);
-    add(lo[0], hi[0], lo[1], hi[1], hi[2], g.n2);
-    sb.start[0] = 0;
-    for (int q = 0; q < sb.n; ++q)
-        sb.start[q + 1] = sb.start[q] + (long long)(sb.hi[q][0] - sb.lo[q][0]) * (sb.hi[q][1] - sb.lo[q][1]) *
-                                             (sb.hi[q][2] - sb.lo[q][2]);
-    for (int q = sb.n; q < 6; ++q) sb.start[q + 1] = sb.start[sb.n];
+    // the shell rows around the clean box
+    ShellRows& sr = out.shell;
+    sr.xa = out.lo[0]; sr.xb = out.hi[0];
+    sr.ya = out.lo[1]; sr.yb = out.hi[1];
+    sr.za = out.lo[2]; sr.zb = out.hi[2];
+    sr.ra = unsigned((sr.xa + g.n0 - sr.xb) * g.n1);
+    sr.rb = unsigned((sr.xb - sr.xa) * (sr.ya + g.n1 - sr.yb));
+    sr.rc = (sr.za > 0 || sr.zb < g.n2) ? unsigned((sr.xb - sr.xa) * (sr.yb - sr.ya)) : 0u;
     out.ok = true;
     return out;
 }
@@ -312,6 +301,7 @@ LocalClasses build_local(const HostSim& sim, const Geom& g, const CleanPlan& cp)
         if (over) continue;
         const int4 b = blocks[size_t(r)];
         const int k0 = b.x, j0 = b.y, i0 = b.z, i1 = b.w;
+        const int kbeg = std::max(k0, cp.lo[2]);
         int kend = std::min(k0 + TMA_TK, cp.hi[2]);
         if (cp.hi[2] == g.n2 && k0 + TMA_TK == g.n2 - 1) kend = g.n2;  // the owned right-edge column
         const int jend = std::min(j0 + TMA_TJ, cp.hi[1]);
@@ -322,7 +312,7 @@ LocalClasses build_local(const HostSim& sim, const Geom& g, const CleanPlan& cp)
         float* tab = out.tables.data() + size_t(r) * LOCAL_CLASSES * 6;
         for (int i = i0; i < i1 && !over; ++i)
             for (int j = j0; j < jend && !over; ++j)
-                for (int k = k0; k < kend; ++k) {
+                for (int k = kbeg; k < kend; ++k) {
                     const uint32_t gid = sim.node_class[(size_t(i) * n1 + j) * n2 + k];
                     uint32_t h = (gid * 2654435761u) & 511u;
                     while (keys[h] != 0xffffffffu && keys[h] != gid) h = (h + 1) & 511u;
@@ -383,16 +373,16 @@ void plan_tma(Session& s) {
         });
     if (ce != cudaSuccess) { t.why = std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(ce); return; }
     if (!s.tma_blocks) { t.why = "no block list"; return; }
-    // every TMA box origin along k must sit on 16 bytes: k0 - 4 floats and k0 ids of up to 4 bytes
+    // every TMA box origin along k must sit on 16 bytes: k0 - 4 floats, and k0 & ~15 class ids
     for (const int4& bk : s.tma_plan_blocks)
-        if (bk.x % 16 != 0) { t.why = "internal: unaligned tile origin"; return; }
+        if (bk.x % 8 != 0) { t.why = "internal: unaligned tile origin"; return; }
     t.ok = true;
 }
 
 int launch_tma(Session& s, int parity, float* e_out, float* h_out) {
     const TmaPlan& t = s.tma;
-    TmaArgs a{s.geom, s.classes, e_out, h_out, s.sc.k_mu, s.clean_hi[1], s.clean_hi[2], s.tma_blocks, s.tables,
-              s.counter, s.error};
+    TmaArgs a{s.geom, s.classes, e_out, h_out, s.sc.k_mu, s.clean_lo[2], s.clean_hi[1], s.clean_hi[2], s.tma_blocks,
+              s.tables, s.counter, s.error};
     with_tma_kernel(s.cid_bytes, s.local, t.shape, [&](auto kern, int smem) {
         kern<<<unsigned(t.blocks), TMA_CONSUMERS + 32, smem, s.stream>>>(t.e[parity], t.h[parity], t.c, a);
         return true;
@@ -441,9 +431,10 @@ int enqueue_step(Session& s, int parity, std::string& err) {
                                     parity ? s.psi_h2 : s.psi, parity ? s.psi : s.psi_h2, s.sc.k_mu, s.counter,
                                     s.n_wires > 0, st);
         if (rc) { err = "fused step launch failed"; return FG_ERR_CUDA; }
-        if (s.tma.ok && s.shell.n > 0) {
-            // the CPML shell around the march's clean box
-            const unsigned gb = unsigned((s.shell.start[s.shell.n] + SHELL_THREADS - 1) / SHELL_THREADS);
+        const unsigned shell_rows = s.shell.ra + s.shell.rb + s.shell.rc;
+        if (s.tma.ok && shell_rows > 0) {
+            // the CPML shell around the march's clean box, one warp per row
+            const unsigned gb = (shell_rows + SHELL_THREADS / 32 - 1) / (SHELL_THREADS / 32);
             mark("shell_h");
             k_shell_h<<<gb, SHELL_THREADS, 0, st>>>(g, s.shell, e_in, h_in, h_out, parity ? s.psi_h2 : s.psi,
                                                     parity ? s.psi : s.psi_h2, s.sc.k_mu);
@@ -489,7 +480,7 @@ int enqueue_step(Session& s, int parity, std::string& err) {
 
 uint64_t count_launches(const Session& s) {
     uint64_t n = 1;  // the field update (fused) or H update (separate)
-    if (s.tma.ok && s.shell.n > 0) n += 2;  // the CPML shell around the TMA march
+    if (s.tma.ok && s.shell.ra + s.shell.rb + s.shell.rc > 0) n += 2;  // the CPML shell around the TMA march
     if (!s.fused) n += 1 + (s.n_debye ? 1 : 0);
     if (s.n_wires) n++;
     if (s.n_sheets) n += 2;
@@ -898,8 +889,8 @@ int session_new(Gpu* gpu, const HostSim& sim, const RunSpec& rs, Session** out, 
     if (s->tma.ok)
         s->variant = "TMA fused march, tile " + std::to_string(s->tma.tj) + "x" + std::to_string(s->tma.tk) + ", " +
                      std::to_string(s->tma.seg) + " planes per block, " + std::to_string(s->tma.blocks) +
-                     " blocks on the clean box, CPML shell of " + std::to_string(s->shell.start[s->shell.n]) +
-                     " nodes, " +
+                     " blocks on the clean box, CPML shell of " +
+                     std::to_string(s->shell.ra + s->shell.rb + s->shell.rc) + " rows, " +
                      std::to_string(TMA_SHAPES[s->tma.shape].stages) + " stages, " +
                      std::to_string(TMA_SHAPES[s->tma.shape].minb) + " blocks/SM, " +
                      (s->local ? "per-block class tables" : "global class table");

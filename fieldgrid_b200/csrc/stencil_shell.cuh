@@ -1,7 +1,8 @@
 // The CPML shell of the fused step: every node outside the clean box the TMA march covers (the
 // absorbing slabs and a one-node ring inside them), updated out of place by two plain kernels.
-// One thread owns one node and its three components; the arithmetic, operation order and guards
-// are those of the reference's CPU step (sims-field cpu.rs:48-167), as in the other pipelines:
+// One warp walks one row of shell nodes along k, a lane owning a node and its three components;
+// the arithmetic, operation order and guards are those of the reference's CPU step (sims-field
+// cpu.rs:48-167), as in the other pipelines:
 //   k_shell_h: H_out from E_in, H_in and the input set of H psi slabs (written to the output set);
 //   k_shell_e: E_out from E_in and the new H (the clean box's H written by the march, the shell's
 //              by k_shell_h), with the E psi slabs updated in place.
@@ -12,129 +13,178 @@
 
 namespace fg {
 
-// Up to six boxes [lo, hi) covering the shell; start[q] counts the nodes of boxes before q.
-struct ShellBoxes {
-    int n;
-    int lo[6][3], hi[6][3];
-    long long start[7];
+// The shell as rows of nodes along k, one warp per row:
+//   A: planes [0, xa) and [xb, n0), every row j, every column;
+//   B: planes [xa, xb), rows [0, ya) and [yb, n1), every column;
+//   C: planes [xa, xb), rows [ya, yb), the two strips of columns [0, za) and [zb, n2).
+struct ShellRows {
+    int xa, xb, ya, yb, za, zb;
+    unsigned ra, rb, rc;      // rows in A, B, C
 };
 
-// The node of shell index t, k fastest inside each box.
-__device__ __forceinline__ void shell_node(const ShellBoxes& b, long long t, int p[3]) {
-    int q = 0;
-    while (q + 1 < b.n && t >= b.start[q + 1]) ++q;
-    long long l = t - b.start[q];
-    const int w2 = b.hi[q][2] - b.lo[q][2], w1 = b.hi[q][1] - b.lo[q][1];
-    p[2] = b.lo[q][2] + int(l % w2);
-    l /= w2;
-    p[1] = b.lo[q][1] + int(l % w1);
-    p[0] = b.lo[q][0] + int(l / w1);
-}
-
-// H_c = H_c - k_mu [(dE_v/du) inv_d_u + psi_u - (dE_u/dv) inv_d_v - psi_v]   (cpu.rs:65-102)
-template <int C>
-__device__ __forceinline__ void h_shell_one(const Geom& g, const int p[3], long long id, const long long st[3],
-                                            const float* __restrict__ e, const float* __restrict__ h_in,
-                                            float* __restrict__ h_out, const float* __restrict__ psi_in,
-                                            float* __restrict__ psi_out, float k_mu) {
-    constexpr int U = (C + 1) % 3, V = (C + 2) % 3;
-    const int nu = U == 0 ? g.n0 : (U == 1 ? g.n1 : g.n2);
-    const int nv = V == 0 ? g.n0 : (V == 1 ? g.n1 : g.n2);
-    float hv = h_in[C * g.cs + id];
-    if (p[U] + 1 < nu && p[V] + 1 < nv) {
-        const float ev = e[V * g.cs + id + st[U]] - e[V * g.cs + id];
-        const float eu = e[U * g.cs + id + st[V]] - e[U * g.cs + id];
-        const AxisNode* au = g.ax[U] + p[U];
-        const AxisNode* av = g.ax[V] + p[V];
-        float t1 = ev * __ldg(&au->inv_d);
-        float t2 = eu * __ldg(&av->inv_d);
-        const int su = __ldg(&au->slot_h);
-        if (su >= 0) {
-            const long long q = g.psi_off[9 + C * 3 + U] + psi_at(g, U, p[0], p[1], p[2], su);
-            const float r = __ldg(&au->bh) * psi_in[q] + __ldg(&au->ch) * ev * __ldg(&au->raw_inv_d);
-            psi_out[q] = r;
-            t1 += r;
-        }
-        const int sv = __ldg(&av->slot_h);
-        if (sv >= 0) {
-            const long long q = g.psi_off[9 + C * 3 + V] + psi_at(g, V, p[0], p[1], p[2], sv);
-            const float r = __ldg(&av->bh) * psi_in[q] + __ldg(&av->ch) * eu * __ldg(&av->raw_inv_d);
-            psi_out[q] = r;
-            t2 += r;
-        }
-        hv = hv - k_mu * (t1 - t2);
+// Row r's (i, j); `strips` when the row covers only the two k strips.
+__device__ __forceinline__ void shell_row(const Geom& g, const ShellRows& b, unsigned r, int& i, int& j, bool& strips) {
+    if (r < b.ra) {
+        const unsigned pi = r / unsigned(g.n1);
+        j = int(r - pi * unsigned(g.n1));
+        i = int(pi) < b.xa ? int(pi) : b.xb + (int(pi) - b.xa);
+        strips = false;
+    } else if (r < b.ra + b.rb) {
+        r -= b.ra;
+        const unsigned ny = unsigned(b.ya + g.n1 - b.yb);
+        const unsigned pi = r / ny, jj = r - pi * ny;
+        i = b.xa + int(pi);
+        j = int(jj) < b.ya ? int(jj) : b.yb + (int(jj) - b.ya);
+        strips = false;
+    } else {
+        r -= b.ra + b.rb;
+        const unsigned ny = unsigned(b.yb - b.ya);
+        const unsigned pi = r / ny;
+        i = b.xa + int(pi);
+        j = b.ya + int(r - pi * ny);
+        strips = true;
     }
-    h_out[C * g.cs + id] = hv;
 }
 
-// E_c = ca E_c + cb [(dH_v/du) inv_dd_u + psi_u - (dH_u/dv) inv_dd_v - psi_v], kept where
-// cb == 0 (cpu.rs:125-162)
-template <int C>
-__device__ __forceinline__ void e_shell_one(const Geom& g, const int p[3], long long id, const long long st[3],
-                                            const DevCoef& cf, const float* __restrict__ h,
-                                            const float* __restrict__ e_in, float* __restrict__ e_out,
-                                            float* __restrict__ psi) {
-    constexpr int U = (C + 1) % 3, V = (C + 2) % 3;
-    const float cb = cf.cb[C];
-    float ev = e_in[C * g.cs + id];
-    if (cb != 0.0f && p[U] != 0 && p[V] != 0) {
-        const float hv = h[V * g.cs + id] - h[V * g.cs + id - st[U]];
-        const float hu = h[U * g.cs + id] - h[U * g.cs + id - st[V]];
-        const AxisNode* au = g.ax[U] + p[U];
-        const AxisNode* av = g.ax[V] + p[V];
-        float t1 = hv * __ldg(&au->inv_dd);
-        float t2 = hu * __ldg(&av->inv_dd);
-        const int su = __ldg(&au->slot_e);
-        if (su >= 0) {
-            const long long q = g.psi_off[C * 3 + U] + psi_at(g, U, p[0], p[1], p[2], su);
-            const float r = __ldg(&au->be) * psi[q] + __ldg(&au->ce) * hv * __ldg(&au->raw_inv_dd);
-            psi[q] = r;
-            t1 += r;
-        }
-        const int sv = __ldg(&av->slot_e);
-        if (sv >= 0) {
-            const long long q = g.psi_off[C * 3 + V] + psi_at(g, V, p[0], p[1], p[2], sv);
-            const float r = __ldg(&av->be) * psi[q] + __ldg(&av->ce) * hu * __ldg(&av->raw_inv_dd);
-            psi[q] = r;
-            t2 += r;
-        }
-        ev = cf.ca[C] * ev + cb * (t1 - t2);
-    }
-    e_out[C * g.cs + id] = ev;
-}
+// One CPML term, r = b psi + c d raw (cpu.rs:73-99, :135-159), in the reference's operation order.
+__device__ __forceinline__ float cpml_term(float b, float psi, float c, float d, float raw) { return b * psi + c * d * raw; }
 
-constexpr int SHELL_THREADS = 256;
+constexpr int SHELL_THREADS = 256;   // 8 rows per block
 
-__global__ void __launch_bounds__(SHELL_THREADS) k_shell_h(Geom g, ShellBoxes b, const float* __restrict__ e_in,
+// The new H of one row of shell nodes (cpu.rs:48-107): H_c = H_c - k_mu [(dE_v/du) inv_d_u + psi_u
+// - (dE_u/dv) inv_d_v - psi_v], each psi_a updated where the node's slot along a is live. All loads
+// of a node come before its stores.
+__global__ void __launch_bounds__(SHELL_THREADS) k_shell_h(Geom g, ShellRows b, const float* __restrict__ e_in,
                                                            const float* __restrict__ h_in, float* __restrict__ h_out,
                                                            const float* __restrict__ psi_in, float* __restrict__ psi_out,
                                                            float k_mu) {
-    const long long t = (long long)blockIdx.x * SHELL_THREADS + threadIdx.x;
-    if (t >= b.start[b.n]) return;
-    int p[3];
-    shell_node(b, t, p);
-    const long long st[3] = {(long long)g.n1 * g.p2, g.p2, 1};
-    const long long id = ((long long)p[0] * g.n1 + p[1]) * g.p2 + p[2];
-    h_shell_one<0>(g, p, id, st, e_in, h_in, h_out, psi_in, psi_out, k_mu);
-    h_shell_one<1>(g, p, id, st, e_in, h_in, h_out, psi_in, psi_out, k_mu);
-    h_shell_one<2>(g, p, id, st, e_in, h_in, h_out, psi_in, psi_out, k_mu);
+    const unsigned r = blockIdx.x * (SHELL_THREADS / 32) + (threadIdx.x >> 5);
+    if (r >= b.ra + b.rb + b.rc) return;
+    int i, j;
+    bool strips;
+    shell_row(g, b, r, i, j, strips);
+    const int len = strips ? b.za + (g.n2 - b.zb) : g.n2;
+    const AxisNode ai = g.ax[0][i], aj = g.ax[1][j];     // uniform over the warp
+    const bool in_i = i + 1 < g.n0, in_j = j + 1 < g.n1;
+    const long long cs = g.cs;
+    const long long row = ((long long)i * g.n1 + j) * g.p2;
+    const long long si = (long long)g.n1 * g.p2, sj = g.p2;
+    // psi offsets of this row in the x and y slabs (psi_idx, sim.rs:659-665); the z slab per node
+    const long long px = ai.slot_h >= 0 ? ((long long)ai.slot_h * g.n1 + j) * g.n2 : 0;
+    const long long py = aj.slot_h >= 0 ? ((long long)i * (2 * g.pml) + aj.slot_h) * g.n2 : 0;
+    const long long pz = ((long long)i * g.n1 + j) * g.pw;
+    for (int q = int(threadIdx.x & 31); q < len; q += 32) {
+        const int k = strips && q >= b.za ? b.zb + (q - b.za) : q;
+        const AxisNode ak = g.ax[2][k];
+        const bool in_k = k + 1 < g.n2;
+        const long long id = row + k;
+        const bool run0 = in_j && in_k, run1 = in_k && in_i, run2 = in_i && in_j;
+        const float ex = e_in[id], ey = e_in[cs + id], ez = e_in[2 * cs + id];
+        const float ez_j = in_j ? e_in[2 * cs + id + sj] : 0.f, ex_j = in_j ? e_in[id + sj] : 0.f;
+        const float ey_k = in_k ? e_in[cs + id + 1] : 0.f, ex_k = in_k ? e_in[id + 1] : 0.f;
+        const float ez_i = in_i ? e_in[2 * cs + id + si] : 0.f, ey_i = in_i ? e_in[cs + id + si] : 0.f;
+        float hx = h_in[id], hy = h_in[cs + id], hz = h_in[2 * cs + id];
+        // psi of the input set, by (component, axis): Hx (j, k), Hy (k, i), Hz (i, j)
+        const long long o0j = g.psi_off[9 + 0 * 3 + 1] + py + k, o0k = g.psi_off[9 + 0 * 3 + 2] + pz + ak.slot_h;
+        const long long o1k = g.psi_off[9 + 1 * 3 + 2] + pz + ak.slot_h, o1i = g.psi_off[9 + 1 * 3 + 0] + px + k;
+        const long long o2i = g.psi_off[9 + 2 * 3 + 0] + px + k, o2j = g.psi_off[9 + 2 * 3 + 1] + py + k;
+        const bool lj = aj.slot_h >= 0, lk = ak.slot_h >= 0, li = ai.slot_h >= 0;
+        const float s0j = run0 && lj ? psi_in[o0j] : 0.f, s0k = run0 && lk ? psi_in[o0k] : 0.f;
+        const float s1k = run1 && lk ? psi_in[o1k] : 0.f, s1i = run1 && li ? psi_in[o1i] : 0.f;
+        const float s2i = run2 && li ? psi_in[o2i] : 0.f, s2j = run2 && lj ? psi_in[o2j] : 0.f;
+        if (run0) {   // Hx: U = j, V = k
+            const float ev = ez_j - ez, eu = ey_k - ey;
+            float t1 = ev * aj.inv_d, t2 = eu * ak.inv_d;
+            if (lj) { const float rr = cpml_term(aj.bh, s0j, aj.ch, ev, aj.raw_inv_d); psi_out[o0j] = rr; t1 += rr; }
+            if (lk) { const float rr = cpml_term(ak.bh, s0k, ak.ch, eu, ak.raw_inv_d); psi_out[o0k] = rr; t2 += rr; }
+            hx = hx - k_mu * (t1 - t2);
+        }
+        if (run1) {   // Hy: U = k, V = i
+            const float ev = ex_k - ex, eu = ez_i - ez;
+            float t1 = ev * ak.inv_d, t2 = eu * ai.inv_d;
+            if (lk) { const float rr = cpml_term(ak.bh, s1k, ak.ch, ev, ak.raw_inv_d); psi_out[o1k] = rr; t1 += rr; }
+            if (li) { const float rr = cpml_term(ai.bh, s1i, ai.ch, eu, ai.raw_inv_d); psi_out[o1i] = rr; t2 += rr; }
+            hy = hy - k_mu * (t1 - t2);
+        }
+        if (run2) {   // Hz: U = i, V = j
+            const float ev = ey_i - ey, eu = ex_j - ex;
+            float t1 = ev * ai.inv_d, t2 = eu * aj.inv_d;
+            if (li) { const float rr = cpml_term(ai.bh, s2i, ai.ch, ev, ai.raw_inv_d); psi_out[o2i] = rr; t1 += rr; }
+            if (lj) { const float rr = cpml_term(aj.bh, s2j, aj.ch, eu, aj.raw_inv_d); psi_out[o2j] = rr; t2 += rr; }
+            hz = hz - k_mu * (t1 - t2);
+        }
+        h_out[id] = hx;
+        h_out[cs + id] = hy;
+        h_out[2 * cs + id] = hz;
+    }
 }
 
+// The new E of one row of shell nodes (cpu.rs:109-167): E_c = ca E_c + cb [(dH_v/du) inv_dd_u +
+// psi_u - (dH_u/dv) inv_dd_v - psi_v], kept where cb == 0; the E psi slabs are updated in place,
+// so every psi read of a node precedes its writes.
 template <typename CID>
-__global__ void __launch_bounds__(SHELL_THREADS) k_shell_e(Geom g, ShellBoxes b, const CID* __restrict__ node_class,
+__global__ void __launch_bounds__(SHELL_THREADS) k_shell_e(Geom g, ShellRows b, const CID* __restrict__ node_class,
                                                            const DevCoef* __restrict__ classes,
                                                            const float* __restrict__ h, const float* __restrict__ e_in,
                                                            float* __restrict__ e_out, float* __restrict__ psi) {
-    const long long t = (long long)blockIdx.x * SHELL_THREADS + threadIdx.x;
-    if (t >= b.start[b.n]) return;
-    int p[3];
-    shell_node(b, t, p);
-    const long long st[3] = {(long long)g.n1 * g.p2, g.p2, 1};
-    const long long id = ((long long)p[0] * g.n1 + p[1]) * g.p2 + p[2];
-    const DevCoef cf = classes[node_class[id]];
-    e_shell_one<0>(g, p, id, st, cf, h, e_in, e_out, psi);
-    e_shell_one<1>(g, p, id, st, cf, h, e_in, e_out, psi);
-    e_shell_one<2>(g, p, id, st, cf, h, e_in, e_out, psi);
+    const unsigned r = blockIdx.x * (SHELL_THREADS / 32) + (threadIdx.x >> 5);
+    if (r >= b.ra + b.rb + b.rc) return;
+    int i, j;
+    bool strips;
+    shell_row(g, b, r, i, j, strips);
+    const int len = strips ? b.za + (g.n2 - b.zb) : g.n2;
+    const AxisNode ai = g.ax[0][i], aj = g.ax[1][j];
+    const long long cs = g.cs;
+    const long long row = ((long long)i * g.n1 + j) * g.p2;
+    const long long si = (long long)g.n1 * g.p2, sj = g.p2;
+    const long long px = ai.slot_e >= 0 ? ((long long)ai.slot_e * g.n1 + j) * g.n2 : 0;
+    const long long py = aj.slot_e >= 0 ? ((long long)i * (2 * g.pml) + aj.slot_e) * g.n2 : 0;
+    const long long pz = ((long long)i * g.n1 + j) * g.pw;
+    for (int q = int(threadIdx.x & 31); q < len; q += 32) {
+        const int k = strips && q >= b.za ? b.zb + (q - b.za) : q;
+        const AxisNode ak = g.ax[2][k];
+        const long long id = row + k;
+        const DevCoef cf = classes[node_class[id]];
+        const bool run0 = cf.cb[0] != 0.0f && j > 0 && k > 0;
+        const bool run1 = cf.cb[1] != 0.0f && k > 0 && i > 0;
+        const bool run2 = cf.cb[2] != 0.0f && i > 0 && j > 0;
+        const float hx = h[id], hy = h[cs + id], hz = h[2 * cs + id];
+        const float hz_j = j > 0 ? h[2 * cs + id - sj] : 0.f, hx_j = j > 0 ? h[id - sj] : 0.f;
+        const float hy_k = k > 0 ? h[cs + id - 1] : 0.f, hx_k = k > 0 ? h[id - 1] : 0.f;
+        const float hz_i = i > 0 ? h[2 * cs + id - si] : 0.f, hy_i = i > 0 ? h[cs + id - si] : 0.f;
+        float ex = e_in[id], ey = e_in[cs + id], ez = e_in[2 * cs + id];
+        const long long o0j = g.psi_off[0 * 3 + 1] + py + k, o0k = g.psi_off[0 * 3 + 2] + pz + ak.slot_e;
+        const long long o1k = g.psi_off[1 * 3 + 2] + pz + ak.slot_e, o1i = g.psi_off[1 * 3 + 0] + px + k;
+        const long long o2i = g.psi_off[2 * 3 + 0] + px + k, o2j = g.psi_off[2 * 3 + 1] + py + k;
+        const bool lj = aj.slot_e >= 0, lk = ak.slot_e >= 0, li = ai.slot_e >= 0;
+        const float s0j = run0 && lj ? psi[o0j] : 0.f, s0k = run0 && lk ? psi[o0k] : 0.f;
+        const float s1k = run1 && lk ? psi[o1k] : 0.f, s1i = run1 && li ? psi[o1i] : 0.f;
+        const float s2i = run2 && li ? psi[o2i] : 0.f, s2j = run2 && lj ? psi[o2j] : 0.f;
+        if (run0) {   // Ex: U = j, V = k
+            const float hv = hz - hz_j, hu = hy - hy_k;
+            float t1 = hv * aj.inv_dd, t2 = hu * ak.inv_dd;
+            if (lj) { const float rr = cpml_term(aj.be, s0j, aj.ce, hv, aj.raw_inv_dd); psi[o0j] = rr; t1 += rr; }
+            if (lk) { const float rr = cpml_term(ak.be, s0k, ak.ce, hu, ak.raw_inv_dd); psi[o0k] = rr; t2 += rr; }
+            ex = cf.ca[0] * ex + cf.cb[0] * (t1 - t2);
+        }
+        if (run1) {   // Ey: U = k, V = i
+            const float hv = hx - hx_k, hu = hz - hz_i;
+            float t1 = hv * ak.inv_dd, t2 = hu * ai.inv_dd;
+            if (lk) { const float rr = cpml_term(ak.be, s1k, ak.ce, hv, ak.raw_inv_dd); psi[o1k] = rr; t1 += rr; }
+            if (li) { const float rr = cpml_term(ai.be, s1i, ai.ce, hu, ai.raw_inv_dd); psi[o1i] = rr; t2 += rr; }
+            ey = cf.ca[1] * ey + cf.cb[1] * (t1 - t2);
+        }
+        if (run2) {   // Ez: U = i, V = j
+            const float hv = hy - hy_i, hu = hx - hx_j;
+            float t1 = hv * ai.inv_dd, t2 = hu * aj.inv_dd;
+            if (li) { const float rr = cpml_term(ai.be, s2i, ai.ce, hv, ai.raw_inv_dd); psi[o2i] = rr; t1 += rr; }
+            if (lj) { const float rr = cpml_term(aj.be, s2j, aj.ce, hu, aj.raw_inv_dd); psi[o2j] = rr; t2 += rr; }
+            ez = cf.ca[2] * ez + cf.cb[2] * (t1 - t2);
+        }
+        e_out[id] = ex;
+        e_out[cs + id] = ey;
+        e_out[2 * cs + id] = ez;
+    }
 }
 
 }  // namespace fg

@@ -5,7 +5,7 @@
 // cp.async.bulk.tensor (4-D maps over (k, j, i, component)):
 //   E(p)     rows j0-1 .. j0+TJ,   columns k0-4 .. k0+TK+3 (all 3 components)
 //   H_in(p)  rows j0-1 .. j0+TJ-1, columns k0-4 .. k0+TK-1 (all 3 components)
-//   class(p) rows j0   .. j0+TJ-1, columns k0   .. k0+TK-1 (the node class ids)
+//   class(p) rows j0   .. j0+TJ-1, columns from k0 rounded down to 16 (the node class ids)
 // Box origins in k are rounded down to 16 bytes; rows or planes outside the grid arrive as zeros.
 // Eight consumer warps then, per plane i:
 //   1. form the new H on the tile and on its j-1 row and k-1 column (the halo the E update needs;
@@ -112,7 +112,7 @@ template <int TJ, int TK, typename CID, int STAGES, int SEGMAX, bool LOCAL = fal
 struct TmaLayout {
     static constexpr int EW = TK + 8, ER = TJ + 2;   // E box: columns k0-4 .. k0+TK+3, rows j0-1 .. j0+TJ
     static constexpr int HW = TK + 8, HR = TJ + 1;   // H box: columns k0-4 .. k0+TK+3, rows j0-1 .. j0+TJ-1
-    static constexpr int CW = TK + 16, CR = TJ;      // class box: columns k0 .. k0+TK+15, rows j0 .. j0+TJ-1
+    static constexpr int CW = TK + 16, CR = TJ;      // class box: columns (k0 & ~15) + 0 .. 79, rows j0 .. j0+TJ-1
     static constexpr int NW = TK + 4, NR = TJ + 1;   // new-H tile: column k at k-k0+2, row j at j-j0+1
     static constexpr int E_BYTES = 3 * ER * EW * 4;
     static constexpr int H_BYTES = 3 * HR * HW * 4;
@@ -134,7 +134,7 @@ struct TmaArgs {
     float* __restrict__ e_out;
     float* __restrict__ h_out;
     float k_mu;
-    int jend, kend;                      // the clean box ends: rows < jend, columns < kend are owned
+    int kbeg, jend, kend;                // the clean box: rows < jend, columns kbeg .. kend-1 are owned
     const int4* blocks;                  // per block: (k0, j0, i0, i1) of its tile and x-segment
     const float* tables;                 // LOCAL: per block (entry of `blocks`), LOCAL_CLASSES x (ca[3], cb[3])
     unsigned* counter;
@@ -216,8 +216,8 @@ __device__ __forceinline__ CoefRef coef_of(const TmaArgs& a, const float* lt, un
 // row j0 - 1), each lane a pair of columns k0 + 2 lane, +1. Warp 0 lanes 0..TJ-1 also take the
 // halo column k0 - 1, lanes TJ..2TJ-1 the column k0 + TK when the tile owns it (a clean box
 // reaching the end of a grid whose node count along k is 64t + 1). Points past jend / kend are
-// computed when they exist in the grid but never written; kend - k0 is even unless kend = n2,
-// so a column pair is owned whole.
+// computed when they exist in the grid but never written, and so are the first tile's columns
+// below kbeg; kbeg and kend are even (unless kend = n2), so a column pair is owned whole.
 template <int TJ, int TK, typename CID, int STAGES, int SEGMAX, bool LOCAL, int MINB>
 __global__ void __launch_bounds__(TMA_CONSUMERS + 32, MINB)
     k_tma_step(const __grid_constant__ CUtensorMap map_e, const __grid_constant__ CUtensorMap map_h,
@@ -282,7 +282,7 @@ __global__ void __launch_bounds__(TMA_CONSUMERS + 32, MINB)
             tma::mbar_expect_tx(&full[s], L::TX);
             tma::load_4d(st, &map_e, &full[s], k0 - 4, j0 - 1, p, 0);
             tma::load_4d(st + L::al(L::E_BYTES), &map_h, &full[s], k0 - 4, j0 - 1, p, 0);
-            tma::load_3d(st + L::al(L::E_BYTES) + L::al(L::H_BYTES), &map_c, &full[s], k0, j0, p);
+            tma::load_3d(st + L::al(L::E_BYTES) + L::al(L::H_BYTES), &map_c, &full[s], k0 & ~15, j0, p);
         }
         return;
     }
@@ -295,7 +295,7 @@ __global__ void __launch_bounds__(TMA_CONSUMERS + 32, MINB)
     const int jj = j0 + r, kk = k0 + c;
     const bool row_live = jj >= 0 && jj < g.n1;
     const bool live0 = row_live && kk < g.n2, live1 = row_live && kk + 1 < g.n2;
-    const bool own_row = r >= 0 && jj < a.jend && kk < a.kend;   // the pair is written
+    const bool own_row = r >= 0 && jj < a.jend && kk >= a.kbeg && kk < a.kend;   // the pair is written
     const AxisNode* rj = axj + (r + 1);
     const PtAxes q0{rj, axk + (c + 1), jj + 1 < g.n1, kk + 1 < g.n2};
     const PtAxes q1{rj, axk + (c + 2), jj + 1 < g.n1, kk + 2 < g.n2};
@@ -324,7 +324,9 @@ __global__ void __launch_bounds__(TMA_CONSUMERS + 32, MINB)
         const float* E = reinterpret_cast<const float*>(stages + s * L::STAGE);
         const float* E1 = reinterpret_cast<const float*>(stages + s1 * L::STAGE);
         const float* H = reinterpret_cast<const float*>(stages + s * L::STAGE + L::al(L::E_BYTES));
-        const CID* CL = reinterpret_cast<const CID*>(stages + s * L::STAGE + L::al(L::E_BYTES) + L::al(L::H_BYTES));
+        // the class box starts at k0 rounded down to 16 ids: column k sits at k - k0 + (k0 & 15)
+        const CID* CL = reinterpret_cast<const CID*>(stages + s * L::STAGE + L::al(L::E_BYTES) + L::al(L::H_BYTES)) +
+                        (k0 & 15);
         float* hn = hn_all + (u & 1) * (L::HN / 4);
         const int i = p;
         const AxisNode& ai = axi[u];

@@ -234,11 +234,16 @@ def test_the_pipelines_are_the_cuda_kernels(gpu):
     assert s.launches_per_step >= 4
     assert s.stream != 0
     s.close()
-    # too small for a clean box: the direct-load fused march does the whole step
-    sc = W.dielectric_box(16, pml=3, steps=4)
-    s = fdtd.Session(gpu, fdtd.Sim.try_new(*sc.args()), 0, sc.pulse, sc.extras)
+    # 11 nodes with a 4-cell CPML leave no clean box (along k it would start at node 8): the
+    # direct-load fused march does the whole step, and agrees with the oracle
+    sc = W.spheres(10, pml=4, count=2, rmin=1, rmax=2, steps=30, fused=True)
+    sim = fdtd.Sim.try_new(*sc.args())
+    s = fdtd.Session(gpu, sim, 0, sc.pulse, sc.extras)
     assert "fused" in s.variant and "TMA" not in s.variant, s.variant
     s.close()
+    rec = fdtd.run(gpu, sim, 0, sc.pulse, sc.extras)
+    ref = O.run_cpu(O.OracleSim(*sc.args(), bits=32), 0, sc.pulse, sc.extras)
+    assert rel_l2(rec.series, ref.series) <= 1e-4
 
 
 def test_the_tma_step_and_the_direct_march_agree_bit_for_bit(gpu, monkeypatch):

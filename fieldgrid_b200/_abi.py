@@ -86,6 +86,18 @@ class fg_extras(C.Structure):
 PROGRESS_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, u64, dbl)
 
 
+class fg_flux_spec(C.Structure):
+    _fields_ = [("design_lo", C.c_uint64 * 3), ("design_hi", C.c_uint64 * 3), ("plane_k", C.c_uint64),
+                ("window_lo", C.c_uint64 * 2), ("window_hi", C.c_uint64 * 2), ("freq", C.c_double),
+                ("steps", C.c_uint64), ("checkpoints", C.c_uint64)]
+
+
+class fg_flux_result(C.Structure):
+    _fields_ = [("objective", C.c_double), ("flux_re", C.c_double), ("flux_im", C.c_double),
+                ("forward_ms", C.c_double), ("recompute_ms", C.c_double), ("adjoint_ms", C.c_double),
+                ("segments", C.c_uint64), ("segment_len", C.c_uint64), ("design_edges", C.c_uint64)]
+
+
 def _ptr(arr: np.ndarray | None, ctype):
     if arr is None:
         return C.cast(None, P(ctype))

@@ -84,6 +84,8 @@ def _declare(L):
         "fg_far_field": (C.c_int, [vp, vp, P(dbl), u64, P(dbl)]),
         "fg_far_intensity": (C.c_int, [vp, vp, P(dbl), u64, P(dbl)]),
         "fg_far_radiated": (C.c_int, [vp, vp, u64, P(dbl), P(dbl)]),
+        "fg_flux_gradient": (C.c_int, [vp, vp, u64, P(A.fg_pulse), P(A.fg_flux_spec), P(A.fg_flux_result), P(dbl),
+                                       P(dbl), cp, sz]),
         "fg_energy_noalloc": (C.c_int, [vp, vp, u64, vp, vp]),
     }
     for name, (res, args) in sig.items():

@@ -486,4 +486,47 @@ int fg_far_radiated(fg_gpu* g, const fg_far* f, uint64_t steps, double* total, d
     return FG_OK;
 }
 
+int fg_flux_gradient(fg_gpu* g, const fg_sim* sim, uint64_t driven, const fg_pulse* pulse, const fg_flux_spec* spec,
+                     fg_flux_result* out, double* grad_eps, double* grad_sigma, char* err, size_t errlen) {
+    if (!g) return fail(FG_ERR_NO_DEVICE, "no GPU: this engine has no CPU path", err, errlen);
+    if (!sim || !pulse || !spec || !out) return fail(FG_ERR_INVALID, "null argument", err, errlen);
+    if ((grad_eps == nullptr) != (grad_sigma == nullptr))
+        return fail(FG_ERR_INVALID, "grad_eps and grad_sigma are both given or both NULL", err, errlen);
+    const HostSim& hs = *sim->s;
+    FluxSpec sp;
+    for (int a = 0; a < 3; ++a) { sp.lo[a] = spec->design_lo[a]; sp.hi[a] = spec->design_hi[a]; }
+    sp.plane_k = spec->plane_k;
+    for (int a = 0; a < 2; ++a) {
+        sp.win_lo[a] = spec->window_lo[a];
+        sp.win_hi[a] = spec->window_hi[a];
+    }
+    if (sp.win_hi[0] == 0 && sp.win_hi[1] == 0)
+        for (int a = 0; a < 2; ++a) {
+            sp.win_lo[a] = hs.pml;
+            sp.win_hi[a] = hs.n[a] > hs.pml ? hs.n[a] - hs.pml : 0;
+        }
+    sp.freq = spec->freq;
+    sp.steps = spec->steps;
+    sp.checkpoints = spec->checkpoints;
+    FluxResult r;
+    std::string e;
+    const bool want = grad_eps != nullptr;
+    int rc = flux_gradient(g->g, hs, driven, pulse->f0, pulse->fc, sp, want, r, e);
+    if (rc) return fail(rc, e, err, errlen);
+    out->objective = r.J;
+    out->flux_re = r.f_re;
+    out->flux_im = r.f_im;
+    out->forward_ms = r.forward_ms;
+    out->recompute_ms = r.recompute_ms;
+    out->adjoint_ms = r.adjoint_ms;
+    out->segments = r.segments;
+    out->segment_len = r.segment_len;
+    out->design_edges = r.design_edges;
+    if (want) {
+        std::copy(r.g_eps.begin(), r.g_eps.end(), grad_eps);
+        std::copy(r.g_sig.begin(), r.g_sig.end(), grad_sigma);
+    }
+    return FG_OK;
+}
+
 }  // extern "C"

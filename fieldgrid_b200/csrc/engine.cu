@@ -20,6 +20,7 @@
 #include "stencil_separate.cuh"
 #include "stencil_shell.cuh"
 #include "stencil_tma.cuh"
+#include "adjoint_kernels.cuh"
 
 #include <cudaTypedefs.h>
 
@@ -101,6 +102,12 @@ struct Session {
     std::vector<int4> tma_plan_blocks;  // the same list on the host
     int clean_lo[3] = {0, 0, 0}, clean_hi[3] = {0, 0, 0};
     ShellRows shell{};              // the CPML shell around the clean box
+    // adjoint support: the design edges and the ring of their recorded E^n and curl terms
+    int n_design = 0;
+    int4* design = nullptr;
+    float *hist_e = nullptr, *hist_s = nullptr;
+    int hist_cap = 0;
+    long long* hist_base = nullptr;
     float* tables = nullptr;        // per block region: LOCAL_CLASSES x (ca[3], cb[3])
     bool local = false;
     // counts
@@ -474,6 +481,11 @@ int enqueue_step(Session& s, int parity, std::string& err) {
     }
     if (s.ntff_len) mark("ntff");
     if (s.ntff_len) k_ntff<<<(s.n_patches + 127) / 128, 128, 0, st>>>(s.patch, s.n_patches, g.cs, s.sc, s.counter, e_now, h_now, s.ntff);
+    if (s.n_design && s.fused) {
+        mark("design_record");
+        k_design_record<<<(s.n_design + 127) / 128, 128, 0, st>>>(g, s.design, s.n_design, e_in, h_now, s.psi, s.counter,
+                                                                   s.hist_base, s.hist_cap, s.hist_e, s.hist_s);
+    }
     mark(nullptr);
     return FG_OK;
 }
@@ -489,6 +501,7 @@ uint64_t count_launches(const Session& s) {
     if (s.n_ports) n++;
     if (s.plane_len) n++;
     if (s.ntff_len) n++;
+    if (s.n_design && s.fused) n++;
     return n;
 }
 
@@ -884,6 +897,18 @@ int session_new(Gpu* gpu, const HostSim& sim, const RunSpec& rs, Session** out, 
     if (rc) return FG_ERR_CUDA;
     FG_CUDA(cudaStreamSynchronize(st));
 
+    if (rs.design && !rs.design->empty()) {
+        if (!s->fused) { err = "design recording needs the fused step"; return FG_ERR_INVALID; }
+        s->n_design = int(rs.design->size());
+        s->hist_cap = std::max(rs.hist_cap, 1);
+        const size_t hb = size_t(s->hist_cap) * size_t(s->n_design) * 4;
+        FG_CUDA(cudaMalloc(&s->design, rs.design->size() * sizeof(int4)));
+        FG_CUDA(cudaMalloc(&s->hist_e, hb));
+        FG_CUDA(cudaMalloc(&s->hist_s, hb));
+        FG_CUDA(cudaMalloc(&s->hist_base, sizeof(long long)));
+        FG_CUDA(cudaMemcpy(s->design, rs.design->data(), rs.design->size() * sizeof(int4), cudaMemcpyHostToDevice));
+        FG_CUDA(cudaMemset(s->hist_base, 0, sizeof(long long)));
+    }
     s->shape = choose_shape(g, s->cid_bytes, s->n_wires > 0);
     plan_tma(*s);
     if (s->tma.ok)
@@ -917,6 +942,10 @@ void session_free(Session* s) {
     for (auto& gx : s->graph_one)
         if (gx) cudaGraphExecDestroy(gx);
     if (s->arena) cudaFree(s->arena);
+    cudaFree(s->design);
+    cudaFree(s->hist_e);
+    cudaFree(s->hist_s);
+    cudaFree(s->hist_base);
     if (s->stream) cudaStreamDestroy(s->stream);
     delete s;
 }
@@ -1077,3 +1106,5 @@ uint64_t session_h2d_bytes(const Session* s) { return s->h2d_bytes; }
 uint64_t session_d2h_bytes(const Session* s) { return s->d2h_bytes; }
 
 }  // namespace fg
+
+#include "adjoint.cuh"

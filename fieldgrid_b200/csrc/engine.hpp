@@ -5,6 +5,8 @@
 #include <string>
 #include <vector>
 
+#include <vector_types.h>
+
 #include "host.hpp"
 
 namespace fg {
@@ -20,6 +22,10 @@ struct RunSpec {               // pack() inputs that are not part of the Sim (ru
     std::vector<uint32_t> ntff;
     bool fused = true;          // the fused E+H march; false = the separate H and E kernels
     bool profile = false;
+    // adjoint support: E edges (comp, i, j, k) whose E^n and curl term every fused step records
+    // into a ring of hist_cap slots (slot = step - base)
+    const std::vector<int4>* design = nullptr;
+    int hist_cap = 0;
 };
 
 struct Session;
@@ -57,5 +63,26 @@ int far_field_gpu(Gpu* g, const double* pos, const double* area, const double* j
                   const double* dirs, uint64_t n, double* out, std::string& err);
 
 int sim_try_new(const struct fg_sim_spec* spec, HostSim** out, std::string& err);
+
+// The flux objective J = |F|^2 on a z-plane window at one frequency and, when want_grad, its
+// gradient over the permittivity and conductivity of a design box of voxels (adjoint.cuh).
+struct FluxSpec {
+    uint64_t lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};   // design cells [lo, hi)
+    uint64_t plane_k = 0;
+    uint64_t win_lo[2] = {0, 0}, win_hi[2] = {0, 0};  // (i, j) nodes of the flux sum
+    double freq = 0;
+    uint64_t steps = 0;
+    uint64_t checkpoints = 0;                          // 0: keep every step's design history
+};
+
+struct FluxResult {
+    double J = 0, f_re = 0, f_im = 0;
+    double forward_ms = 0, recompute_ms = 0, adjoint_ms = 0;
+    uint64_t segments = 0, segment_len = 0, design_edges = 0;
+    std::vector<double> g_eps, g_sig;   // per design cell, k fastest
+};
+
+int flux_gradient(Gpu* gpu, const HostSim& sim, uint64_t driven, double f0, double fc, const FluxSpec& sp,
+                  bool want_grad, FluxResult& res, std::string& err);
 
 }  // namespace fg

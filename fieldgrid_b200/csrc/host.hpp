@@ -105,6 +105,7 @@ struct HostSim {
     std::vector<std::pair<double, double>> poles;
     std::vector<DebyeEdge> debye_edges;
     std::vector<WireH> wires;
+    std::vector<float> cell_eps, cell_sig;   // per cell as given (empty: the defaults 1 and 0)
 
     size_t cells() const { return (n[0] - 1) * (n[1] - 1) * (n[2] - 1); }
     size_t idx(size_t i, size_t j, size_t k) const { return (i * n[1] + j) * n[2] + k; }

@@ -181,6 +181,8 @@ int sim_try_new(const fg_sim_spec* spec, HostSim** out, std::string& err) {
     const float* m_sig = spec->sigma;
     const float* m_inf = spec->inf;
     const float* m_dd = spec->debye;
+    if (m_eps) S.cell_eps.assign(m_eps, m_eps + cells);
+    if (m_sig) S.cell_sig.assign(m_sig, m_sig + cells);
     auto mat = [&](size_t ci, size_t cj, size_t ck, double out4[4]) {
         size_t id = (ci * (n[1] - 1) + cj) * (n[2] - 1) + ck;
         out4[0] = m_eps ? double(m_eps[id]) : 1.0;

@@ -557,3 +557,79 @@ class Far:
         if code:
             raise FdtdError(lib().fg_last_error().decode(), code)
         return t.value, p.value
+
+
+# ---- adjoint (no counterpart in the reference) ----
+
+@dataclass
+class FluxSpec:
+    """The flux objective J = |F|^2, F = sum over the (i, j) window of z-plane `plane_k` of
+    dA (Ex^ conj(Hy^) - Ey^ conj(Hx^)) at `freq`, and the design box of cells [lo, hi) whose
+    relative permittivity and conductivity the gradient is over. `window` None: the nodes inside
+    the CPML. `checkpoints` 0 keeps every step's design-edge history; c > 0 keeps about c field
+    checkpoints and re-runs each segment in the backward sweep."""
+    design_lo: tuple
+    design_hi: tuple
+    plane_k: int
+    freq: float
+    steps: int
+    window: Optional[tuple] = None   # ((i0, j0), (i1, j1))
+    checkpoints: int = 0
+
+    def struct(self) -> A.fg_flux_spec:
+        s = A.fg_flux_spec()
+        s.design_lo[:] = [int(v) for v in self.design_lo]
+        s.design_hi[:] = [int(v) for v in self.design_hi]
+        s.plane_k = int(self.plane_k)
+        if self.window is not None:
+            s.window_lo[:] = [int(v) for v in self.window[0]]
+            s.window_hi[:] = [int(v) for v in self.window[1]]
+        s.freq = float(self.freq)
+        s.steps = int(self.steps)
+        s.checkpoints = int(self.checkpoints)
+        return s
+
+    def cells(self) -> int:
+        return int(np.prod([h - l for l, h in zip(self.design_lo, self.design_hi)]))
+
+    def shape(self) -> tuple:
+        return tuple(int(h - l) for l, h in zip(self.design_lo, self.design_hi))
+
+
+@dataclass
+class FluxResult:
+    objective: float
+    flux: complex
+    grad_eps: Optional[np.ndarray]     # dJ / d eps_r per design cell, shaped like the box
+    grad_sigma: Optional[np.ndarray]   # dJ / d sigma (S/m)
+    forward_ms: float
+    recompute_ms: float
+    adjoint_ms: float
+    segments: int
+    segment_len: int
+    design_edges: int
+
+
+def flux_gradient(g, sim: Sim, driven: int, pulse: Pulse, spec: FluxSpec, grad: bool = True) -> FluxResult:
+    """The flux objective and, with `grad`, its gradient over the design box (a discrete adjoint of
+    the f32 update on the device: one forward run and one backward sweep)."""
+    if g is None:
+        raise FdtdError("no GPU: this engine has no CPU path", 3)
+    L = lib()
+    pl = A.pulse_struct(pulse)
+    st = spec.struct()
+    out = A.fg_flux_result()
+    n = spec.cells()
+    ge = np.zeros(n, np.float64) if grad else None
+    gs = np.zeros(n, np.float64) if grad else None
+    P = C.POINTER(C.c_double)
+    err = C.create_string_buffer(ERRLEN)
+    code = L.fg_flux_gradient(g._h, sim._h, driven, C.byref(pl), C.byref(st), C.byref(out),
+                              None if ge is None else ge.ctypes.data_as(P),
+                              None if gs is None else gs.ctypes.data_as(P), err, ERRLEN)
+    _check(code, err)
+    shp = spec.shape()
+    return FluxResult(out.objective, complex(out.flux_re, out.flux_im),
+                      None if ge is None else ge.reshape(shp), None if gs is None else gs.reshape(shp),
+                      out.forward_ms, out.recompute_ms, out.adjoint_ms, int(out.segments), int(out.segment_len),
+                      int(out.design_edges))

@@ -262,3 +262,41 @@ def wire_cavity(radius: float, steps: int = 40000) -> Scene:
     extras = Extras(max_steps=steps, decay_db=math.inf)
     return Scene(f"wire cavity r={radius}", grid, Materials.new(grid), None, [], [port], [], Media(wires=wires),
                  Pulse(3.0e9, 2.5e9), extras)
+
+
+def flux_design(nx: int = 160, ny: int = 160, nz: int = 96, dx: float = 1e-3, pml: int = 8,
+                design: tuple = (32, 32, 8), steps: int = 4000, checkpoints: int = 64, seed: int = 4,
+                freq: float = 10e9):
+    """Adjoint workload: an nx x ny x nz vacuum grid with a 50-ohm z-port source below a design
+    block of per-voxel eps_r ~ U[1, 12] and sigma ~ U[0, 0.01] S/m (seed), and the flux objective
+    |F|^2 at `freq` on a z-plane above it. Returns (scene, spec, eps0, sig0): the scene built with
+    the initial design, the FluxSpec, and the design arrays (shaped like the block)."""
+    from .fdtd import FluxSpec
+    grid = Grid.uniform((0.0, 0.0, 0.0), (nx * dx, ny * dx, nz * dx), (nx, ny, nz), pml)
+    rng = SplitMix64(seed)
+    dw = tuple(int(v) for v in design)
+    cnt = dw[0] * dw[1] * dw[2]
+    eps0 = np.array([rng.uniform(1.0, 12.0) for _ in range(cnt)], np.float32).reshape(dw)
+    sig0 = np.array([rng.uniform(0.0, 0.01) for _ in range(cnt)], np.float32).reshape(dw)
+    ks = pml + max(2, nz // 8)                       # source node height
+    kd = ks + max(2, nz // 8)                        # design block bottom cell
+    kp = min(kd + dw[2] + max(2, nz // 8), nz - pml - 2)   # flux plane
+    lo = (nx // 2 - dw[0] // 2, ny // 2 - dw[1] // 2, kd)
+    hi = (lo[0] + dw[0], lo[1] + dw[1], lo[2] + dw[2])
+    ports = [PortDef("source", [[Edge(2, (nx // 2, ny // 2, ks))]], 50.0, False)]
+    extras = Extras(max_steps=steps, decay_db=math.inf, fused_e=True, check_every=min(steps, 1000) or 1000,
+                    freqs=[freq], plane_k=kp)
+    spec = FluxSpec(design_lo=lo, design_hi=hi, plane_k=kp, freq=freq, steps=steps, checkpoints=checkpoints)
+
+    def scene(eps=eps0, sig=sig0) -> Scene:
+        mats = Materials.new(grid)
+        e = mats.eps.reshape(nx, ny, nz)
+        s = mats.sigma.reshape(nx, ny, nz)
+        e[lo[0]:hi[0], lo[1]:hi[1], lo[2]:hi[2]] = np.asarray(eps, np.float32)
+        s[lo[0]:hi[0], lo[1]:hi[1], lo[2]:hi[2]] = np.asarray(sig, np.float32)
+        sc = Scene(f"flux design {nx}x{ny}x{nz}, block {dw[0]}x{dw[1]}x{dw[2]}", grid, mats, None, [], ports, [],
+                   Media(), Pulse(freq, freq / 2), extras)
+        sc.info.update(dx=dx, pml=pml, design=dw, plane_k=kp)
+        return sc
+
+    return scene, spec, eps0, sig0

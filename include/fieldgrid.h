@@ -260,6 +260,39 @@ int fg_far_intensity(fg_gpu* g, const fg_far* f, const double* dirs, uint64_t n,
 /* Far::radiated (ntff.rs:122-136): total radiated power and peak intensity. */
 int fg_far_radiated(fg_gpu* g, const fg_far* f, uint64_t steps, double* total, double* peak);
 
+/* ---- adjoint: the gradient of a flux objective over a box of design voxels ----
+ * No counterpart in the reference (sims_field::fdtd has no adjoint). The objective is
+ * J = |F|^2, F = sum over the (i, j) window of the z-plane plane_k of
+ * dA (Ex^ conj(Hy^) - Ey^ conj(Hx^)), with Ex^..Hy^ the running DFT at `freq` that run() keeps for
+ * Extras.plane_k (cpu.rs:336-361) and dA = dd_x(i) dd_y(j). The gradient is over the relative
+ * permittivity and the conductivity of every cell of the design box (the Materials arrays),
+ * exact for the f32 update as the device runs it (a discrete adjoint), from one forward run on the
+ * fused step and one backward sweep. checkpoints = 0 keeps each step's E and curl term on the
+ * design edges; checkpoints = c keeps the full field state at the start of about c segments and
+ * re-runs each segment before sweeping it (sqrt(steps) checkpoints: segment recomputation).
+ * The design box must stay off the grid boundary and off PEC, lumped, port and Debye edges; the
+ * Sim must hold no Debye media, inductors, thin wires or resistive sheets. */
+typedef struct fg_flux_spec {
+    uint64_t design_lo[3], design_hi[3];  /* design cells [lo, hi), cell indices as in Materials */
+    uint64_t plane_k;                     /* node index of the flux plane along z */
+    uint64_t window_lo[2], window_hi[2];  /* (i, j) nodes summed; window_hi {0, 0}: those inside the CPML */
+    double freq;                          /* Hz */
+    uint64_t steps;
+    uint64_t checkpoints;
+} fg_flux_spec;
+
+typedef struct fg_flux_result {
+    double objective, flux_re, flux_im;   /* J, and F */
+    double forward_ms, recompute_ms, adjoint_ms;
+    uint64_t segments, segment_len, design_edges;
+} fg_flux_result;
+
+/* grad_eps, grad_sigma: one entry per design cell, (i, j, k) order with k fastest; both NULL to
+ * compute the objective alone. */
+int fg_flux_gradient(fg_gpu* g, const fg_sim* sim, uint64_t driven, const fg_pulse* pulse,
+                     const fg_flux_spec* spec, fg_flux_result* out, double* grad_eps, double* grad_sigma,
+                     char* err, size_t errlen);
+
 #ifdef __cplusplus
 }
 #endif

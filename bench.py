@@ -51,6 +51,10 @@ def parse():
     p.add_argument("--cpu-steps", type=int, default=8, help="full time steps the CPU baseline times")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--workload", choices=["throughput", "adjoint"], default="throughput",
+                   help="throughput: the 512^3 spheres step (the headline); adjoint: the flux-objective "
+                        "gradient over a 32x32x8 design block on 160x160x96 cells, 4000 steps")
+    p.add_argument("--checkpoints", type=int, default=64, help="adjoint: field checkpoints (0: keep the history)")
     return p.parse_args()
 
 
@@ -185,10 +189,70 @@ def cpu_baseline(args, sc):
                       f"C++ restatement of the reference's CPU FDTD (cpu.rs), OpenMP over x-planes"}
 
 
+def run_adjoint(args):
+    """The adjoint workload: time of the gradient (forward with checkpoints + segment recomputation
+    + backward sweep) over the time of a plain forward of the same run, device-timed per phase, and
+    wall-clock through the public call (fdtd.flux_gradient) with host buffers."""
+    import numpy as np
+    import torch
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    from fieldgrid_b200 import fdtd
+    from fieldgrid_b200 import workloads as W
+    from fieldgrid_b200.gpu import Gpu, Options
+    g = Gpu.open(Options(device=torch.cuda.current_device()))
+    scene, spec, _, _ = W.flux_design(steps=args.steps if args.steps != 2000 else 4000, checkpoints=args.checkpoints)
+    sc = scene()
+    sim = fdtd.Sim.try_new(*sc.args())
+    fwd, grad = [], []
+    sampler = None
+    for rep in range(max(args.warmup, 3) + 3):
+        timed = rep >= max(args.warmup, 3)
+        if timed and sampler is None:
+            sampler = ClockSampler(device_id(int(os.environ.get("LOCAL_RANK", "0"))))
+        t = time.perf_counter()
+        f = fdtd.flux_gradient(g, sim, 0, sc.pulse, spec, grad=False)
+        tf = time.perf_counter() - t
+        t = time.perf_counter()
+        r = fdtd.flux_gradient(g, sim, 0, sc.pulse, spec, grad=True)
+        tg = time.perf_counter() - t
+        if timed:
+            fwd.append((tf, f.forward_ms))
+            grad.append((tg, r))
+    clocks = sampler.stop()
+    if rank != 0:
+        return 0
+    dev_f = float(np.median([x[1] for x in fwd]))
+    dev_g = float(np.median([x[1].forward_ms + x[1].recompute_ms + x[1].adjoint_ms for x in grad]))
+    wall_f = float(np.median([x[0] for x in fwd]))
+    wall_g = float(np.median([x[0] for x in grad]))
+    r = grad[-1][1]
+    line = {
+        "metric": "adjoint grad time / forward", "value": dev_g / dev_f, "unit": "x", "n_gpus": world,
+        "steps": spec.steps, "warmup": max(args.warmup, 3), "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": sc.name, "cells": [160, 160, 96], "design_cells": spec.cells(),
+                   "parameters": 2 * spec.cells(), "checkpoints": args.checkpoints, "segments": r.segments,
+                   "segment_len": r.segment_len, "design_edges": r.design_edges, "freq_hz": spec.freq},
+        "forward_ms": dev_f, "gradient_ms": dev_g,
+        "gradient_parts_ms": {"forward": r.forward_ms, "recompute": r.recompute_ms, "adjoint": r.adjoint_ms},
+        "e2e": {"value": wall_g / wall_f, "unit": "x", "forward_s": wall_f, "gradient_s": wall_g,
+                "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0,
+                "run": "fdtd.flux_gradient wall clock: setup of the session, the steps, read-back of the plane and "
+                       "the gradient"},
+        "objective": r.objective, "clocks": clocks,
+    }
+    print(json.dumps(line))
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "adjoint":
+        return run_adjoint(args)
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))

@@ -162,12 +162,18 @@ int flux_gradient(Gpu* gpu, const HostSim& sim, uint64_t driven, double f0, doub
     const size_t fbytes = size_t(3 * g.cs) * 4, pbytes = size_t(std::max<long long>(s->psi_total, 1)) * 4;
     struct Ck { float *e = nullptr, *h = nullptr, *psi = nullptr; };
     std::vector<Ck> cks;
-    auto free_cks = [&] {
-        for (auto& c : cks) { cudaFree(c.e); cudaFree(c.h); cudaFree(c.psi); }
-        cks.clear();
-    };
-    std::unique_ptr<void, std::function<void(void*)>> ck_guard((void*)1, [&](void*) { free_cks(); });
+    char* ck_mem = nullptr;   // all checkpoints in one allocation
+    std::unique_ptr<void, std::function<void(void*)>> ck_guard((void*)1, [&](void*) { cudaFree(ck_mem); });
     const bool ckpt = want_grad && S > 1;
+    if (ckpt) {
+        const size_t per = carve_size(fbytes) * 2 + carve_size(pbytes);
+        FG_CUDA(cudaMalloc(&ck_mem, per * S));
+        for (uint64_t q = 0; q < S; ++q) {
+            char* c = ck_mem + per * q;
+            cks.push_back(Ck{reinterpret_cast<float*>(c), reinterpret_cast<float*>(c + carve_size(fbytes)),
+                             reinterpret_cast<float*>(c + 2 * carve_size(fbytes))});
+        }
+    }
 
     // 1. forward
     auto t0 = now();
@@ -176,11 +182,7 @@ int flux_gradient(Gpu* gpu, const HostSim& sim, uint64_t driven, double f0, doub
         if ((rc = session_step(s, N, err))) return rc;
     } else {
         for (uint64_t q = 0; q < S; ++q) {
-            Ck c;
-            FG_CUDA(cudaMalloc(&c.e, fbytes));
-            FG_CUDA(cudaMalloc(&c.h, fbytes));
-            FG_CUDA(cudaMalloc(&c.psi, pbytes));
-            cks.push_back(c);
+            const Ck& c = cks[q];
             FG_CUDA(cudaMemcpyAsync(c.e, s->e, fbytes, cudaMemcpyDeviceToDevice, st));
             FG_CUDA(cudaMemcpyAsync(c.h, s->h, fbytes, cudaMemcpyDeviceToDevice, st));
             FG_CUDA(cudaMemcpyAsync(c.psi, s->psi, pbytes, cudaMemcpyDeviceToDevice, st));

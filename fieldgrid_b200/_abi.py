@@ -98,6 +98,11 @@ class fg_flux_result(C.Structure):
                 ("segments", C.c_uint64), ("segment_len", C.c_uint64), ("design_edges", C.c_uint64)]
 
 
+class fg_batch_options(C.Structure):
+    _fields_ = [("tune", C.c_int), ("tile", C.c_int), ("blocks_per_sm", C.c_int), ("seg", C.c_int),
+                ("graph_steps", C.c_int)]
+
+
 def _ptr(arr: np.ndarray | None, ctype):
     if arr is None:
         return C.cast(None, P(ctype))

@@ -84,6 +84,12 @@ def _declare(L):
         "fg_far_field": (C.c_int, [vp, vp, P(dbl), u64, P(dbl)]),
         "fg_far_intensity": (C.c_int, [vp, vp, P(dbl), u64, P(dbl)]),
         "fg_far_radiated": (C.c_int, [vp, vp, u64, P(dbl), P(dbl)]),
+        "fg_batch_new": (C.c_int, [vp, P(vp), P(u64), P(A.fg_pulse), u64, u64, P(A.fg_batch_options), P(vp), cp, sz]),
+        "fg_batch_step": (C.c_int, [vp, u64, cp, sz]),
+        "fg_batch_sync": (C.c_int, [vp]),
+        "fg_batch_read": (C.c_int, [vp, u64, cp, P(C.c_float), u64, cp, sz]),
+        "fg_batch_info": (C.c_int, [vp, P(A.fg_batch_options), P(C.c_int), P(dbl), P(u64)]),
+        "fg_batch_free": (None, [vp]),
         "fg_flux_gradient": (C.c_int, [vp, vp, u64, P(A.fg_pulse), P(A.fg_flux_spec), P(A.fg_flux_result), P(dbl),
                                        P(dbl), cp, sz]),
         "fg_energy_noalloc": (C.c_int, [vp, vp, u64, vp, vp]),

@@ -1,0 +1,410 @@
+// Many independent grids of uneven sizes stepped together: one persistent launch per step marches
+// every grid's tiles from a shared work-list, then one launch each applies every grid's Debye
+// edges, sources and port probes, and the step loop is captured in a CUDA graph. Each grid keeps
+// its own buffers, coefficients, CPML and element lists (a Session built without graphs), so the
+// arithmetic is per grid exactly that of stepping it alone with the direct-load march.
+//
+// Work items: for grid b, tiles_k x tiles_j tiles of TJ x TK columns times ceil(n0 / seg) x-segments;
+// item numbers are prefix-summed over the grids, and a block takes the next item from an atomic
+// counter (reset at the start of every step), finds its grid by binary search over the prefix
+// sums, and marches that tile (fused_tile, stencil_fused.cuh). Large grids therefore fill the GPU
+// while small ones finish in the same launch, with no per-grid launch or tail.
+//
+// The autotuner times a few steps of each candidate (tile shape, blocks per SM of the persistent
+// launch, planes per item) on the real batch, keeps the fastest, resets every grid to step 0 and
+// captures the graphs with it.
+//
+// Included at the end of engine.cu (it builds on Session).
+#pragma once
+
+namespace fg {
+
+struct BatchInstance {
+    FusedArgs a[2];                 // the march's arguments for input set 0 / 1
+    int tiles_k, tiles_j, seg;
+    const long long* debye_f;
+    const float* debye_dd;
+    int n_debye;
+    const float* debye_table;
+    float* debye_state;
+    const DevSource* src;
+    int ns;
+    DevInductor* ind;
+    int ni;
+    StepConst sc;
+    unsigned* counter;
+    const DevProbe* probes;
+    const DevPortEdge* pe;
+    const DevLoop* lp;
+    int n_ports;
+    float* series;
+    float* e[2];
+    float* h[2];
+};
+
+// the index b with first[b] <= t < first[b + 1]
+__device__ __forceinline__ int batch_find(const long long* __restrict__ first, int n, long long t) {
+    int lo = 0, hi = n;
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (first[mid] <= t) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+// Opens step n of every grid (the counters the later kernels read) and rewinds the work-list.
+__global__ void k_batch_begin(const BatchInstance* __restrict__ bi, int n, unsigned long long* queue) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n) *bi[t].counter += 1u;
+    if (t == 0) *queue = 0ull;
+}
+
+template <typename CID, int TK, int TJ>
+__global__ void __launch_bounds__(TK* TJ) k_batch_march(const BatchInstance* __restrict__ bi,
+                                                        const long long* __restrict__ first, int n,
+                                                        unsigned long long* queue, int parity) {
+    __shared__ float hs[2][3][TJ + 1][TK + 1];
+    __shared__ long long item;
+    const long long total = first[n];
+    for (;;) {
+        __syncthreads();   // the previous item's tile is read no more
+        if (threadIdx.x == 0 && threadIdx.y == 0) item = (long long)atomicAdd(queue, 1ull);
+        __syncthreads();
+        const long long it = item;
+        if (it >= total) return;
+        const int b = batch_find(first, n, it);
+        const BatchInstance& in = bi[b];
+        const long long l = it - first[b];
+        const int per = in.tiles_k * in.tiles_j;
+        const int bz = int(l / per), r = int(l - (long long)bz * per);
+        const int i0 = bz * in.seg;
+        const FusedArgs& a = in.a[parity];
+        fused_tile<CID, TK, TJ>(a, hs, r % in.tiles_k, r / in.tiles_k, i0, min(i0 + in.seg, a.g.n0));
+    }
+}
+
+template <typename CID>
+__global__ void k_batch_debye(const BatchInstance* __restrict__ bi, const long long* __restrict__ first, int n,
+                              int parity) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= first[n]) return;
+    const int b = batch_find(first, n, t);
+    const BatchInstance& in = bi[b];
+    debye_post_edge<CID>(int(t - first[b]), in.debye_f, in.debye_dd, in.n_debye, nullptr, in.e[parity],
+                         static_cast<const CID*>(in.a[0].node_class), in.a[0].classes, in.a[0].g.cs, in.debye_table,
+                         in.debye_state, in.e[1 - parity]);
+}
+
+// one block per grid
+__global__ void k_batch_lumped(const BatchInstance* __restrict__ bi, int parity) {
+    const BatchInstance& in = bi[blockIdx.x];
+    lumped_block(in.src, in.ns, in.ind, in.ni, in.sc, in.counter, in.e[1 - parity]);
+}
+
+// one block per port of any grid
+__global__ void __launch_bounds__(256) k_batch_probe(const BatchInstance* __restrict__ bi,
+                                                     const long long* __restrict__ first, int n, int parity) {
+    const int b = batch_find(first, n, blockIdx.x);
+    const BatchInstance& in = bi[b];
+    probe_block(int(blockIdx.x - first[b]), in.probes, in.pe, in.lp, in.a[0].g.cs, in.e[1 - parity],
+                in.h[1 - parity], in.counter, in.sc, in.series);
+}
+
+struct BatchShape {
+    int tile = 0;             // 0: 32 x 8, 1: 64 x 4, 2: 32 x 4 (TK x TJ)
+    int blocks_per_sm = 0;    // persistent blocks per SM; 0: the occupancy limit
+    int seg = 32;             // x-planes per work item
+};
+
+constexpr int BATCH_TILES[3][2] = {{32, 8}, {64, 4}, {32, 4}};
+
+struct Batch {
+    Gpu* gpu = nullptr;
+    cudaStream_t stream = nullptr;
+    std::vector<Session*> s;
+    int cid_bytes = 1;
+    BatchShape shape{};
+    BatchInstance* d_inst = nullptr;
+    long long* d_items = nullptr;   // n + 1 prefix sums of work items
+    long long* d_edges = nullptr;   // n + 1 prefix sums of Debye edges
+    long long* d_ports = nullptr;   // n + 1 prefix sums of ports
+    unsigned long long* d_queue = nullptr;
+    std::vector<BatchInstance> inst;
+    long long total_edges = 0, total_ports = 0;
+    int persistent_blocks = 0;
+    uint64_t steps = 0;
+    int graph_steps = 0;
+    cudaGraphExec_t graph_many = nullptr, graph_one[2] = {nullptr, nullptr};
+    double tuned_ms = 0;      // ms per step of the chosen shape while tuning
+    std::vector<std::pair<BatchShape, double>> trials;
+};
+
+template <typename F>
+bool with_batch_march(int cid_bytes, int tile, F&& f) {
+    auto go = [&](auto cid) {
+        using C = decltype(cid);
+        switch (tile) {
+            case 1: return f(k_batch_march<C, 64, 4>, 64, 4);
+            case 2: return f(k_batch_march<C, 32, 4>, 32, 4);
+            default: return f(k_batch_march<C, 32, 8>, 32, 8);
+        }
+    };
+    if (cid_bytes == 1) return go(uint8_t{});
+    if (cid_bytes == 2) return go(uint16_t{});
+    return go(uint32_t{});
+}
+
+// Work items of every grid for a shape; uploads the per-grid tiling and the prefix sums.
+int batch_apply_shape(Batch& B, const BatchShape& sh, std::string& err) {
+    const int TK = BATCH_TILES[sh.tile][0], TJ = BATCH_TILES[sh.tile][1];
+    std::vector<long long> items(B.s.size() + 1, 0);
+    for (size_t b = 0; b < B.s.size(); ++b) {
+        const Geom& g = B.s[b]->geom;
+        BatchInstance& in = B.inst[b];
+        in.tiles_k = (g.n2 + TK - 1) / TK;
+        in.tiles_j = (g.n1 + TJ - 1) / TJ;
+        in.seg = std::min(sh.seg, g.n0);
+        items[b + 1] = items[b] + (long long)in.tiles_k * in.tiles_j * ((g.n0 + in.seg - 1) / in.seg);
+    }
+    FG_CUDA(cudaMemcpy(B.d_inst, B.inst.data(), B.inst.size() * sizeof(BatchInstance), cudaMemcpyHostToDevice));
+    FG_CUDA(cudaMemcpy(B.d_items, items.data(), items.size() * 8, cudaMemcpyHostToDevice));
+    int occ = 0;
+    cudaError_t ce = cudaSuccess;
+    with_batch_march(B.cid_bytes, sh.tile, [&](auto kern, int tk, int tj) {
+        ce = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, tk * tj, 0);
+        return true;
+    });
+    if (ce != cudaSuccess) { err = std::string("cudaOccupancyMaxActiveBlocksPerMultiprocessor: ") + cudaGetErrorString(ce); return FG_ERR_CUDA; }
+    int sms = 0;
+    FG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, B.gpu->device));
+    const int per_sm = sh.blocks_per_sm > 0 ? std::min(sh.blocks_per_sm, std::max(occ, 1)) : std::max(occ, 1);
+    B.persistent_blocks = per_sm * sms;
+    B.shape = sh;
+    return FG_OK;
+}
+
+int batch_enqueue_step(Batch& B, int parity, std::string& err) {
+    cudaStream_t st = B.stream;
+    const int n = int(B.s.size());
+    k_batch_begin<<<(n + 127) / 128, 128, 0, st>>>(B.d_inst, n, B.d_queue);
+    with_batch_march(B.cid_bytes, B.shape.tile, [&](auto kern, int tk, int tj) {
+        kern<<<B.persistent_blocks, dim3(tk, tj), 0, st>>>(B.d_inst, B.d_items, n, B.d_queue, parity);
+        return true;
+    });
+    if (B.total_edges > 0) {
+        const unsigned blocks = unsigned((B.total_edges + 255) / 256);
+        switch (B.cid_bytes) {
+            case 1: k_batch_debye<uint8_t><<<blocks, 256, 0, st>>>(B.d_inst, B.d_edges, n, parity); break;
+            case 2: k_batch_debye<uint16_t><<<blocks, 256, 0, st>>>(B.d_inst, B.d_edges, n, parity); break;
+            default: k_batch_debye<uint32_t><<<blocks, 256, 0, st>>>(B.d_inst, B.d_edges, n, parity); break;
+        }
+    }
+    k_batch_lumped<<<n, 256, 0, st>>>(B.d_inst, parity);
+    if (B.total_ports > 0) k_batch_probe<<<unsigned(B.total_ports), 256, 0, st>>>(B.d_inst, B.d_ports, n, parity);
+    const cudaError_t ce = cudaPeekAtLastError();
+    if (ce != cudaSuccess) { err = std::string("batched step launch: ") + cudaGetErrorString(ce); return FG_ERR_CUDA; }
+    return FG_OK;
+}
+
+void batch_free(Batch* B) {
+    if (!B) return;
+    if (B->gpu) cudaSetDevice(B->gpu->device);
+    if (B->stream) cudaStreamSynchronize(B->stream);
+    if (B->graph_many) cudaGraphExecDestroy(B->graph_many);
+    for (auto& gx : B->graph_one)
+        if (gx) cudaGraphExecDestroy(gx);
+    cudaFree(B->d_inst);
+    cudaFree(B->d_items);
+    cudaFree(B->d_edges);
+    cudaFree(B->d_ports);
+    cudaFree(B->d_queue);
+    for (Session* s : B->s) session_free(s);
+    if (B->stream) cudaStreamDestroy(B->stream);
+    delete B;
+}
+
+int batch_capture(Batch& B, int steps, int parity0, cudaGraphExec_t* out, std::string& err) {
+    cudaGraph_t graph;
+    FG_CUDA(cudaStreamBeginCapture(B.stream, cudaStreamCaptureModeThreadLocal));
+    int rc = FG_OK;
+    for (int q = 0; q < steps && rc == FG_OK; ++q) rc = batch_enqueue_step(B, (parity0 + q) & 1, err);
+    cudaError_t ce = cudaStreamEndCapture(B.stream, &graph);
+    if (rc) return rc;
+    if (ce != cudaSuccess) { err = std::string("cudaStreamEndCapture: ") + cudaGetErrorString(ce); return FG_ERR_CUDA; }
+    ce = cudaGraphInstantiate(out, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ce != cudaSuccess) { err = std::string("cudaGraphInstantiate: ") + cudaGetErrorString(ce); return FG_ERR_CUDA; }
+    return FG_OK;
+}
+
+int batch_reset(Batch& B, std::string& err) {
+    for (Session* s : B.s) {
+        const int rc = session_reset(s, err);
+        if (rc) return rc;
+    }
+    B.steps = 0;
+    return FG_OK;
+}
+
+int batch_step(Batch& B, uint64_t k, std::string& err) {
+    FG_CUDA(cudaSetDevice(B.gpu->device));
+    uint64_t done = 0;
+    while (done < k) {
+        const int parity = int(B.steps & 1);
+        if (parity == 0 && k - done >= uint64_t(B.graph_steps) && B.graph_many) {
+            FG_CUDA(cudaGraphLaunch(B.graph_many, B.stream));
+            done += B.graph_steps;
+            B.steps += B.graph_steps;
+        } else {
+            FG_CUDA(cudaGraphLaunch(B.graph_one[parity], B.stream));
+            done += 1;
+            B.steps += 1;
+        }
+    }
+    for (Session* s : B.s) s->steps = B.steps;   // for session_read's choice of the latest buffers
+    FG_CUDA(cudaGetLastError());
+    return FG_OK;
+}
+
+// opt: a fixed shape (tune = false) or the tuner's candidates (tune = true).
+int batch_new(Gpu* gpu, const std::vector<const HostSim*>& sims, const std::vector<RunSpec>& specs, bool tune,
+              const BatchShape& fixed, int graph_steps, Batch** out, std::string& err) {
+    *out = nullptr;
+    if (!gpu) { err = "no GPU: this engine has no CPU path"; return FG_ERR_NO_DEVICE; }
+    if (sims.empty() || sims.size() != specs.size()) { err = "a batch needs one run spec per grid"; return FG_ERR_INVALID; }
+    FG_CUDA(cudaSetDevice(gpu->device));
+    auto B = std::unique_ptr<Batch, void (*)(Batch*)>(new Batch, batch_free);
+    B->gpu = gpu;
+    FG_CUDA(cudaStreamCreateWithFlags(&B->stream, cudaStreamNonBlocking));
+    // one class-id width for all grids
+    int cid = 1;
+    for (const HostSim* h : sims) cid = std::max(cid, h->classes.size() <= 256 ? 1 : (h->classes.size() <= 65536 ? 2 : 4));
+    B->cid_bytes = cid;
+    for (size_t b = 0; b < sims.size(); ++b) {
+        const HostSim& h = *sims[b];
+        if (!h.wires.empty() || !h.sheets.empty()) { err = "grid " + std::to_string(b) + ": a batch takes no thin wires or resistive sheets"; return FG_ERR_INVALID; }
+        RunSpec rs = specs[b];
+        if (rs.has_plane_k || rs.has_ntff) { err = "grid " + std::to_string(b) + ": a batch records no plane DFT or NTFF"; return FG_ERR_INVALID; }
+        rs.fused = true;
+        rs.tma = false;
+        rs.graphs = false;
+        rs.cid_bytes = cid;
+        Session* s = nullptr;
+        const int rc = session_new(gpu, h, rs, &s, err);
+        if (rc) { err = "grid " + std::to_string(b) + ": " + err; return rc; }
+        B->s.push_back(s);
+    }
+    // descriptors
+    std::vector<long long> edges(sims.size() + 1, 0), ports(sims.size() + 1, 0);
+    for (size_t b = 0; b < B->s.size(); ++b) {
+        Session& s = *B->s[b];
+        BatchInstance in{};
+        in.a[0] = FusedArgs{s.geom, s.node_class, s.classes, s.e, s.h, s.e2, s.h2, s.psi, s.psi, s.psi_h2, s.sc.k_mu, s.counter};
+        in.a[1] = FusedArgs{s.geom, s.node_class, s.classes, s.e2, s.h2, s.e, s.h, s.psi, s.psi_h2, s.psi, s.sc.k_mu, s.counter};
+        in.debye_f = s.debye_f;
+        in.debye_dd = s.debye_dd;
+        in.n_debye = s.n_debye;
+        in.debye_table = s.debye_table;
+        in.debye_state = s.debye_state;
+        in.src = s.sources;
+        in.ns = s.n_sources;
+        in.ind = s.inductors;
+        in.ni = s.n_inductors;
+        in.sc = s.sc;
+        in.counter = s.counter;
+        in.probes = s.probes;
+        in.pe = s.port_edges;
+        in.lp = s.loops;
+        in.n_ports = s.n_ports;
+        in.series = s.series;
+        in.e[0] = s.e; in.e[1] = s.e2;
+        in.h[0] = s.h; in.h[1] = s.h2;
+        B->inst.push_back(in);
+        edges[b + 1] = edges[b] + s.n_debye;
+        ports[b + 1] = ports[b] + s.n_ports;
+    }
+    B->total_edges = edges.back();
+    B->total_ports = ports.back();
+    const size_t n = B->s.size();
+    FG_CUDA(cudaMalloc(&B->d_inst, n * sizeof(BatchInstance)));
+    FG_CUDA(cudaMalloc(&B->d_items, (n + 1) * 8));
+    FG_CUDA(cudaMalloc(&B->d_edges, (n + 1) * 8));
+    FG_CUDA(cudaMalloc(&B->d_ports, (n + 1) * 8));
+    FG_CUDA(cudaMalloc(&B->d_queue, 8));
+    FG_CUDA(cudaMemcpy(B->d_edges, edges.data(), (n + 1) * 8, cudaMemcpyHostToDevice));
+    FG_CUDA(cudaMemcpy(B->d_ports, ports.data(), (n + 1) * 8, cudaMemcpyHostToDevice));
+    int rc = FG_OK;
+    // the tuner: each candidate runs a warm-up step then a timed block of steps from the live state
+    BatchShape best = fixed;
+    if (tune) {
+        cudaEvent_t e0, e1;
+        FG_CUDA(cudaEventCreate(&e0));
+        FG_CUDA(cudaEventCreate(&e1));
+        double best_ms = 1e300;
+        const int timed = 4;
+        for (int tile = 0; tile < 3; ++tile)
+            for (int seg : {16, 32, 64})
+                for (int bps : {0, 2}) {
+                    BatchShape sh{tile, bps, seg};
+                    if ((rc = batch_apply_shape(*B, sh, err))) break;
+                    for (int q = 0; q < 2 && !rc; ++q) rc = batch_enqueue_step(*B, q & 1, err);
+                    FG_CUDA(cudaEventRecord(e0, B->stream));
+                    for (int q = 0; q < timed && !rc; ++q) rc = batch_enqueue_step(*B, q & 1, err);
+                    FG_CUDA(cudaEventRecord(e1, B->stream));
+                    FG_CUDA(cudaEventSynchronize(e1));
+                    float ms = 0;
+                    FG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+                    B->trials.push_back({sh, ms / timed});
+                    if (ms / timed < best_ms) { best_ms = ms / timed; best = sh; }
+                }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        if (rc) return rc;
+        B->tuned_ms = best_ms;
+        if ((rc = batch_reset(*B, err))) return rc;
+    }
+    if ((rc = batch_apply_shape(*B, best, err))) return rc;
+    B->graph_steps = std::max(2, graph_steps + (graph_steps & 1));
+    if ((rc = batch_capture(*B, B->graph_steps, 0, &B->graph_many, err))) return rc;
+    if ((rc = batch_capture(*B, 1, 0, &B->graph_one[0], err))) return rc;
+    if ((rc = batch_capture(*B, 1, 1, &B->graph_one[1], err))) return rc;
+    *out = B.release();
+    return FG_OK;
+}
+
+int batch_new_c(Gpu* gpu, const std::vector<const HostSim*>& sims, const std::vector<RunSpec>& specs, bool tune,
+                int tile, int blocks_per_sm, int seg, int graph_steps, Batch** out, std::string& err) {
+    BatchShape sh;
+    sh.tile = std::min(std::max(tile, 0), 2);
+    sh.blocks_per_sm = std::max(blocks_per_sm, 0);
+    sh.seg = seg > 0 ? seg : 32;
+    return batch_new(gpu, sims, specs, tune, sh, graph_steps > 0 ? graph_steps : 10, out, err);
+}
+
+int batch_sync(Batch& B, std::string& err) {
+    FG_CUDA(cudaSetDevice(B.gpu->device));
+    FG_CUDA(cudaStreamSynchronize(B.stream));
+    return FG_OK;
+}
+
+int batch_read(Batch& B, uint64_t index, const std::string& which, float* dst, uint64_t len, std::string& err) {
+    if (index >= B.s.size()) { err = "no grid " + std::to_string(index) + " in this batch"; return FG_ERR_INVALID; }
+    const int rc = batch_sync(B, err);
+    if (rc) return rc;
+    return session_read(B.s[index], which, dst, len, err);
+}
+
+void batch_info(const Batch& B, int* tile, int* blocks_per_sm, int* seg, int* persistent_blocks, double* tuned_ms,
+                uint64_t* steps) {
+    if (tile) *tile = B.shape.tile;
+    if (blocks_per_sm) *blocks_per_sm = B.shape.blocks_per_sm;
+    if (seg) *seg = B.shape.seg;
+    if (persistent_blocks) *persistent_blocks = B.persistent_blocks;
+    if (tuned_ms) *tuned_ms = B.tuned_ms;
+    if (steps) *steps = B.steps;
+}
+
+uint64_t batch_size(const Batch& B) { return B.s.size(); }
+
+}  // namespace fg

@@ -529,4 +529,70 @@ int fg_flux_gradient(fg_gpu* g, const fg_sim* sim, uint64_t driven, const fg_pul
     return FG_OK;
 }
 
+struct fg_batch { Batch* b; };
+
+int fg_batch_new(fg_gpu* g, const fg_sim* const* sims, const uint64_t* driven, const fg_pulse* pulses, uint64_t count,
+                 uint64_t max_steps, const fg_batch_options* opt, fg_batch** out, char* err, size_t errlen) {
+    if (!out) return fail(FG_ERR_INVALID, "null output handle", err, errlen);
+    *out = nullptr;
+    if (!g) return fail(FG_ERR_NO_DEVICE, "no GPU: this engine has no CPU path", err, errlen);
+    if (!sims || !pulses || count == 0) return fail(FG_ERR_INVALID, "a batch needs grids and pulses", err, errlen);
+    std::vector<const HostSim*> hs;
+    std::vector<RunSpec> specs;
+    for (uint64_t b = 0; b < count; ++b) {
+        if (!sims[b]) return fail(FG_ERR_INVALID, "null grid in the batch", err, errlen);
+        hs.push_back(sims[b]->s);
+        RunSpec rs;
+        rs.driven = driven ? driven[b] : 0;
+        rs.f0 = pulses[b].f0;
+        rs.fc = pulses[b].fc;
+        rs.max_steps = max_steps;
+        specs.push_back(rs);
+    }
+    fg_batch_options o{1, 0, 0, 32, 10};
+    if (opt) o = *opt;
+    Batch* B = nullptr;
+    std::string e;
+    int rc = batch_new_c(g->g, hs, specs, o.tune != 0, o.tile, o.blocks_per_sm, o.seg, o.graph_steps, &B, e);
+    if (rc) return fail(rc, e, err, errlen);
+    *out = new fg_batch{B};
+    return FG_OK;
+}
+
+int fg_batch_step(fg_batch* b, uint64_t steps, char* err, size_t errlen) {
+    if (!b) return fail(FG_ERR_INVALID, "null batch", err, errlen);
+    std::string e;
+    int rc = batch_step(*b->b, steps, e);
+    return rc ? fail(rc, e, err, errlen) : FG_OK;
+}
+
+int fg_batch_sync(fg_batch* b) {
+    if (!b) return FG_ERR_INVALID;
+    std::string e;
+    int rc = batch_sync(*b->b, e);
+    if (rc) fg::set_last_error(e);
+    return rc;
+}
+
+int fg_batch_read(fg_batch* b, uint64_t index, const char* which, float* dst, uint64_t len, char* err, size_t errlen) {
+    if (!b || !which || !dst) return fail(FG_ERR_INVALID, "null argument", err, errlen);
+    std::string e;
+    int rc = batch_read(*b->b, index, which, dst, len, e);
+    return rc ? fail(rc, e, err, errlen) : FG_OK;
+}
+
+int fg_batch_info(const fg_batch* b, fg_batch_options* opt, int* persistent_blocks, double* tuned_ms, uint64_t* steps) {
+    if (!b) return FG_ERR_INVALID;
+    int tile = 0, bps = 0, seg = 0;
+    batch_info(*b->b, &tile, &bps, &seg, persistent_blocks, tuned_ms, steps);
+    if (opt) *opt = fg_batch_options{0, tile, bps, seg, 0};
+    return FG_OK;
+}
+
+void fg_batch_free(fg_batch* b) {
+    if (!b) return;
+    batch_free(b->b);
+    delete b;
+}
+
 }  // extern "C"

@@ -108,6 +108,10 @@ struct Session {
     float *hist_e = nullptr, *hist_s = nullptr;
     int hist_cap = 0;
     long long* hist_base = nullptr;
+    // what a reset to step 0 restores
+    int n_poles = 0;
+    size_t currents_len = 0;
+    std::vector<DevInductor> ind_host;
     float* tables = nullptr;        // per block region: LOCAL_CLASSES x (ca[3], cb[3])
     bool local = false;
     // counts
@@ -568,6 +572,7 @@ int session_new(Gpu* gpu, const HostSim& sim, const RunSpec& rs, Session** out, 
     // class ids narrowed to the smallest width that holds them
     const size_t ncls = sim.classes.size();
     s->cid_bytes = ncls <= 256 ? 1 : (ncls <= 65536 ? 2 : 4);
+    if (rs.cid_bytes > s->cid_bytes) s->cid_bytes = rs.cid_bytes == 2 ? 2 : 4;
 
     // sparse lists (pack, run.rs:243-340)
     std::vector<DevSource> src;
@@ -723,7 +728,7 @@ int session_new(Gpu* gpu, const HostSim& sim, const RunSpec& rs, Session** out, 
     // per-region class tables for the TMA step (fused runs on sm_100)
     LocalClasses lc;
     CleanPlan cp;
-    if (s->fused && !(std::getenv("FIELDGRID_NO_TMA") && std::getenv("FIELDGRID_NO_TMA")[0] == '1')) {
+    if (s->fused && rs.tma && !(std::getenv("FIELDGRID_NO_TMA") && std::getenv("FIELDGRID_NO_TMA")[0] == '1')) {
         cp = plan_clean(sim, g);
         if (cp.ok) {
             lc = build_local(sim, g, cp);
@@ -922,6 +927,13 @@ int session_new(Gpu* gpu, const HostSim& sim, const RunSpec& rs, Session** out, 
     else
         s->variant = s->fused ? fused_name(s->shape) + " (" + s->tma.why + ")" : std::string("separate H+E, 64x4 threads");
     s->launches = count_launches(*s);
+    s->n_poles = int(sim.poles.size());
+    s->currents_len = sheets.size() * nr_nc;
+    s->ind_host = ind;
+    if (!rs.graphs) {
+        *out = s.release();
+        return FG_OK;
+    }
     // graphs: a block of even length (the fused step alternates buffers), a pair and singles
     s->graph_steps = 32;
     rc = capture(*s, s->graph_steps, 0, &s->graph_many, err);
@@ -950,7 +962,36 @@ void session_free(Session* s) {
     delete s;
 }
 
+// Back to step 0: fields, psi, Debye and sheet state, inductor currents, records and the step
+// counter cleared; coefficients and element lists kept.
+int session_reset(Session* s, std::string& err) {
+    FG_CUDA(cudaSetDevice(s->gpu->device));
+    cudaStream_t st = s->stream;
+    const size_t fb = size_t(3 * s->geom.cs) * 4;
+    for (float* p : {s->e, s->h, s->e2, s->h2})
+        if (p) FG_CUDA(cudaMemsetAsync(p, 0, fb, st));
+    FG_CUDA(cudaMemsetAsync(s->psi, 0, size_t(std::max<long long>(s->psi_total, 1)) * 4, st));
+    if (s->fused && s->psi_total > s->psi_hbase)
+        FG_CUDA(cudaMemsetAsync(s->psi_h2 + s->psi_hbase, 0, size_t(s->psi_total - s->psi_hbase) * 4, st));
+    FG_CUDA(cudaMemsetAsync(s->counter, 0, 16 * sizeof(unsigned), st));
+    FG_CUDA(cudaMemsetAsync(s->series, 0, std::max<uint64_t>(s->series_len, 1) * 4, st));
+    FG_CUDA(cudaMemsetAsync(s->plane, 0, std::max<uint64_t>(s->plane_len, 1) * 4, st));
+    FG_CUDA(cudaMemsetAsync(s->ntff, 0, std::max<uint64_t>(s->ntff_len, 1) * 4, st));
+    if (s->n_debye) {
+        FG_CUDA(cudaMemsetAsync(s->debye_old, 0, size_t(s->n_debye) * 4, st));
+        FG_CUDA(cudaMemsetAsync(s->debye_state, 0, size_t(s->n_debye) * size_t(std::max(s->n_poles, 1)) * 4, st));
+    }
+    if (s->currents_len) FG_CUDA(cudaMemsetAsync(s->currents, 0, s->currents_len * 4, st));
+    if (!s->ind_host.empty())
+        FG_CUDA(cudaMemcpyAsync(s->inductors, s->ind_host.data(), s->ind_host.size() * sizeof(DevInductor),
+                                cudaMemcpyHostToDevice, st));
+    FG_CUDA(cudaStreamSynchronize(st));
+    s->steps = 0;
+    return FG_OK;
+}
+
 int session_step(Session* s, uint64_t k, std::string& err) {
+    if (!s->graph_many && !s->graph_one[0]) { err = "this session steps only as part of a batch"; return FG_ERR_INVALID; }
     FG_CUDA(cudaSetDevice(s->gpu->device));
     uint64_t done = 0;
     // the fused step alternates buffers: a whole graph block needs an even start
@@ -1108,3 +1149,4 @@ uint64_t session_d2h_bytes(const Session* s) { return s->d2h_bytes; }
 }  // namespace fg
 
 #include "adjoint.cuh"
+#include "batch.cuh"

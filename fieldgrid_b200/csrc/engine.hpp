@@ -26,6 +26,11 @@ struct RunSpec {               // pack() inputs that are not part of the Sim (ru
     // into a ring of hist_cap slots (slot = step - base)
     const std::vector<int4>* design = nullptr;
     int hist_cap = 0;
+    // batched use: the direct-load march only, no captured graphs, and a class-id width of at
+    // least cid_bytes (so instances share one kernel instantiation)
+    bool tma = true;
+    bool graphs = true;
+    int cid_bytes = 0;
 };
 
 struct Session;
@@ -81,6 +86,20 @@ struct FluxResult {
     uint64_t segments = 0, segment_len = 0, design_edges = 0;
     std::vector<double> g_eps, g_sig;   // per design cell, k fastest
 };
+
+// Batches of independent grids stepped by shared launches (batch.cuh).
+struct Batch;
+struct BatchShape;
+int session_reset(Session* s, std::string& err);
+int batch_new_c(Gpu* gpu, const std::vector<const HostSim*>& sims, const std::vector<RunSpec>& specs, bool tune,
+                int tile, int blocks_per_sm, int seg, int graph_steps, Batch** out, std::string& err);
+void batch_free(Batch* b);
+int batch_step(Batch& b, uint64_t k, std::string& err);
+int batch_sync(Batch& b, std::string& err);
+int batch_read(Batch& b, uint64_t index, const std::string& which, float* dst, uint64_t len, std::string& err);
+void batch_info(const Batch& b, int* tile, int* blocks_per_sm, int* seg, int* persistent_blocks, double* tuned_ms,
+                uint64_t* steps);
+uint64_t batch_size(const Batch& b);
 
 int flux_gradient(Gpu* gpu, const HostSim& sim, uint64_t driven, double f0, double fc, const FluxSpec& sp,
                   bool want_grad, FluxResult& res, std::string& err);

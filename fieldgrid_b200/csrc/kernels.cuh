@@ -157,12 +157,12 @@ __global__ void k_debye_pre(const long long* __restrict__ f, int count, const fl
 // cpu.rs:239-260: E -= cb * sum_k 0.5 (1 + b_k) s_k; s_k = b_k s_k + dd c_k (E_new - E_old).
 // `eold` is either the saved copy (separate step) or the step's input buffer (fused step).
 template <typename CID>
-__global__ void k_debye_post(const long long* __restrict__ f, const float* __restrict__ dd, int count,
-                             const float* __restrict__ eold_saved, const float* __restrict__ eold_field,
-                             const CID* __restrict__ node_class, const DevCoef* __restrict__ classes, long long cs,
-                             const float* __restrict__ table, float* __restrict__ state, float* __restrict__ e) {
-    int q = blockIdx.x * blockDim.x + threadIdx.x;
-    if (q >= count) return;
+__device__ __forceinline__ void debye_post_edge(int q, const long long* __restrict__ f, const float* __restrict__ dd,
+                                                int count, const float* __restrict__ eold_saved,
+                                                const float* __restrict__ eold_field, const CID* __restrict__ node_class,
+                                                const DevCoef* __restrict__ classes, long long cs,
+                                                const float* __restrict__ table, float* __restrict__ state,
+                                                float* __restrict__ e) {
     const long long fi = f[q];
     const int c = int(fi / cs);
     const long long id = fi - c * cs;
@@ -181,6 +181,15 @@ __global__ void k_debye_post(const long long* __restrict__ f, const float* __res
     }
 }
 
+template <typename CID>
+__global__ void k_debye_post(const long long* __restrict__ f, const float* __restrict__ dd, int count,
+                             const float* __restrict__ eold_saved, const float* __restrict__ eold_field,
+                             const CID* __restrict__ node_class, const DevCoef* __restrict__ classes, long long cs,
+                             const float* __restrict__ table, float* __restrict__ state, float* __restrict__ e) {
+    int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q < count) debye_post_edge(q, f, dd, count, eold_saved, eold_field, node_class, classes, cs, table, state, e);
+}
+
 // cpu.rs:262-265
 __device__ __forceinline__ float pulse_at(const StepConst& sc, float t) {
     float x = (t - sc.t0) / sc.tau;
@@ -189,8 +198,9 @@ __device__ __forceinline__ float pulse_at(const StepConst& sc, float t) {
 
 // cpu.rs:291-303: the driven port's soft source at t = (n + 1/2) dt, then the inductor ADE.
 // One block; the source edges of a port are distinct, as are the inductor edges.
-__global__ void k_lumped(const DevSource* __restrict__ src, int ns, DevInductor* __restrict__ ind, int ni,
-                         StepConst sc, const unsigned* __restrict__ counter, float* __restrict__ e) {
+__device__ __forceinline__ void lumped_block(const DevSource* __restrict__ src, int ns, DevInductor* __restrict__ ind,
+                                             int ni, const StepConst& sc, const unsigned* __restrict__ counter,
+                                             float* __restrict__ e) {
     const unsigned n = step_index(counter);
     const float p = n < sc.cap ? sc.pulse[n] : pulse_at(sc, (float(n) + 0.5f) * sc.dt);
     for (int q = threadIdx.x; q < ns; q += blockDim.x) {
@@ -206,13 +216,20 @@ __global__ void k_lumped(const DevSource* __restrict__ src, int ns, DevInductor*
     }
 }
 
+__global__ void k_lumped(const DevSource* __restrict__ src, int ns, DevInductor* __restrict__ ind, int ni,
+                         StepConst sc, const unsigned* __restrict__ counter, float* __restrict__ e) {
+    lumped_block(src, ns, ind, ni, sc, counter, e);
+}
+
 // cpu.rs:309-334: per port V = -sum E*w over its edges and I = sum H*w around the loop, summed
 // in f64 like the CPU path; one block per port.
-__global__ void k_probe(const DevProbe* __restrict__ defs, const DevPortEdge* __restrict__ pe, const DevLoop* __restrict__ lp,
-                        long long cs, const float* __restrict__ e, const float* __restrict__ h,
-                        const unsigned* __restrict__ counter, StepConst sc, float* __restrict__ series) {
+__device__ __forceinline__ void probe_block(int port, const DevProbe* __restrict__ defs,
+                                            const DevPortEdge* __restrict__ pe, const DevLoop* __restrict__ lp,
+                                            long long cs, const float* __restrict__ e, const float* __restrict__ h,
+                                            const unsigned* __restrict__ counter, const StepConst& sc,
+                                            float* __restrict__ series) {
     __shared__ double sv[256], si[256];
-    const DevProbe d = defs[blockIdx.x];
+    const DevProbe d = defs[port];
     double v = 0.0, cur = 0.0;
     for (int q = threadIdx.x; q < d.count; q += blockDim.x) {
         DevPortEdge x = pe[d.first + q];
@@ -234,10 +251,16 @@ __global__ void k_probe(const DevProbe* __restrict__ defs, const DevPortEdge* __
     }
     const unsigned n = step_index(counter);
     if (threadIdx.x == 0 && n < sc.cap) {
-        long long o = ((long long)n * sc.ports + blockIdx.x) * 2;
+        long long o = ((long long)n * sc.ports + port) * 2;
         series[o] = float(sv[0]);
         series[o + 1] = float(si[0]);
     }
+}
+
+__global__ void k_probe(const DevProbe* __restrict__ defs, const DevPortEdge* __restrict__ pe, const DevLoop* __restrict__ lp,
+                        long long cs, const float* __restrict__ e, const float* __restrict__ h,
+                        const unsigned* __restrict__ counter, StepConst sc, float* __restrict__ series) {
+    probe_block(blockIdx.x, defs, pe, lp, cs, e, h, counter, sc, series);
 }
 
 // cpu.rs:336-361: running DFT of Ex, Ey, Ez (at (n+1) dt) and Hx, Hy (at (n+1/2) dt) on the

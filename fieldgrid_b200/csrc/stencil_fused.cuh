@@ -114,24 +114,23 @@ __device__ __forceinline__ float e_new(const FusedArgs& a, const int p[3], float
     return ca * e_own + cb * (t1 - t2);
 }
 
+// One tile (bx, by) of TJ x TK columns over planes [i0, i1): the block's whole march. The block
+// is (TK, TJ) threads; `hs` is its double-buffered H tile.
 template <typename CID, int TK, int TJ>
-__global__ void __launch_bounds__(TK* TJ) k_fused_step(FusedArgs a, int seg) {
-    __shared__ float hs[2][3][TJ + 1][TK + 1];
+__device__ __forceinline__ void fused_tile(const FusedArgs& a, float (&hs)[2][3][TJ + 1][TK + 1], int bx, int by, int i0,
+                                           int i1) {
     const Geom& g = a.g;
     const int lk = threadIdx.x, lj = threadIdx.y;
-    const int k = blockIdx.x * TK + lk;
-    const int j = blockIdx.y * TJ + lj;
-    const int i0 = blockIdx.z * seg;
-    const int i1 = min(i0 + seg, g.n0);
+    const int k = bx * TK + lk;
+    const int j = by * TJ + lj;
     const bool live = k < g.n2 && j < g.n1;
-    if ((blockIdx.x | blockIdx.y | blockIdx.z | threadIdx.x | threadIdx.y) == 0) *a.counter += 1u;
     const CID* cls = static_cast<const CID*>(a.node_class);
     float prev_y = 0.0f, prev_z = 0.0f;
     if (live && i0 > 0) {
         prev_y = h_new<1>(a, i0 - 1, j, k, false);
         prev_z = h_new<2>(a, i0 - 1, j, k, false);
     }
-    const int halo_j = blockIdx.y * TJ + lk;  // row served by the k-1 halo lanes
+    const int halo_j = by * TJ + lk;  // row served by the k-1 halo lanes
     for (int i = i0; i < i1; ++i) {
         const int o = i & 1;
         float hx = 0.f, hy = 0.f, hz = 0.f;
@@ -151,8 +150,8 @@ __global__ void __launch_bounds__(TK* TJ) k_fused_step(FusedArgs a, int seg) {
                 hs[o][2][0][lk + 1] = h_new<2>(a, i, j - 1, k, false);
             }
         }
-        if (lj == 1 % TJ && lk < TJ && halo_j < g.n1 && blockIdx.x > 0) {
-            const int ck = blockIdx.x * TK - 1;
+        if (lj == 1 % TJ && lk < TJ && halo_j < g.n1 && bx > 0) {
+            const int ck = bx * TK - 1;
             hs[o][0][lk + 1][0] = h_new<0>(a, i, halo_j, ck, false);
             hs[o][1][lk + 1][0] = h_new<1>(a, i, halo_j, ck, false);
         }
@@ -173,6 +172,14 @@ __global__ void __launch_bounds__(TK* TJ) k_fused_step(FusedArgs a, int seg) {
             prev_z = hz;
         }
     }
+}
+
+template <typename CID, int TK, int TJ>
+__global__ void __launch_bounds__(TK* TJ) k_fused_step(FusedArgs a, int seg) {
+    __shared__ float hs[2][3][TJ + 1][TK + 1];
+    if ((blockIdx.x | blockIdx.y | blockIdx.z | threadIdx.x | threadIdx.y) == 0) *a.counter += 1u;
+    const int i0 = blockIdx.z * seg;
+    fused_tile<CID, TK, TJ>(a, hs, blockIdx.x, blockIdx.y, i0, min(i0 + seg, a.g.n0));
 }
 
 inline FusedShape choose_shape(const Geom& g, int /*cid_bytes*/, bool /*wires*/) {

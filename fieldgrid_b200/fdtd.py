@@ -633,3 +633,64 @@ def flux_gradient(g, sim: Sim, driven: int, pulse: Pulse, spec: FluxSpec, grad: 
                       None if ge is None else ge.reshape(shp), None if gs is None else gs.reshape(shp),
                       out.forward_ms, out.recompute_ms, out.adjoint_ms, int(out.segments), int(out.segment_len),
                       int(out.design_edges))
+
+
+# ---- batches of independent grids (no counterpart in the reference) ----
+
+class Batch:
+    """Many Sims stepped together: one persistent work-list launch marches every grid per step,
+    then one launch each for all grids' Debye edges, sources and probes, in a captured graph.
+    `tune` times the candidate shapes first (tile, persistent blocks per SM, planes per item) and
+    keeps the fastest. Each grid's results equal stepping it alone with the fused step."""
+
+    def __init__(self, g, sims, pulses, max_steps: int, driven=None, tune: bool = True, tile: int = 0,
+                 blocks_per_sm: int = 0, seg: int = 32, graph_steps: int = 10):
+        if g is None:
+            raise FdtdError("no GPU: this engine has no CPU path", 3)
+        n = len(sims)
+        self._sims = list(sims)   # keep the Sims alive with the batch
+        hs = (C.c_void_p * n)(*[s._h for s in sims])
+        pl = (A.fg_pulse * n)(*[A.pulse_struct(p) for p in pulses])
+        dv = (C.c_uint64 * n)(*([0] * n if driven is None else [int(d) for d in driven]))
+        opt = A.fg_batch_options(1 if tune else 0, tile, blocks_per_sm, seg, graph_steps)
+        out = C.c_void_p()
+        err = C.create_string_buffer(ERRLEN)
+        code = lib().fg_batch_new(g._h, hs, dv, pl, n, max_steps, C.byref(opt), C.byref(out), err, ERRLEN)
+        _check(code, err)
+        self._h = out
+        self.size = n
+
+    def step(self, k: int) -> None:
+        err = C.create_string_buffer(ERRLEN)
+        _check(lib().fg_batch_step(self._h, k, err, ERRLEN), err)
+
+    def sync(self) -> None:
+        code = lib().fg_batch_sync(self._h)
+        if code:
+            raise FdtdError(lib().fg_last_error().decode(), code)
+
+    def read(self, index: int, which: str, n: int) -> np.ndarray:
+        out = np.zeros(n, np.float32)
+        err = C.create_string_buffer(ERRLEN)
+        _check(lib().fg_batch_read(self._h, index, which.encode(), out.ctypes.data_as(C.POINTER(C.c_float)), n,
+                                   err, ERRLEN), err)
+        return out
+
+    def info(self) -> dict:
+        o = A.fg_batch_options()
+        pb, tm, st = C.c_int(), C.c_double(), C.c_uint64()
+        lib().fg_batch_info(self._h, C.byref(o), C.byref(pb), C.byref(tm), C.byref(st))
+        tiles = ["32x8", "64x4", "32x4"]
+        return {"tile": tiles[o.tile], "blocks_per_sm": o.blocks_per_sm, "seg": o.seg,
+                "persistent_blocks": pb.value, "tuned_ms_per_step": tm.value, "steps": st.value}
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib().fg_batch_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -144,18 +144,19 @@ def dielectric_box(cells: int = 64, dx: float = 1e-3, pml: int = 8, steps: int =
 
 
 def sphere_materials(cells, count, rmin, rmax, pml, seed, debye_share=0.2):
-    """Seeded random spheres (later ones overwrite earlier ones) on a cubic cell grid.
-    Returns (Materials arrays eps, sigma, inf, debye) and the Debye time constant."""
-    n = cells
-    eps = np.ones((n, n, n), np.float32)
-    sig = np.zeros((n, n, n), np.float32)
-    inf = np.ones((n, n, n), np.float32)
-    deb = np.zeros((n, n, n), np.float32)
+    """Seeded random spheres (later ones overwrite earlier ones) on a cell grid of `cells` per axis
+    (an int, or a 3-tuple for a box). Returns (Materials arrays eps, sigma, inf, debye) and the
+    Debye time constant."""
+    dims = (cells,) * 3 if np.isscalar(cells) else tuple(int(v) for v in cells)
+    eps = np.ones(dims, np.float32)
+    sig = np.zeros(dims, np.float32)
+    inf = np.ones(dims, np.float32)
+    deb = np.zeros(dims, np.float32)
     rng = SplitMix64(seed)
     tau = rng.uniform(5e-12, 50e-12)
     spheres = []
     for _ in range(count):
-        cx, cy, cz = (rng.uniform(pml, n - pml) for _ in range(3))
+        cx, cy, cz = (rng.uniform(pml, dims[a] - pml) for a in range(3))
         r = rng.integer(rmin, rmax)
         er = rng.uniform(1.0, 10.0)
         s = rng.uniform(0.0, 0.05)
@@ -164,7 +165,7 @@ def sphere_materials(cells, count, rmin, rmax, pml, seed, debye_share=0.2):
         spheres.append((cx, cy, cz, r, er, s, is_debye, de))
     for cx, cy, cz, r, er, s, is_debye, de in spheres:
         lo = [max(int(math.floor(v - r)), 0) for v in (cx, cy, cz)]
-        hi = [min(int(math.ceil(v + r)) + 1, n) for v in (cx, cy, cz)]
+        hi = [min(int(math.ceil(v + r)) + 1, dims[a]) for a, v in enumerate((cx, cy, cz))]
         if any(h <= l for l, h in zip(lo, hi)):
             continue
         x = np.arange(lo[0], hi[0], dtype=np.float64)[:, None, None] + 0.5 - cx
@@ -300,3 +301,28 @@ def flux_design(nx: int = 160, ny: int = 160, nz: int = 96, dx: float = 1e-3, pm
         return sc
 
     return scene, spec, eps0, sig0
+
+
+def batch_grids(count: int = 192, lo: int = 48, hi: int = 160, pml: int = 8, steps: int = 1500, seed: int = 6,
+                dx: float = 1e-3):
+    """Batched workload: `count` grids, each nx, ny, nz ~ U{lo..hi} in steps of 8 cells (seed), an
+    8-cell CPML, seeded random spheres as in the throughput workload (count and radii scaled to the
+    grid, 20 % Debye) and one randomly placed 1e7-ohm Ez point source. Returns a list of Scenes."""
+    rng = SplitMix64(seed)
+    scenes = []
+    for b in range(count):
+        dims = tuple(8 * rng.integer(lo // 8, hi // 8) for _ in range(3))
+        grid = Grid.uniform((0.0, 0.0, 0.0), tuple(d * dx for d in dims), dims, pml)
+        nsph = max(4, int(200 * (min(dims) / 512.0) ** 2 * 4))
+        (eps, sig, inf, deb), tau = sphere_materials(dims, nsph, max(2, min(dims) // 40), max(4, min(dims) // 6),
+                                                     pml, rng.next_u64())
+        mats = Materials(eps, sig, inf, deb)
+        media = Media(Sheets(), Debye([(1.0 / tau, 1.0)]), [])
+        at = tuple(rng.integer(pml + 2, d - pml - 3) for d in dims)
+        ports = [_point_port("source", at)]
+        extras = Extras(max_steps=steps, decay_db=math.inf, fused_e=True, check_every=min(steps, 1000) or 1000)
+        sc = Scene(f"batch grid {b}: {dims[0]}x{dims[1]}x{dims[2]}", grid, mats, None, [], ports, [], media,
+                   Pulse(10e9, 5e9), extras)
+        sc.info.update(dims=dims, pml=pml, spheres=nsph)
+        scenes.append(sc)
+    return scenes

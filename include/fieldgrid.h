@@ -293,6 +293,35 @@ int fg_flux_gradient(fg_gpu* g, const fg_sim* sim, uint64_t driven, const fg_pul
                      const fg_flux_spec* spec, fg_flux_result* out, double* grad_eps, double* grad_sigma,
                      char* err, size_t errlen);
 
+/* ---- batches: many independent grids stepped together ----
+ * No counterpart in the reference (it runs one Sim per run() call). Each grid is a Sim with its
+ * own driven port and pulse; every step runs one persistent launch that marches the tiles of all
+ * grids from a shared work-list (the direct-load fused march), then one launch each for all
+ * grids' Debye edges, sources and port probes, captured in a CUDA graph. Each grid's results are
+ * those of stepping it alone (fused step). Grids with thin wires or resistive sheets, or that ask
+ * for a plane DFT or NTFF, are refused. With tune = 1 the batch times each candidate shape (tile
+ * 32x8, 64x4 or 32x4; persistent blocks per SM; x-planes per work item) for a few steps, keeps the
+ * fastest and resets every grid to step 0; with tune = 0 it uses the shape given. */
+typedef struct fg_batch fg_batch;
+typedef struct fg_batch_options {
+    int tune;
+    int tile;                /* 0: 32x8, 1: 64x4, 2: 32x4 (k x j) */
+    int blocks_per_sm;       /* 0: the occupancy limit */
+    int seg;                 /* x-planes per work item; 0: 32 */
+    int graph_steps;         /* steps per captured graph; 0: 10 */
+} fg_batch_options;
+
+int fg_batch_new(fg_gpu* g, const fg_sim* const* sims, const uint64_t* driven, const fg_pulse* pulses,
+                 uint64_t count, uint64_t max_steps, const fg_batch_options* opt, fg_batch** out,
+                 char* err, size_t errlen);
+int fg_batch_step(fg_batch* b, uint64_t steps, char* err, size_t errlen);
+int fg_batch_sync(fg_batch* b);
+/* which: "series", "e" or "h" of grid `index` (as fg_session_read) */
+int fg_batch_read(fg_batch* b, uint64_t index, const char* which, float* dst, uint64_t len, char* err, size_t errlen);
+/* the shape in use (opt), the persistent launch's blocks, the tuned step time (ms) and steps taken */
+int fg_batch_info(const fg_batch* b, fg_batch_options* opt, int* persistent_blocks, double* tuned_ms, uint64_t* steps);
+void fg_batch_free(fg_batch* b);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,60 @@
+"""Batches of uneven grids (fg_batch_*): every grid's series and final fields equal stepping that
+grid alone with the fused step, bit for bit, with a fixed shape and after the autotuner."""
+import numpy as np
+import pytest
+
+from fieldgrid_b200 import fdtd
+from fieldgrid_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def scenes():
+    return W.batch_grids(count=5, lo=16, hi=48, pml=4, steps=64, seed=11)
+
+
+def alone(gpu, sc, steps):
+    sim = fdtd.Sim.try_new(*sc.args())
+    s = fdtd.Session(gpu, sim, 0, sc.pulse, sc.extras)
+    s.step(steps)
+    nn = int(np.prod(sc.grid.dims()))
+    out = (s.read("series", steps * 2), s.read("e", 3 * nn), s.read("h", 3 * nn))
+    s.close()
+    return out
+
+
+def check(gpu, b, scenes, steps):
+    for q, sc in enumerate(scenes):
+        nn = int(np.prod(sc.grid.dims()))
+        ser, e, h = alone(gpu, sc, steps)
+        assert np.array_equal(b.read(q, "series", steps * 2), ser), q
+        assert np.array_equal(b.read(q, "e", 3 * nn), e), q
+        assert np.array_equal(b.read(q, "h", 3 * nn), h), q
+        assert np.abs(e).max() > 0
+
+
+def test_a_batch_steps_each_grid_as_alone(gpu, scenes):
+    sims = [fdtd.Sim.try_new(*sc.args()) for sc in scenes]
+    b = fdtd.Batch(gpu, sims, [sc.pulse for sc in scenes], 64, tune=False, tile=1, seg=16, graph_steps=8)
+    b.step(7)    # odd counts: the single-step graphs of both parities
+    b.step(33)
+    assert b.info()["steps"] == 40
+    check(gpu, b, scenes, 40)
+    b.close()
+
+
+def test_the_tuned_batch_starts_from_step_zero(gpu, scenes):
+    sims = [fdtd.Sim.try_new(*sc.args()) for sc in scenes]
+    b = fdtd.Batch(gpu, sims, [sc.pulse for sc in scenes], 64, tune=True)
+    info = b.info()
+    assert info["steps"] == 0 and info["tuned_ms_per_step"] > 0 and info["persistent_blocks"] > 0
+    b.step(24)
+    check(gpu, b, scenes, 24)
+    b.close()
+
+
+def test_a_batch_refuses_wires_and_sheets(gpu):
+    sc = W.everything(steps=10, fused=True)
+    with pytest.raises(fdtd.FdtdError, match="no thin wires"):
+        fdtd.Batch(gpu, [fdtd.Sim.try_new(*sc.args())], [sc.pulse], 10)

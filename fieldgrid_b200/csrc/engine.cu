@@ -102,6 +102,8 @@ struct Session {
     std::vector<int4> tma_plan_blocks;  // the same list on the host
     int clean_lo[3] = {0, 0, 0}, clean_hi[3] = {0, 0, 0};
     ShellRows shell{};              // the CPML shell around the clean box
+    KAxis kax{};                    // the k axis as separate arrays, for the shell kernels
+    std::vector<float> kaxis_host;
     // adjoint support: the design edges and the ring of their recorded E^n and curl terms
     int n_design = 0;
     int4* design = nullptr;
@@ -447,13 +449,13 @@ int enqueue_step(Session& s, int parity, std::string& err) {
             // the CPML shell around the march's clean box, one warp per row
             const unsigned gb = (shell_rows + SHELL_THREADS / 32 - 1) / (SHELL_THREADS / 32);
             mark("shell_h");
-            k_shell_h<<<gb, SHELL_THREADS, 0, st>>>(g, s.shell, e_in, h_in, h_out, parity ? s.psi_h2 : s.psi,
+            k_shell_h<<<gb, SHELL_THREADS, 0, st>>>(g, s.shell, s.kax, e_in, h_in, h_out, parity ? s.psi_h2 : s.psi,
                                                     parity ? s.psi : s.psi_h2, s.sc.k_mu);
             mark("shell_e");
             switch (s.cid_bytes) {
-                case 1: k_shell_e<uint8_t><<<gb, SHELL_THREADS, 0, st>>>(g, s.shell, (const uint8_t*)s.node_class, s.classes, h_out, e_in, e_out, s.psi); break;
-                case 2: k_shell_e<uint16_t><<<gb, SHELL_THREADS, 0, st>>>(g, s.shell, (const uint16_t*)s.node_class, s.classes, h_out, e_in, e_out, s.psi); break;
-                default: k_shell_e<uint32_t><<<gb, SHELL_THREADS, 0, st>>>(g, s.shell, (const uint32_t*)s.node_class, s.classes, h_out, e_in, e_out, s.psi); break;
+                case 1: k_shell_e<uint8_t><<<gb, SHELL_THREADS, 0, st>>>(g, s.shell, s.kax, (const uint8_t*)s.node_class, s.classes, h_out, e_in, e_out, s.psi); break;
+                case 2: k_shell_e<uint16_t><<<gb, SHELL_THREADS, 0, st>>>(g, s.shell, s.kax, (const uint16_t*)s.node_class, s.classes, h_out, e_in, e_out, s.psi); break;
+                default: k_shell_e<uint32_t><<<gb, SHELL_THREADS, 0, st>>>(g, s.shell, s.kax, (const uint32_t*)s.node_class, s.classes, h_out, e_in, e_out, s.psi); break;
             }
         }
         if (s.n_sheets) {
@@ -745,6 +747,7 @@ int session_new(Gpu* gpu, const HostSim& sim, const RunSpec& rs, Session** out, 
     need += carve_size(nnp * size_t(s->cid_bytes));
     need += carve_size(ncls * sizeof(DevCoef));
     need += carve_size((n0 + n1 + n2) * sizeof(AxisNode));
+    need += carve_size(10 * n2 * 4);
     need += carve_size(64);
     need += carve_size(std::max<uint64_t>(s->series_len, 1) * 4);
     need += carve_size(std::max<uint64_t>(s->plane_len, 1) * 4);
@@ -791,6 +794,7 @@ int session_new(Gpu* gpu, const HostSim& sim, const RunSpec& rs, Session** out, 
     s->node_class = carve<char>(cur, nnp * size_t(s->cid_bytes));
     s->classes = carve<DevCoef>(cur, ncls);
     s->axes = carve<AxisNode>(cur, n0 + n1 + n2);
+    float* kax = carve<float>(cur, 10 * n2);   // the k axis as separate arrays (KAxis)
     s->counter = carve<unsigned>(cur, 16);
     s->series = carve<float>(cur, std::max<uint64_t>(s->series_len, 1));
     s->plane = carve<float>(cur, std::max<uint64_t>(s->plane_len, 1));
@@ -869,6 +873,20 @@ int session_new(Gpu* gpu, const HostSim& sim, const RunSpec& rs, Session** out, 
     g.ax[0] = s->axes;
     g.ax[1] = s->axes + n0;
     g.ax[2] = s->axes + n0 + n1;
+    {
+        std::vector<float> kv(10 * n2);
+        for (size_t k = 0; k < n2; ++k) {
+            const AxisNode& a = sim.ax[2].node[k];
+            const float f[8] = {a.inv_d, a.inv_dd, a.raw_inv_d, a.raw_inv_dd, a.be, a.ce, a.bh, a.ch};
+            for (int q = 0; q < 8; ++q) kv[q * n2 + k] = f[q];
+            std::memcpy(&kv[8 * n2 + k], &a.slot_e, 4);
+            std::memcpy(&kv[9 * n2 + k], &a.slot_h, 4);
+        }
+        FG_CUDA(cudaMemcpyAsync(kax, kv.data(), kv.size() * 4, cudaMemcpyHostToDevice, st));
+        s->kaxis_host = std::move(kv);   // the copy must outlive the asynchronous upload
+        s->kax = KAxis{kax, kax + n2, kax + 2 * n2, kax + 3 * n2, kax + 4 * n2, kax + 5 * n2, kax + 6 * n2,
+                       kax + 7 * n2, reinterpret_cast<const int*>(kax + 8 * n2), reinterpret_cast<const int*>(kax + 9 * n2)};
+    }
     s->h2d_bytes += ncls * sizeof(DevCoef) + axes.size() * sizeof(AxisNode);
     auto up = [&](void* dst, const void* srcp, size_t bytes) -> int {
         s->h2d_bytes += bytes;

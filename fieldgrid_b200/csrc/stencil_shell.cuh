@@ -46,6 +46,34 @@ __device__ __forceinline__ void shell_row(const Geom& g, const ShellRows& b, uns
     }
 }
 
+// The k axis's factors as separate arrays of n2 entries: a warp walking a row along k reads each
+// as one coalesced line (an AxisNode per lane would be a 40-byte-stride gather per field).
+struct KAxis {
+    const float *inv_d, *inv_dd, *raw_inv_d, *raw_inv_dd, *be, *ce, *bh, *ch;
+    const int *slot_e, *slot_h;
+};
+
+// The factors of node k that an H (F = 1) or E (F = 0) update reads; the CPML ones only inside
+// the layer.
+struct KNode {
+    float inv, raw, b, c;
+    int slot;
+};
+
+template <int F>
+__device__ __forceinline__ KNode k_node(const KAxis& kx, int k) {
+    KNode n;
+    n.inv = F ? kx.inv_d[k] : kx.inv_dd[k];
+    n.slot = F ? kx.slot_h[k] : kx.slot_e[k];
+    n.raw = n.b = n.c = 0.f;
+    if (n.slot >= 0) {
+        n.raw = F ? kx.raw_inv_d[k] : kx.raw_inv_dd[k];
+        n.b = F ? kx.bh[k] : kx.be[k];
+        n.c = F ? kx.ch[k] : kx.ce[k];
+    }
+    return n;
+}
+
 // One CPML term, r = b psi + c d raw (cpu.rs:73-99, :135-159), in the reference's operation order.
 __device__ __forceinline__ float cpml_term(float b, float psi, float c, float d, float raw) { return b * psi + c * d * raw; }
 
@@ -54,7 +82,7 @@ constexpr int SHELL_THREADS = 256;   // 8 rows per block
 // The new H of one row of shell nodes (cpu.rs:48-107): H_c = H_c - k_mu [(dE_v/du) inv_d_u + psi_u
 // - (dE_u/dv) inv_d_v - psi_v], each psi_a updated where the node's slot along a is live. All loads
 // of a node come before its stores.
-__global__ void __launch_bounds__(SHELL_THREADS) k_shell_h(Geom g, ShellRows b, const float* __restrict__ e_in,
+__global__ void __launch_bounds__(SHELL_THREADS) k_shell_h(Geom g, ShellRows b, KAxis kx, const float* __restrict__ e_in,
                                                            const float* __restrict__ h_in, float* __restrict__ h_out,
                                                            const float* __restrict__ psi_in, float* __restrict__ psi_out,
                                                            float k_mu) {
@@ -75,7 +103,7 @@ __global__ void __launch_bounds__(SHELL_THREADS) k_shell_h(Geom g, ShellRows b, 
     const long long pz = ((long long)i * g.n1 + j) * g.pw;
     for (int q = int(threadIdx.x & 31); q < len; q += 32) {
         const int k = strips && q >= b.za ? b.zb + (q - b.za) : q;
-        const AxisNode ak = g.ax[2][k];
+        const KNode ak = k_node<1>(kx, k);
         const bool in_k = k + 1 < g.n2;
         const long long id = row + k;
         const bool run0 = in_j && in_k, run1 = in_k && in_i, run2 = in_i && in_j;
@@ -85,24 +113,24 @@ __global__ void __launch_bounds__(SHELL_THREADS) k_shell_h(Geom g, ShellRows b, 
         const float ez_i = in_i ? e_in[2 * cs + id + si] : 0.f, ey_i = in_i ? e_in[cs + id + si] : 0.f;
         float hx = h_in[id], hy = h_in[cs + id], hz = h_in[2 * cs + id];
         // psi of the input set, by (component, axis): Hx (j, k), Hy (k, i), Hz (i, j)
-        const long long o0j = g.psi_off[9 + 0 * 3 + 1] + py + k, o0k = g.psi_off[9 + 0 * 3 + 2] + pz + ak.slot_h;
-        const long long o1k = g.psi_off[9 + 1 * 3 + 2] + pz + ak.slot_h, o1i = g.psi_off[9 + 1 * 3 + 0] + px + k;
+        const long long o0j = g.psi_off[9 + 0 * 3 + 1] + py + k, o0k = g.psi_off[9 + 0 * 3 + 2] + pz + ak.slot;
+        const long long o1k = g.psi_off[9 + 1 * 3 + 2] + pz + ak.slot, o1i = g.psi_off[9 + 1 * 3 + 0] + px + k;
         const long long o2i = g.psi_off[9 + 2 * 3 + 0] + px + k, o2j = g.psi_off[9 + 2 * 3 + 1] + py + k;
-        const bool lj = aj.slot_h >= 0, lk = ak.slot_h >= 0, li = ai.slot_h >= 0;
+        const bool lj = aj.slot_h >= 0, lk = ak.slot >= 0, li = ai.slot_h >= 0;
         const float s0j = run0 && lj ? psi_in[o0j] : 0.f, s0k = run0 && lk ? psi_in[o0k] : 0.f;
         const float s1k = run1 && lk ? psi_in[o1k] : 0.f, s1i = run1 && li ? psi_in[o1i] : 0.f;
         const float s2i = run2 && li ? psi_in[o2i] : 0.f, s2j = run2 && lj ? psi_in[o2j] : 0.f;
         if (run0) {   // Hx: U = j, V = k
             const float ev = ez_j - ez, eu = ey_k - ey;
-            float t1 = ev * aj.inv_d, t2 = eu * ak.inv_d;
+            float t1 = ev * aj.inv_d, t2 = eu * ak.inv;
             if (lj) { const float rr = cpml_term(aj.bh, s0j, aj.ch, ev, aj.raw_inv_d); psi_out[o0j] = rr; t1 += rr; }
-            if (lk) { const float rr = cpml_term(ak.bh, s0k, ak.ch, eu, ak.raw_inv_d); psi_out[o0k] = rr; t2 += rr; }
+            if (lk) { const float rr = cpml_term(ak.b, s0k, ak.c, eu, ak.raw); psi_out[o0k] = rr; t2 += rr; }
             hx = hx - k_mu * (t1 - t2);
         }
         if (run1) {   // Hy: U = k, V = i
             const float ev = ex_k - ex, eu = ez_i - ez;
-            float t1 = ev * ak.inv_d, t2 = eu * ai.inv_d;
-            if (lk) { const float rr = cpml_term(ak.bh, s1k, ak.ch, ev, ak.raw_inv_d); psi_out[o1k] = rr; t1 += rr; }
+            float t1 = ev * ak.inv, t2 = eu * ai.inv_d;
+            if (lk) { const float rr = cpml_term(ak.b, s1k, ak.c, ev, ak.raw); psi_out[o1k] = rr; t1 += rr; }
             if (li) { const float rr = cpml_term(ai.bh, s1i, ai.ch, eu, ai.raw_inv_d); psi_out[o1i] = rr; t2 += rr; }
             hy = hy - k_mu * (t1 - t2);
         }
@@ -123,7 +151,7 @@ __global__ void __launch_bounds__(SHELL_THREADS) k_shell_h(Geom g, ShellRows b, 
 // psi_u - (dH_u/dv) inv_dd_v - psi_v], kept where cb == 0; the E psi slabs are updated in place,
 // so every psi read of a node precedes its writes.
 template <typename CID>
-__global__ void __launch_bounds__(SHELL_THREADS) k_shell_e(Geom g, ShellRows b, const CID* __restrict__ node_class,
+__global__ void __launch_bounds__(SHELL_THREADS) k_shell_e(Geom g, ShellRows b, KAxis kx, const CID* __restrict__ node_class,
                                                            const DevCoef* __restrict__ classes,
                                                            const float* __restrict__ h, const float* __restrict__ e_in,
                                                            float* __restrict__ e_out, float* __restrict__ psi) {
@@ -142,7 +170,7 @@ __global__ void __launch_bounds__(SHELL_THREADS) k_shell_e(Geom g, ShellRows b, 
     const long long pz = ((long long)i * g.n1 + j) * g.pw;
     for (int q = int(threadIdx.x & 31); q < len; q += 32) {
         const int k = strips && q >= b.za ? b.zb + (q - b.za) : q;
-        const AxisNode ak = g.ax[2][k];
+        const KNode ak = k_node<0>(kx, k);
         const long long id = row + k;
         const DevCoef cf = classes[node_class[id]];
         const bool run0 = cf.cb[0] != 0.0f && j > 0 && k > 0;
@@ -153,24 +181,24 @@ __global__ void __launch_bounds__(SHELL_THREADS) k_shell_e(Geom g, ShellRows b, 
         const float hy_k = k > 0 ? h[cs + id - 1] : 0.f, hx_k = k > 0 ? h[id - 1] : 0.f;
         const float hz_i = i > 0 ? h[2 * cs + id - si] : 0.f, hy_i = i > 0 ? h[cs + id - si] : 0.f;
         float ex = e_in[id], ey = e_in[cs + id], ez = e_in[2 * cs + id];
-        const long long o0j = g.psi_off[0 * 3 + 1] + py + k, o0k = g.psi_off[0 * 3 + 2] + pz + ak.slot_e;
-        const long long o1k = g.psi_off[1 * 3 + 2] + pz + ak.slot_e, o1i = g.psi_off[1 * 3 + 0] + px + k;
+        const long long o0j = g.psi_off[0 * 3 + 1] + py + k, o0k = g.psi_off[0 * 3 + 2] + pz + ak.slot;
+        const long long o1k = g.psi_off[1 * 3 + 2] + pz + ak.slot, o1i = g.psi_off[1 * 3 + 0] + px + k;
         const long long o2i = g.psi_off[2 * 3 + 0] + px + k, o2j = g.psi_off[2 * 3 + 1] + py + k;
-        const bool lj = aj.slot_e >= 0, lk = ak.slot_e >= 0, li = ai.slot_e >= 0;
+        const bool lj = aj.slot_e >= 0, lk = ak.slot >= 0, li = ai.slot_e >= 0;
         const float s0j = run0 && lj ? psi[o0j] : 0.f, s0k = run0 && lk ? psi[o0k] : 0.f;
         const float s1k = run1 && lk ? psi[o1k] : 0.f, s1i = run1 && li ? psi[o1i] : 0.f;
         const float s2i = run2 && li ? psi[o2i] : 0.f, s2j = run2 && lj ? psi[o2j] : 0.f;
         if (run0) {   // Ex: U = j, V = k
             const float hv = hz - hz_j, hu = hy - hy_k;
-            float t1 = hv * aj.inv_dd, t2 = hu * ak.inv_dd;
+            float t1 = hv * aj.inv_dd, t2 = hu * ak.inv;
             if (lj) { const float rr = cpml_term(aj.be, s0j, aj.ce, hv, aj.raw_inv_dd); psi[o0j] = rr; t1 += rr; }
-            if (lk) { const float rr = cpml_term(ak.be, s0k, ak.ce, hu, ak.raw_inv_dd); psi[o0k] = rr; t2 += rr; }
+            if (lk) { const float rr = cpml_term(ak.b, s0k, ak.c, hu, ak.raw); psi[o0k] = rr; t2 += rr; }
             ex = cf.ca[0] * ex + cf.cb[0] * (t1 - t2);
         }
         if (run1) {   // Ey: U = k, V = i
             const float hv = hx - hx_k, hu = hz - hz_i;
-            float t1 = hv * ak.inv_dd, t2 = hu * ai.inv_dd;
-            if (lk) { const float rr = cpml_term(ak.be, s1k, ak.ce, hv, ak.raw_inv_dd); psi[o1k] = rr; t1 += rr; }
+            float t1 = hv * ak.inv, t2 = hu * ai.inv_dd;
+            if (lk) { const float rr = cpml_term(ak.b, s1k, ak.c, hv, ak.raw); psi[o1k] = rr; t1 += rr; }
             if (li) { const float rr = cpml_term(ai.be, s1i, ai.ce, hu, ai.raw_inv_dd); psi[o1i] = rr; t2 += rr; }
             ey = cf.ca[1] * ey + cf.cb[1] * (t1 - t2);
         }

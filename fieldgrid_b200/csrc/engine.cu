@@ -191,32 +191,37 @@ struct TmaShape {
 constexpr TmaShape TMA_SHAPES[] = {{4, 2}, {3, 3}, {2, 3}};
 constexpr int TMA_NSHAPES = 3;
 
-template <typename CID, bool LOCAL, int ST>
-using TmaLS = TmaLayout<TMA_TJ, TMA_TK, CID, ST, TMA_SEGMAX, LOCAL>;
+template <typename CID, bool LOCAL, int ST, bool ZL = false>
+using TmaLS = TmaLayout<TMA_TJ, TMA_TK, CID, ST, TMA_SEGMAX, LOCAL, ZL>;
 template <typename CID, bool LOCAL = false>
 using TmaL = TmaLS<CID, LOCAL, TMA_STAGES>;
-template <typename CID, bool LOCAL, int SHAPE>
+template <typename CID, bool LOCAL, int SHAPE, bool ZL>
 constexpr auto tma_kernel_s =
-    k_tma_step<TMA_TJ, TMA_TK, CID, TMA_SHAPES[SHAPE].stages, TMA_SEGMAX, LOCAL, TMA_SHAPES[SHAPE].minb>;
+    k_tma_step<TMA_TJ, TMA_TK, CID, TMA_SHAPES[SHAPE].stages, TMA_SEGMAX, LOCAL, TMA_SHAPES[SHAPE].minb, ZL>;
 
-template <typename CID, bool LOCAL, int SHAPE>
-int tma_smem_s() { return TmaLS<CID, LOCAL, TMA_SHAPES[SHAPE].stages>::TOTAL; }
+template <typename CID, bool LOCAL, int SHAPE, bool ZL>
+int tma_smem_s() { return TmaLS<CID, LOCAL, TMA_SHAPES[SHAPE].stages, ZL>::TOTAL; }
 
-// Calls f(kernel, smem bytes) with the instantiation for (class-id width, local tables, shape).
+// Calls f(kernel, smem bytes) with the instantiation for (class-id width, local tables, shape,
+// k-layer tiles).
 template <typename F>
-bool with_tma_kernel(int cid_bytes, bool local, int shape, F&& f) {
-    auto go = [&](auto sh) {
+bool with_tma_kernel(int cid_bytes, bool local, int shape, bool zl, F&& f) {
+    auto go = [&](auto sh, auto z) {
         constexpr int S = decltype(sh)::value;
-        if (local) return f(tma_kernel_s<uint8_t, true, S>, tma_smem_s<uint8_t, true, S>());
-        if (cid_bytes == 1) return f(tma_kernel_s<uint8_t, false, S>, tma_smem_s<uint8_t, false, S>());
-        if (cid_bytes == 2) return f(tma_kernel_s<uint16_t, false, S>, tma_smem_s<uint16_t, false, S>());
-        return f(tma_kernel_s<uint32_t, false, S>, tma_smem_s<uint32_t, false, S>());
+        constexpr bool Z = decltype(z)::value;
+        if (local) return f(tma_kernel_s<uint8_t, true, S, Z>, tma_smem_s<uint8_t, true, S, Z>());
+        if (cid_bytes == 1) return f(tma_kernel_s<uint8_t, false, S, Z>, tma_smem_s<uint8_t, false, S, Z>());
+        if (cid_bytes == 2) return f(tma_kernel_s<uint16_t, false, S, Z>, tma_smem_s<uint16_t, false, S, Z>());
+        return f(tma_kernel_s<uint32_t, false, S, Z>, tma_smem_s<uint32_t, false, S, Z>());
     };
-    switch (shape) {
-        case 0: return go(std::integral_constant<int, 0>{});
-        case 1: return go(std::integral_constant<int, 1>{});
-        default: return go(std::integral_constant<int, 2>{});
-    }
+    auto by_shape = [&](auto z) {
+        switch (shape) {
+            case 0: return go(std::integral_constant<int, 0>{}, z);
+            case 1: return go(std::integral_constant<int, 1>{}, z);
+            default: return go(std::integral_constant<int, 2>{}, z);
+        }
+    };
+    return zl ? by_shape(std::true_type{}) : by_shape(std::false_type{});
 }
 
 // Tiles along k over [za, zb): when the range reaches n2 and spans 64t + 1 nodes, t tiles, the
@@ -235,7 +240,8 @@ inline int tma_ktiles(int za, int zb, int n2) {
 // k0 rounded down to 16 ids), and the first tile leaves its columns below the box unwritten. The shell around it (the layer and a one-node ring) goes to
 // the shell kernels. Blocks are (k0, j0, i0, i1): a TJ x TK tile over one x-segment.
 struct CleanPlan {
-    std::vector<int4> blocks;
+    std::vector<int4> blocks;    // interior tiles first, then the zblocks tiles that reach the k layer
+    int zblocks = 0;
     int seg = 0;                 // planes per block (at most)
     int lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
     int kbase = 0;               // the tile grid's origin along k: lo[2] rounded down to 8 nodes
@@ -257,11 +263,17 @@ bool clean_range(const Axis& ax, int n, int& a, int& b) {
     return a < b;
 }
 
-CleanPlan plan_clean(const HostSim& sim, const Geom& g) {
+// With z_layer (the z-slab psi fits the march's staged boxes) the box spans every column of its
+// rows and planes, and tiles that reach the k layer run the ZL instantiation.
+CleanPlan plan_clean(const HostSim& sim, const Geom& g, bool z_layer) {
     CleanPlan out;
     const int n[3] = {g.n0, g.n1, g.n2};
     for (int a = 0; a < 3; ++a)
-        if (!clean_range(sim.ax[a], n[a], out.lo[a], out.hi[a])) return out;
+        if (!clean_range(sim.ax[a], n[a], out.lo[a], out.hi[a]) && !(a == 2 && z_layer)) return out;
+    if (z_layer) {
+        out.lo[2] = 0;
+        out.hi[2] = g.n2;
+    }
     out.lo[2] = (out.lo[2] + 1) & ~1;
     if (out.hi[2] < g.n2) out.hi[2] = out.lo[2] + ((out.hi[2] - out.lo[2]) & ~1);
     if (out.lo[2] >= out.hi[2]) return out;
@@ -274,12 +286,20 @@ CleanPlan plan_clean(const HostSim& sim, const Geom& g) {
     while (seg > 8 && (long long)kt * jt * ((xw + seg - 1) / seg) < 148 * 3 * 6) seg /= 2;
     out.seg = seg;
     const int ns = (xw + seg - 1) / seg;
+    auto hot_k = [&](int k) { return sim.ax[2].node[size_t(k)].slot_e >= 0 || sim.ax[2].node[size_t(k)].slot_h >= 0; };
+    std::vector<int4> zl;
     for (int q = 0; q < ns; ++q) {
         const int i0 = out.lo[0] + int((long long)xw * q / ns), i1 = out.lo[0] + int((long long)xw * (q + 1) / ns);
         for (int by = 0; by < jt; ++by)
-            for (int bx = 0; bx < kt; ++bx)
-                out.blocks.push_back(make_int4(out.kbase + bx * TMA_TK, out.lo[1] + by * TMA_TJ, i0, i1));
+            for (int bx = 0; bx < kt; ++bx) {
+                const int k0 = out.kbase + bx * TMA_TK;
+                bool edge = false;   // a column of the tile, its halo column or right-edge column is in the layer
+                for (int k = std::max(k0 - 1, 0); k <= std::min(k0 + TMA_TK, g.n2 - 1); ++k) edge = edge || hot_k(k);
+                (edge ? zl : out.blocks).push_back(make_int4(k0, out.lo[1] + by * TMA_TJ, i0, i1));
+            }
     }
+    out.zblocks = int(zl.size());
+    out.blocks.insert(out.blocks.end(), zl.begin(), zl.end());
     // the shell rows around the clean box
     ShellRows& sr = out.shell;
     sr.xa = out.lo[0]; sr.xb = out.hi[0];
@@ -377,13 +397,28 @@ void plan_tma(Session& s) {
     const cuuint64_t cstr[2] = {cuuint64_t(g.p2) * b, cuuint64_t(g.n1) * g.p2 * b};
     const cuuint32_t cbox[3] = {cuuint32_t(TmaL<float>::CW), cuuint32_t(TmaL<float>::CR), 1};
     if (!encode(&t.c, dt, s.local ? (void*)s.local_ids : s.node_class, 3, cdims, cstr, cbox, t.why)) return;
+    // z-slab psi for the k-layer tiles: (slot, j, i, component) over each field's two adjacent z slabs
+    t.pz = t.zblocks > 0;
+    if (t.pz) {
+        const long long zlen = g.psi_off[1 * 3 + 2] - g.psi_off[0 * 3 + 2];  // slab stride, 128-byte multiple
+        const cuuint64_t zd[4] = {cuuint64_t(g.pw), cuuint64_t(g.n1), cuuint64_t(g.n0), 2};
+        const cuuint64_t zs[3] = {cuuint64_t(g.pw) * 4, cuuint64_t(g.n1) * g.pw * 4, cuuint64_t(zlen) * 4};
+        const cuuint32_t zb[4] = {cuuint32_t(g.pw), cuuint32_t(TMA_TJ + 1), 1, 2};
+        if (!encode(&t.pze, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, s.psi + g.psi_off[0 * 3 + 2], 4, zd, zs, zb, t.why)) return;
+        float* hsets[2] = {s.psi, s.psi_h2};  // the H slabs read by a step whose input set is 0 / 1
+        for (int q = 0; q < 2; ++q)
+            if (!encode(&t.pzh[q], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, hsets[q] + g.psi_off[9 + 0 * 3 + 2], 4, zd, zs, zb,
+                        t.why))
+                return;
+    }
     cudaError_t ce = cudaSuccess;
     for (int sh = 0; sh < TMA_NSHAPES && ce == cudaSuccess; ++sh)
-        with_tma_kernel(b, s.local, sh, [&](auto kern, int smem) {
-            ce = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-            if (sh == t.shape) t.smem = smem;
-            return true;
-        });
+        for (int z = 0; z < 2 && ce == cudaSuccess; ++z)
+            with_tma_kernel(b, s.local, sh, z != 0, [&](auto kern, int smem) {
+                ce = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+                if (sh == t.shape) t.smem = std::max(t.smem, smem);
+                return true;
+            });
     if (ce != cudaSuccess) { t.why = std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(ce); return; }
     if (!s.tma_blocks) { t.why = "no block list"; return; }
     // every TMA box origin along k must sit on 16 bytes: k0 - 4 floats, and k0 & ~15 class ids
@@ -392,14 +427,27 @@ void plan_tma(Session& s) {
     t.ok = true;
 }
 
-int launch_tma(Session& s, int parity, float* e_out, float* h_out) {
+int launch_tma(Session& s, int parity, float* e_out, float* h_out, float* psi_h_out) {
     const TmaPlan& t = s.tma;
     TmaArgs a{s.geom, s.classes, e_out, h_out, s.sc.k_mu, s.clean_lo[2], s.clean_hi[1], s.clean_hi[2], s.tma_blocks,
-              s.tables, s.counter, s.error};
-    with_tma_kernel(s.cid_bytes, s.local, t.shape, [&](auto kern, int smem) {
-        kern<<<unsigned(t.blocks), TMA_CONSUMERS + 32, smem, s.stream>>>(t.e[parity], t.h[parity], t.c, a);
-        return true;
-    });
+              0, 1, s.psi, psi_h_out, s.tables, s.counter, s.error};
+    const int inner = t.blocks - t.zblocks;
+    // without k-layer tiles the last two maps are never read
+    const CUtensorMap& pze = t.pz ? t.pze : t.c;
+    const CUtensorMap& pzh = t.pz ? t.pzh[parity] : t.c;
+    if (inner > 0)
+        with_tma_kernel(s.cid_bytes, s.local, t.shape, false, [&](auto kern, int smem) {
+            kern<<<unsigned(inner), TMA_CONSUMERS + 32, smem, s.stream>>>(t.e[parity], t.h[parity], t.c, pze, pzh, a);
+            return true;
+        });
+    if (t.zblocks > 0) {
+        a.block0 = inner;
+        a.bump = inner == 0;
+        with_tma_kernel(s.cid_bytes, s.local, t.shape, true, [&](auto kern, int smem) {
+            kern<<<unsigned(t.zblocks), TMA_CONSUMERS + 32, smem, s.stream>>>(t.e[parity], t.h[parity], t.c, pze, pzh, a);
+            return true;
+        });
+    }
     return cudaPeekAtLastError() == cudaSuccess ? 0 : 1;
 }
 
@@ -439,7 +487,7 @@ int enqueue_step(Session& s, int parity, std::string& err) {
         }
         mark("fused_step");
         int rc = s.tma.ok
-                     ? launch_tma(s, parity, e_out, h_out)
+                     ? launch_tma(s, parity, e_out, h_out, parity ? s.psi : s.psi_h2)
                      : launch_fused(s.shape, s.cid_bytes, g, s.node_class, s.classes, e_in, h_in, e_out, h_out, s.psi,
                                     parity ? s.psi_h2 : s.psi, parity ? s.psi : s.psi_h2, s.sc.k_mu, s.counter,
                                     s.n_wires > 0, st);
@@ -499,6 +547,7 @@ int enqueue_step(Session& s, int parity, std::string& err) {
 uint64_t count_launches(const Session& s) {
     uint64_t n = 1;  // the field update (fused) or H update (separate)
     if (s.tma.ok && s.shell.ra + s.shell.rb + s.shell.rc > 0) n += 2;  // the CPML shell around the TMA march
+    if (s.tma.ok && s.tma.zblocks > 0 && s.tma.blocks > s.tma.zblocks) n++;  // the k-layer tiles
     if (!s.fused) n += 1 + (s.n_debye ? 1 : 0);
     if (s.n_wires) n++;
     if (s.n_sheets) n += 2;
@@ -731,7 +780,7 @@ int session_new(Gpu* gpu, const HostSim& sim, const RunSpec& rs, Session** out, 
     LocalClasses lc;
     CleanPlan cp;
     if (s->fused && rs.tma && !(std::getenv("FIELDGRID_NO_TMA") && std::getenv("FIELDGRID_NO_TMA")[0] == '1')) {
-        cp = plan_clean(sim, g);
+        cp = plan_clean(sim, g, g.pml > 0 && g.pw <= TmaL<float>::PZW);
         if (cp.ok) {
             lc = build_local(sim, g, cp);
             s->local = lc.ok;
@@ -829,6 +878,7 @@ int session_new(Gpu* gpu, const HostSim& sim, const RunSpec& rs, Session** out, 
     if (!cp.blocks.empty()) s->tma_blocks = carve<int4>(cur, cp.blocks.size());
     s->tma_plan_blocks = cp.blocks;
     s->tma.blocks = int(cp.blocks.size());
+    s->tma.zblocks = cp.zblocks;
     s->tma.seg = cp.seg;
     s->shell = cp.shell;
     for (int q = 0; q < 3; ++q) { s->clean_lo[q] = cp.lo[q]; s->clean_hi[q] = cp.hi[q]; }
@@ -937,7 +987,7 @@ int session_new(Gpu* gpu, const HostSim& sim, const RunSpec& rs, Session** out, 
     if (s->tma.ok)
         s->variant = "TMA fused march, tile " + std::to_string(s->tma.tj) + "x" + std::to_string(s->tma.tk) + ", " +
                      std::to_string(s->tma.seg) + " planes per block, " + std::to_string(s->tma.blocks) +
-                     " blocks on the clean box, CPML shell of " +
+                     " blocks on the clean box (" + std::to_string(s->tma.zblocks) + " reaching the k layer), CPML shell of " +
                      std::to_string(s->shell.ra + s->shell.rb + s->shell.rc) + " rows, " +
                      std::to_string(TMA_SHAPES[s->tma.shape].stages) + " stages, " +
                      std::to_string(TMA_SHAPES[s->tma.shape].minb) + " blocks/SM, " +

@@ -108,7 +108,7 @@ constexpr uint64_t WAIT_LIMIT_NS = 2000000000ull;  // 2 s: far beyond any legiti
 // (ca[3], cb[3]) records that the block keeps in shared memory.
 constexpr int LOCAL_CLASSES = 256;
 
-template <int TJ, int TK, typename CID, int STAGES, int SEGMAX, bool LOCAL = false>
+template <int TJ, int TK, typename CID, int STAGES, int SEGMAX, bool LOCAL = false, bool ZL = false>
 struct TmaLayout {
     static constexpr int EW = TK + 8, ER = TJ + 2;   // E box: columns k0-4 .. k0+TK+3, rows j0-1 .. j0+TJ
     static constexpr int HW = TK + 8, HR = TJ + 1;   // H box: columns k0-4 .. k0+TK+3, rows j0-1 .. j0+TJ-1
@@ -118,8 +118,13 @@ struct TmaLayout {
     static constexpr int H_BYTES = 3 * HR * HW * 4;
     static constexpr int C_BYTES = CR * CW * int(sizeof(CID));
     __host__ __device__ static constexpr int al(int b) { return (b + 127) & ~127; }
-    static constexpr int STAGE = al(E_BYTES) + al(H_BYTES) + al(C_BYTES);
-    static constexpr int TX = E_BYTES + H_BYTES + C_BYTES;  // bytes one stage's copies deliver
+    // ZL (tiles that reach the k layer): per field a staged z-slab box of 2 components x
+    // (TJ + 1) rows (j0-1 .. j0+TJ-1) x pw slots, pw <= PZW
+    static constexpr int PZW = 32;
+    static constexpr int PZ_FIELD = 2 * (TJ + 1) * PZW * 4;
+    static constexpr int PZ_OFF = al(E_BYTES) + al(H_BYTES) + al(C_BYTES);
+    static constexpr int STAGE = PZ_OFF + (ZL ? 2 * PZ_FIELD : 0);
+    static constexpr int TX = E_BYTES + H_BYTES + C_BYTES;  // bytes one stage's field copies deliver
     static constexpr int HN = al(3 * NR * NW * 4);
     static constexpr int NAX = (TJ + 2) + (TK + 4) + (SEGMAX + 2);
     static constexpr int AX = al(NAX * int(sizeof(AxisNode)));
@@ -136,6 +141,10 @@ struct TmaArgs {
     float k_mu;
     int kbeg, jend, kend;                // the clean box: rows < jend, columns kbeg .. kend-1 are owned
     const int4* blocks;                  // per block: (k0, j0, i0, i1) of its tile and x-segment
+    int block0;                          // this launch's first entry of `blocks`
+    int bump;                            // this launch opens the step (raises the step counter)
+    float* psi_e;                        // ZL: the E psi slabs (z slabs updated in place)
+    float* psi_h_out;                    // ZL: the H psi slabs of the output set
     const float* tables;                 // LOCAL: per block (entry of `blocks`), LOCAL_CLASSES x (ca[3], cb[3])
     unsigned* counter;
     int* error;
@@ -159,9 +168,37 @@ struct CoefRef {          // three ca then three cb
     float ca[3], cb[3];
 };
 
+// The k-layer CPML term of one point (cpu.rs:65-102 for H, :125-162 for E) for the two curl
+// components that differentiate along k (CA = 0 in t[0][1], CB = 1 in t[1][0]), with the old psi
+// from the block's staged z box (`zrow` = the point's row, `zc` = the component stride); owned
+// points store the new psi (H: to the output set; E: in place).
+template <int F>   // 1: H (bh, ch, raw_inv_d), 0: E (be, ce, raw_inv_dd)
+__device__ __forceinline__ void z_terms(const TmaArgs& a, const AxisNode& ak, const float (&d)[3][2],
+                                        float (&t)[3][2], bool run0, bool run1, const float* zrow, int zc, int i,
+                                        int j, bool own) {
+    const int sl = F ? ak.slot_h : ak.slot_e;
+    if (sl < 0) return;
+    const Geom& g = a.g;
+    const float bb = F ? ak.bh : ak.be, cc = F ? ak.ch : ak.ce, raw = F ? ak.raw_inv_d : ak.raw_inv_dd;
+    const long long o = ((long long)i * g.n1 + j) * g.pw + sl;
+    float* dst = F ? a.psi_h_out : a.psi_e;
+    if (run0) {
+        const float r = bb * zrow[sl] + cc * d[0][1] * raw;
+        if (own) dst[g.psi_off[F * 9 + 0 * 3 + 2] + o] = r;
+        t[0][1] += r;
+    }
+    if (run1) {
+        const float r = bb * zrow[zc + sl] + cc * d[1][0] * raw;
+        if (own) dst[g.psi_off[F * 9 + 1 * 3 + 2] + o] = r;
+        t[1][0] += r;
+    }
+}
+
 // New H at one point outside the CPML (the update of cpu.rs:48-107 with no psi term).
+template <bool ZL = false>
 __device__ __forceinline__ void h_node(const TmaArgs& a, const ENb& n, float& hx, float& hy, float& hz,
-                                       const PtAxes& q, const AxisNode& ai, bool in) {
+                                       const PtAxes& q, const AxisNode& ai, bool in, const float* zrow = nullptr,
+                                       int zc = 0, int i = 0, int j = 0, bool own = false) {
     const AxisNode* ax[3] = {&ai, q.aj, q.ak};            // by axis 0 (i), 1 (j), 2 (k)
     const float d[3][2] = {{n.z_jp - n.z, n.y_kp - n.y}, {n.x_kp - n.x, n.z_ip - n.z}, {n.y_ip - n.y, n.x_jp - n.x}};
     float t[3][2];
@@ -169,6 +206,7 @@ __device__ __forceinline__ void h_node(const TmaArgs& a, const ENb& n, float& hx
     for (int c = 0; c < 3; ++c)
 #pragma unroll
         for (int u = 0; u < 2; ++u) t[c][u] = d[c][u] * ax[(c + 1 + u) % 3]->inv_d;
+    if constexpr (ZL) z_terms<1>(a, *q.ak, d, t, q.jn && q.kn, q.kn && in, zrow, zc, i, j, own);
     if (q.jn && q.kn) hx = hx - a.k_mu * (t[0][0] - t[0][1]);
     if (q.kn && in) hy = hy - a.k_mu * (t[1][0] - t[1][1]);
     if (in && q.jn) hz = hz - a.k_mu * (t[2][0] - t[2][1]);
@@ -176,9 +214,11 @@ __device__ __forceinline__ void h_node(const TmaArgs& a, const ENb& n, float& hx
 
 // New E at one owned point outside the CPML (cpu.rs:109-167); h*_jm / h*_km are the new H at
 // j-1 / k-1, py / pz the H of plane i-1.
-__device__ __forceinline__ void e_node(const CoefRef& cf, float& ex, float& ey, float& ez, float hx, float hy,
-                                       float hz, float hz_jm, float hx_jm, float hy_km, float hx_km, float py,
-                                       float pz, const PtAxes& q, const AxisNode& ai, int i, int j, int k) {
+template <bool ZL = false>
+__device__ __forceinline__ void e_node(const TmaArgs& a, const CoefRef& cf, float& ex, float& ey, float& ez, float hx,
+                                       float hy, float hz, float hz_jm, float hx_jm, float hy_km, float hx_km,
+                                       float py, float pz, const PtAxes& q, const AxisNode& ai, int i, int j, int k,
+                                       const float* zrow = nullptr, int zc = 0) {
     const AxisNode* ax[3] = {&ai, q.aj, q.ak};
     const float d[3][2] = {{hz - hz_jm, hy - hy_km}, {hx - hx_km, hz - pz}, {hy - py, hx - hx_jm}};
     float t[3][2];
@@ -186,8 +226,10 @@ __device__ __forceinline__ void e_node(const CoefRef& cf, float& ex, float& ey, 
     for (int c = 0; c < 3; ++c)
 #pragma unroll
         for (int u = 0; u < 2; ++u) t[c][u] = d[c][u] * ax[(c + 1 + u) % 3]->inv_dd;
-    if (cf.cb[0] != 0.0f && j > 0 && k > 0) ex = cf.ca[0] * ex + cf.cb[0] * (t[0][0] - t[0][1]);
-    if (cf.cb[1] != 0.0f && k > 0 && i > 0) ey = cf.ca[1] * ey + cf.cb[1] * (t[1][0] - t[1][1]);
+    const bool run0 = cf.cb[0] != 0.0f && j > 0 && k > 0, run1 = cf.cb[1] != 0.0f && k > 0 && i > 0;
+    if constexpr (ZL) z_terms<0>(a, *q.ak, d, t, run0, run1, zrow, zc, i, j, true);
+    if (run0) ex = cf.ca[0] * ex + cf.cb[0] * (t[0][0] - t[0][1]);
+    if (run1) ey = cf.ca[1] * ey + cf.cb[1] * (t[1][0] - t[1][1]);
     if (cf.cb[2] != 0.0f && i > 0 && j > 0) ez = cf.ca[2] * ez + cf.cb[2] * (t[2][0] - t[2][1]);
 }
 
@@ -218,12 +260,15 @@ __device__ __forceinline__ CoefRef coef_of(const TmaArgs& a, const float* lt, un
 // reaching the end of a grid whose node count along k is 64t + 1). Points past jend / kend are
 // computed when they exist in the grid but never written, and so are the first tile's columns
 // below kbeg; kbeg and kend are even (unless kend = n2), so a column pair is owned whole.
-template <int TJ, int TK, typename CID, int STAGES, int SEGMAX, bool LOCAL, int MINB>
+// ZL = true: tiles that reach the k layer (in clean rows and planes): the producer also stages
+// the z-slab psi of every plane, and points inside the layer add their k-layer CPML terms.
+template <int TJ, int TK, typename CID, int STAGES, int SEGMAX, bool LOCAL, int MINB, bool ZL>
 __global__ void __launch_bounds__(TMA_CONSUMERS + 32, MINB)
     k_tma_step(const __grid_constant__ CUtensorMap map_e, const __grid_constant__ CUtensorMap map_h,
-               const __grid_constant__ CUtensorMap map_c, TmaArgs a) {
+               const __grid_constant__ CUtensorMap map_c, const __grid_constant__ CUtensorMap map_pze,
+               const __grid_constant__ CUtensorMap map_pzh, TmaArgs a) {
     static_assert(TJ + 1 == TMA_CONSUMERS / 32 && TK == 64, "one warp per row, one column pair per lane");
-    using L = TmaLayout<TJ, TK, CID, STAGES, SEGMAX, LOCAL>;
+    using L = TmaLayout<TJ, TK, CID, STAGES, SEGMAX, LOCAL, ZL>;
     static_assert(!LOCAL || sizeof(CID) == 1, "local class ids are 8-bit");
     extern __shared__ __align__(128) unsigned char smem_raw[];
     unsigned char* base = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
@@ -238,12 +283,14 @@ __global__ void __launch_bounds__(TMA_CONSUMERS + 32, MINB)
 
     const Geom& g = a.g;
     const int tid = threadIdx.x;
-    const int4 bd = a.blocks[blockIdx.x];
+    const int bid = a.block0 + int(blockIdx.x);
+    const int4 bd = a.blocks[bid];
     const int k0 = bd.x, j0 = bd.y, i0 = bd.z, i1 = bd.w;
     const int p_first = i0 > 0 ? i0 - 1 : 0;   // plane i0-1 supplies H(i0-1) for the first E update
     const int p_last = i1;                     // E(i1) for the last H update (zeros past the grid)
     const bool redge = a.kend == g.n2 && k0 + TK == g.n2 - 1;
-    if ((blockIdx.x | tid) == 0) *a.counter += 1u;   // the step's first kernel opens step n
+    if (a.bump && (blockIdx.x | tid) == 0) *a.counter += 1u;   // the step's first kernel opens step n
+    const int zc = (TJ + 1) * g.pw;   // ZL: the component stride inside a staged z box
 
     if (tid == 0) {
         for (int s = 0; s < STAGES; ++s) {
@@ -260,7 +307,7 @@ __global__ void __launch_bounds__(TMA_CONSUMERS + 32, MINB)
         axj[q] = v;
     }
     if constexpr (LOCAL) {
-        const float* src = a.tables + (long long)blockIdx.x * (LOCAL_CLASSES * 6);
+        const float* src = a.tables + (long long)bid * (LOCAL_CLASSES * 6);
         for (int q = tid; q < LOCAL_CLASSES * 6; q += blockDim.x) lt[q] = src[q];
     }
     __syncthreads();
@@ -279,10 +326,15 @@ __global__ void __launch_bounds__(TMA_CONSUMERS + 32, MINB)
                 return;
             }
             unsigned char* st = stages + s * L::STAGE;
-            tma::mbar_expect_tx(&full[s], L::TX);
+            const bool zp = ZL && p < i1;   // plane i1 supplies E only
+            tma::mbar_expect_tx(&full[s], L::TX + (zp ? 2 * 2 * zc * 4 : 0));
             tma::load_4d(st, &map_e, &full[s], k0 - 4, j0 - 1, p, 0);
             tma::load_4d(st + L::al(L::E_BYTES), &map_h, &full[s], k0 - 4, j0 - 1, p, 0);
             tma::load_3d(st + L::al(L::E_BYTES) + L::al(L::H_BYTES), &map_c, &full[s], k0 & ~15, j0, p);
+            if (zp) {
+                tma::load_4d(st + L::PZ_OFF, &map_pze, &full[s], 0, j0 - 1, p, 0);
+                tma::load_4d(st + L::PZ_OFF + L::PZ_FIELD, &map_pzh, &full[s], 0, j0 - 1, p, 0);
+            }
         }
         return;
     }
@@ -328,6 +380,8 @@ __global__ void __launch_bounds__(TMA_CONSUMERS + 32, MINB)
         const CID* CL = reinterpret_cast<const CID*>(stages + s * L::STAGE + L::al(L::E_BYTES) + L::al(L::H_BYTES)) +
                         (k0 & 15);
         float* hn = hn_all + (u & 1) * (L::HN / 4);
+        const float* ZE = ZL ? reinterpret_cast<const float*>(stages + s * L::STAGE + L::PZ_OFF) : nullptr;
+        const float* ZH = ZL ? ZE + L::PZ_FIELD / 4 : nullptr;
         const int i = p;
         const AxisNode& ai = axi[u];
         const bool in = i + 1 < g.n0;
@@ -353,8 +407,9 @@ __global__ void __launch_bounds__(TMA_CONSUMERS + 32, MINB)
             const float2 hz = *reinterpret_cast<const float2*>(H + 2 * HC + ho);
             hx0 = hx.x; hy0 = hy.x; hz0 = hz.x;
             hx1 = hx.y; hy1 = hy.y; hz1 = hz.y;
-            h_node(a, nb0, hx0, hy0, hz0, q0, ai, in);
-            if (live1) h_node(a, nb1, hx1, hy1, hz1, q1, ai, in);
+            const float* zr = ZL ? ZH + (r + 1) * g.pw : nullptr;
+            h_node<ZL>(a, nb0, hx0, hy0, hz0, q0, ai, in, zr, zc, i, jj, own);
+            if (live1) h_node<ZL>(a, nb1, hx1, hy1, hz1, q1, ai, in, zr, zc, i, jj, own);
             *reinterpret_cast<float2*>(hn + no) = make_float2(hx0, hx1);
             *reinterpret_cast<float2*>(hn + NC + no) = make_float2(hy0, hy1);
             *reinterpret_cast<float2*>(hn + 2 * NC + no) = make_float2(hz0, hz1);
@@ -375,7 +430,7 @@ __global__ void __launch_bounds__(TMA_CONSUMERS + 32, MINB)
             hxx = H[xho];
             hyx = H[HC + xho];
             hzx = H[2 * HC + xho];
-            h_node(a, nx, hxx, hyx, hzx, qx, ai, in);
+            h_node<ZL>(a, nx, hxx, hyx, hzx, qx, ai, in, ZL ? ZH + (xr + 1) * g.pw : nullptr, zc, i, xj, xown && !pre);
             hn[xno] = hxx;
             hn[NC + xno] = hyx;
             hn[2 * NC + xno] = hzx;
@@ -413,12 +468,15 @@ __global__ void __launch_bounds__(TMA_CONSUMERS + 32, MINB)
                 const float2 hxj = *reinterpret_cast<const float2*>(hn + no - L::NW);
                 const float hyk = hn[NC + no - 1], hxk = hn[no - 1];
                 float ex0 = nb0.x, ey0 = nb0.y, ez0 = nb0.z;
-                e_node(cf0, ex0, ey0, ez0, hx0, hy0, hz0, hzj.x, hxj.x, hyk, hxk, py0, pz0, q0, ai, i, jj, kk);
+                const float* ze = ZL ? ZE + (r + 1) * g.pw : nullptr;
+                e_node<ZL>(a, cf0, ex0, ey0, ez0, hx0, hy0, hz0, hzj.x, hxj.x, hyk, hxk, py0, pz0, q0, ai, i, jj, kk, ze,
+                           zc);
                 float ex1 = 0.f, ey1 = 0.f, ez1 = 0.f;
                 if (live1) {
                     const CoefRef cf1 = coef_of<LOCAL>(a, lt, id1);
                     ex1 = nb1.x; ey1 = nb1.y; ez1 = nb1.z;
-                    e_node(cf1, ex1, ey1, ez1, hx1, hy1, hz1, hzj.y, hxj.y, hy0, hx0, py1, pz1, q1, ai, i, jj, kk + 1);
+                    e_node<ZL>(a, cf1, ex1, ey1, ez1, hx1, hy1, hz1, hzj.y, hxj.y, hy0, hx0, py1, pz1, q1, ai, i, jj,
+                               kk + 1, ze, zc);
                 }
                 float* o = a.e_out + plane + goff;
                 *reinterpret_cast<float2*>(o) = make_float2(ex0, ex1);
@@ -428,8 +486,9 @@ __global__ void __launch_bounds__(TMA_CONSUMERS + 32, MINB)
             if (xown) {
                 const CoefRef cf = coef_of<LOCAL>(a, lt, CL[xr * L::CW + xc]);
                 float ex = nx.x, ey = nx.y, ez = nx.z;
-                e_node(cf, ex, ey, ez, hxx, hyx, hzx, hn[2 * NC + xno - L::NW], hn[xno - L::NW], hn[NC + xno - 1],
-                       hn[xno - 1], pyx, pzx, qx, ai, i, xj, xk);
+                e_node<ZL>(a, cf, ex, ey, ez, hxx, hyx, hzx, hn[2 * NC + xno - L::NW], hn[xno - L::NW],
+                           hn[NC + xno - 1], hn[xno - 1], pyx, pzx, qx, ai, i, xj, xk,
+                           ZL ? ZE + (xr + 1) * g.pw : nullptr, zc);
                 float* o = a.e_out + plane + xgoff;
                 o[0] = ex;
                 o[g.cs] = ey;
@@ -446,8 +505,11 @@ __global__ void __launch_bounds__(TMA_CONSUMERS + 32, MINB)
 
 struct TmaPlan {
     CUtensorMap e[2], h[2], c;   // per input parity
+    CUtensorMap pze, pzh[2];     // the z-slab psi: E slabs, H slabs of the input set per parity
+    bool pz = false;
     int tj = 8, tk = 64, seg = 64;
     int blocks = 0;              // blocks of the clean box
+    int zblocks = 0;             // of them, the last ones: tiles that reach the k layer
     int shape = 0;               // index into the engine's kernel shapes
     int smem = 0;
     bool ok = false;

@@ -234,12 +234,11 @@ def test_the_pipelines_are_the_cuda_kernels(gpu):
     assert s.launches_per_step >= 4
     assert s.stream != 0
     s.close()
-    # 11 nodes with a 4-cell CPML leave no clean box (along k it would start at node 8): the
-    # direct-load fused march does the whole step, and agrees with the oracle
+    # 11 nodes with a 4-cell CPML: a one-node clean box whose only tile reaches the k layer
     sc = W.spheres(10, pml=4, count=2, rmin=1, rmax=2, steps=30, fused=True)
     sim = fdtd.Sim.try_new(*sc.args())
     s = fdtd.Session(gpu, sim, 0, sc.pulse, sc.extras)
-    assert "fused" in s.variant and "TMA" not in s.variant, s.variant
+    assert "TMA" in s.variant and "(1 reaching the k layer)" in s.variant, s.variant
     s.close()
     rec = fdtd.run(gpu, sim, 0, sc.pulse, sc.extras)
     ref = O.run_cpu(O.OracleSim(*sc.args(), bits=32), 0, sc.pulse, sc.extras)

@@ -112,10 +112,15 @@ __global__ void __launch_bounds__(256) k_batch_probe(const BatchInstance* __rest
 }
 
 struct BatchShape {
-    int tile = 0;             // 0: 32 x 8, 1: 64 x 4, 2: 32 x 4 (TK x TJ)
+    int tile = 0;             // 0: 32 x 8, 1: 64 x 4, 2: 32 x 4 (TK x TJ); 3: graph branches
     int blocks_per_sm = 0;    // persistent blocks per SM; 0: the occupancy limit
     int seg = 32;             // x-planes per work item
 };
+
+// tile 3 is the other execution mode: one graph branch per grid, each running that grid's own
+// step (TMA march where it has a clean box, CPML shell, Debye, sources, probes) on its stream;
+// branches run concurrently
+constexpr int BATCH_BRANCHES = 3;
 
 constexpr int BATCH_TILES[3][2] = {{32, 8}, {64, 4}, {32, 4}};
 
@@ -138,6 +143,8 @@ struct Batch {
     cudaGraphExec_t graph_many = nullptr, graph_one[2] = {nullptr, nullptr};
     double tuned_ms = 0;      // ms per step of the chosen shape while tuning
     std::vector<std::pair<BatchShape, double>> trials;
+    cudaEvent_t fork = nullptr;        // graph branches: the fork and one join per grid
+    std::vector<cudaEvent_t> join;
 };
 
 template <typename F>
@@ -157,6 +164,10 @@ bool with_batch_march(int cid_bytes, int tile, F&& f) {
 
 // Work items of every grid for a shape; uploads the per-grid tiling and the prefix sums.
 int batch_apply_shape(Batch& B, const BatchShape& sh, std::string& err) {
+    if (sh.tile == BATCH_BRANCHES) {
+        B.shape = sh;
+        return FG_OK;
+    }
     const int TK = BATCH_TILES[sh.tile][0], TJ = BATCH_TILES[sh.tile][1];
     std::vector<long long> items(B.s.size() + 1, 0);
     for (size_t b = 0; b < B.s.size(); ++b) {
@@ -187,6 +198,19 @@ int batch_apply_shape(Batch& B, const BatchShape& sh, std::string& err) {
 int batch_enqueue_step(Batch& B, int parity, std::string& err) {
     cudaStream_t st = B.stream;
     const int n = int(B.s.size());
+    if (B.shape.tile == BATCH_BRANCHES) {
+        // fork every grid's stream from the batch stream, step it there, join back
+        FG_CUDA(cudaEventRecord(B.fork, st));
+        for (int b = 0; b < n; ++b) {
+            Session& S = *B.s[size_t(b)];
+            FG_CUDA(cudaStreamWaitEvent(S.stream, B.fork, 0));
+            const int rc = enqueue_step(S, parity, err);
+            if (rc) return rc;
+            FG_CUDA(cudaEventRecord(B.join[size_t(b)], S.stream));
+            FG_CUDA(cudaStreamWaitEvent(st, B.join[size_t(b)], 0));
+        }
+        return FG_OK;
+    }
     k_batch_begin<<<(n + 127) / 128, 128, 0, st>>>(B.d_inst, n, B.d_queue);
     with_batch_march(B.cid_bytes, B.shape.tile, [&](auto kern, int tk, int tj) {
         kern<<<B.persistent_blocks, dim3(tk, tj), 0, st>>>(B.d_inst, B.d_items, n, B.d_queue, parity);
@@ -220,6 +244,8 @@ void batch_free(Batch* B) {
     cudaFree(B->d_ports);
     cudaFree(B->d_queue);
     for (Session* s : B->s) session_free(s);
+    if (B->fork) cudaEventDestroy(B->fork);
+    for (cudaEvent_t e : B->join) cudaEventDestroy(e);
     if (B->stream) cudaStreamDestroy(B->stream);
     delete B;
 }
@@ -228,7 +254,19 @@ int batch_capture(Batch& B, int steps, int parity0, cudaGraphExec_t* out, std::s
     cudaGraph_t graph;
     FG_CUDA(cudaStreamBeginCapture(B.stream, cudaStreamCaptureModeThreadLocal));
     int rc = FG_OK;
-    for (int q = 0; q < steps && rc == FG_OK; ++q) rc = batch_enqueue_step(B, (parity0 + q) & 1, err);
+    if (B.shape.tile == BATCH_BRANCHES) {
+        // the grids are independent: each branch runs all the graph's steps, one join at the end
+        FG_CUDA(cudaEventRecord(B.fork, B.stream));
+        for (size_t b = 0; b < B.s.size() && rc == FG_OK; ++b) {
+            Session& S = *B.s[b];
+            FG_CUDA(cudaStreamWaitEvent(S.stream, B.fork, 0));
+            for (int q = 0; q < steps && rc == FG_OK; ++q) rc = enqueue_step(S, (parity0 + q) & 1, err);
+            FG_CUDA(cudaEventRecord(B.join[b], S.stream));
+            FG_CUDA(cudaStreamWaitEvent(B.stream, B.join[b], 0));
+        }
+    }
+    for (int q = 0; q < steps && rc == FG_OK && B.shape.tile != BATCH_BRANCHES; ++q)
+        rc = batch_enqueue_step(B, (parity0 + q) & 1, err);
     cudaError_t ce = cudaStreamEndCapture(B.stream, &graph);
     if (rc) return rc;
     if (ce != cudaSuccess) { err = std::string("cudaStreamEndCapture: ") + cudaGetErrorString(ce); return FG_ERR_CUDA; }
@@ -287,9 +325,9 @@ int batch_new(Gpu* gpu, const std::vector<const HostSim*>& sims, const std::vect
         RunSpec rs = specs[b];
         if (rs.has_plane_k || rs.has_ntff) { err = "grid " + std::to_string(b) + ": a batch records no plane DFT or NTFF"; return FG_ERR_INVALID; }
         rs.fused = true;
-        rs.tma = false;
         rs.graphs = false;
         rs.cid_bytes = cid;
+        rs.tma_seg = 64;   // the other grids fill the GPU: long segments, few halo planes
         Session* s = nullptr;
         const int rc = session_new(gpu, h, rs, &s, err);
         if (rc) { err = "grid " + std::to_string(b) + ": " + err; return rc; }
@@ -332,6 +370,9 @@ int batch_new(Gpu* gpu, const std::vector<const HostSim*>& sims, const std::vect
     FG_CUDA(cudaMalloc(&B->d_edges, (n + 1) * 8));
     FG_CUDA(cudaMalloc(&B->d_ports, (n + 1) * 8));
     FG_CUDA(cudaMalloc(&B->d_queue, 8));
+    FG_CUDA(cudaEventCreateWithFlags(&B->fork, cudaEventDisableTiming));
+    B->join.assign(n, nullptr);
+    for (auto& e : B->join) FG_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     FG_CUDA(cudaMemcpy(B->d_edges, edges.data(), (n + 1) * 8, cudaMemcpyHostToDevice));
     FG_CUDA(cudaMemcpy(B->d_ports, ports.data(), (n + 1) * 8, cudaMemcpyHostToDevice));
     int rc = FG_OK;
@@ -343,21 +384,27 @@ int batch_new(Gpu* gpu, const std::vector<const HostSim*>& sims, const std::vect
         FG_CUDA(cudaEventCreate(&e1));
         double best_ms = 1e300;
         const int timed = 4;
+        std::vector<BatchShape> cands;
         for (int tile = 0; tile < 3; ++tile)
             for (int seg : {16, 32, 64})
-                for (int bps : {0, 2}) {
-                    BatchShape sh{tile, bps, seg};
-                    if ((rc = batch_apply_shape(*B, sh, err))) break;
-                    for (int q = 0; q < 2 && !rc; ++q) rc = batch_enqueue_step(*B, q & 1, err);
-                    FG_CUDA(cudaEventRecord(e0, B->stream));
-                    for (int q = 0; q < timed && !rc; ++q) rc = batch_enqueue_step(*B, q & 1, err);
-                    FG_CUDA(cudaEventRecord(e1, B->stream));
-                    FG_CUDA(cudaEventSynchronize(e1));
-                    float ms = 0;
-                    FG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-                    B->trials.push_back({sh, ms / timed});
-                    if (ms / timed < best_ms) { best_ms = ms / timed; best = sh; }
-                }
+                for (int bps : {0, 2}) cands.push_back(BatchShape{tile, bps, seg});
+        cands.push_back(BatchShape{BATCH_BRANCHES, 0, 0});
+        for (const BatchShape& sh : cands) {
+            if ((rc = batch_apply_shape(*B, sh, err))) break;
+            // each candidate is timed as captured graphs of `timed` steps (launch costs included)
+            cudaGraphExec_t gx = nullptr;
+            if ((rc = batch_capture(*B, timed, 0, &gx, err))) break;
+            FG_CUDA(cudaGraphLaunch(gx, B->stream));   // warm-up
+            FG_CUDA(cudaEventRecord(e0, B->stream));
+            FG_CUDA(cudaGraphLaunch(gx, B->stream));
+            FG_CUDA(cudaEventRecord(e1, B->stream));
+            FG_CUDA(cudaEventSynchronize(e1));
+            cudaGraphExecDestroy(gx);
+            float ms = 0;
+            FG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+            B->trials.push_back({sh, ms / timed});
+            if (ms / timed < best_ms) { best_ms = ms / timed; best = sh; }
+        }
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
         if (rc) return rc;
@@ -376,7 +423,7 @@ int batch_new(Gpu* gpu, const std::vector<const HostSim*>& sims, const std::vect
 int batch_new_c(Gpu* gpu, const std::vector<const HostSim*>& sims, const std::vector<RunSpec>& specs, bool tune,
                 int tile, int blocks_per_sm, int seg, int graph_steps, Batch** out, std::string& err) {
     BatchShape sh;
-    sh.tile = std::min(std::max(tile, 0), 2);
+    sh.tile = std::min(std::max(tile, 0), BATCH_BRANCHES);
     sh.blocks_per_sm = std::max(blocks_per_sm, 0);
     sh.seg = seg > 0 ? seg : 32;
     return batch_new(gpu, sims, specs, tune, sh, graph_steps > 0 ? graph_steps : 10, out, err);

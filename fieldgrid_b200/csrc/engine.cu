@@ -265,7 +265,7 @@ bool clean_range(const Axis& ax, int n, int& a, int& b) {
 
 // With z_layer (the z-slab psi fits the march's staged boxes) the box spans every column of its
 // rows and planes, and tiles that reach the k layer run the ZL instantiation.
-CleanPlan plan_clean(const HostSim& sim, const Geom& g, bool z_layer) {
+CleanPlan plan_clean(const HostSim& sim, const Geom& g, bool z_layer, int seg_fixed) {
     CleanPlan out;
     const int n[3] = {g.n0, g.n1, g.n2};
     for (int a = 0; a < 3; ++a)
@@ -284,6 +284,7 @@ CleanPlan plan_clean(const HostSim& sim, const Geom& g, bool z_layer) {
     // x-planes per block: enough blocks for several waves of 3 blocks per SM, at most TMA_SEGMAX
     int seg = TMA_SEGMAX;
     while (seg > 8 && (long long)kt * jt * ((xw + seg - 1) / seg) < 148 * 3 * 6) seg /= 2;
+    if (seg_fixed > 0) seg = std::min(seg_fixed, TMA_SEGMAX);
     out.seg = seg;
     const int ns = (xw + seg - 1) / seg;
     auto hot_k = [&](int k) { return sim.ax[2].node[size_t(k)].slot_e >= 0 || sim.ax[2].node[size_t(k)].slot_h >= 0; };
@@ -780,7 +781,7 @@ int session_new(Gpu* gpu, const HostSim& sim, const RunSpec& rs, Session** out, 
     LocalClasses lc;
     CleanPlan cp;
     if (s->fused && rs.tma && !(std::getenv("FIELDGRID_NO_TMA") && std::getenv("FIELDGRID_NO_TMA")[0] == '1')) {
-        cp = plan_clean(sim, g, g.pml > 0 && g.pw <= TmaL<float>::PZW);
+        cp = plan_clean(sim, g, g.pml > 0 && g.pw <= TmaL<float>::PZW, rs.tma_seg);
         if (cp.ok) {
             lc = build_local(sim, g, cp);
             s->local = lc.ok;

@@ -31,6 +31,7 @@ struct RunSpec {               // pack() inputs that are not part of the Sim (ru
     bool tma = true;
     bool graphs = true;
     int cid_bytes = 0;
+    int tma_seg = 0;            // x-planes per march block; 0: enough blocks to fill the GPU alone
 };
 
 struct Session;

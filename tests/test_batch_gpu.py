@@ -44,6 +44,15 @@ def test_a_batch_steps_each_grid_as_alone(gpu, scenes):
     b.close()
 
 
+def test_graph_branches_step_each_grid_as_alone(gpu, scenes):
+    sims = [fdtd.Sim.try_new(*sc.args()) for sc in scenes]
+    b = fdtd.Batch(gpu, sims, [sc.pulse for sc in scenes], 64, tune=False, tile=3, graph_steps=4)
+    assert b.info()["tile"] == "graph branches"
+    b.step(9)
+    check(gpu, b, scenes, 9)
+    b.close()
+
+
 def test_the_tuned_batch_starts_from_step_zero(gpu, scenes):
     sims = [fdtd.Sim.try_new(*sc.args()) for sc in scenes]
     b = fdtd.Batch(gpu, sims, [sc.pulse for sc in scenes], 64, tune=True)

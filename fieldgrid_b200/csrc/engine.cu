@@ -191,37 +191,32 @@ struct TmaShape {
 constexpr TmaShape TMA_SHAPES[] = {{4, 2}, {3, 3}, {2, 3}};
 constexpr int TMA_NSHAPES = 3;
 
-template <typename CID, bool LOCAL, int ST, bool ZL = false>
-using TmaLS = TmaLayout<TMA_TJ, TMA_TK, CID, ST, TMA_SEGMAX, LOCAL, ZL>;
+template <typename CID, bool LOCAL, int ST>
+using TmaLS = TmaLayout<TMA_TJ, TMA_TK, CID, ST, TMA_SEGMAX, LOCAL, true>;
 template <typename CID, bool LOCAL = false>
 using TmaL = TmaLS<CID, LOCAL, TMA_STAGES>;
-template <typename CID, bool LOCAL, int SHAPE, bool ZL>
+template <typename CID, bool LOCAL, int SHAPE>
 constexpr auto tma_kernel_s =
-    k_tma_step<TMA_TJ, TMA_TK, CID, TMA_SHAPES[SHAPE].stages, TMA_SEGMAX, LOCAL, TMA_SHAPES[SHAPE].minb, ZL>;
+    k_tma_step<TMA_TJ, TMA_TK, CID, TMA_SHAPES[SHAPE].stages, TMA_SEGMAX, LOCAL, TMA_SHAPES[SHAPE].minb>;
 
-template <typename CID, bool LOCAL, int SHAPE, bool ZL>
-int tma_smem_s() { return TmaLS<CID, LOCAL, TMA_SHAPES[SHAPE].stages, ZL>::TOTAL; }
+template <typename CID, bool LOCAL, int SHAPE>
+int tma_smem_s() { return TmaLS<CID, LOCAL, TMA_SHAPES[SHAPE].stages>::TOTAL; }
 
-// Calls f(kernel, smem bytes) with the instantiation for (class-id width, local tables, shape,
-// k-layer tiles).
+// Calls f(kernel, smem bytes) with the instantiation for (class-id width, local tables, shape).
 template <typename F>
-bool with_tma_kernel(int cid_bytes, bool local, int shape, bool zl, F&& f) {
-    auto go = [&](auto sh, auto z) {
+bool with_tma_kernel(int cid_bytes, bool local, int shape, F&& f) {
+    auto go = [&](auto sh) {
         constexpr int S = decltype(sh)::value;
-        constexpr bool Z = decltype(z)::value;
-        if (local) return f(tma_kernel_s<uint8_t, true, S, Z>, tma_smem_s<uint8_t, true, S, Z>());
-        if (cid_bytes == 1) return f(tma_kernel_s<uint8_t, false, S, Z>, tma_smem_s<uint8_t, false, S, Z>());
-        if (cid_bytes == 2) return f(tma_kernel_s<uint16_t, false, S, Z>, tma_smem_s<uint16_t, false, S, Z>());
-        return f(tma_kernel_s<uint32_t, false, S, Z>, tma_smem_s<uint32_t, false, S, Z>());
+        if (local) return f(tma_kernel_s<uint8_t, true, S>, tma_smem_s<uint8_t, true, S>());
+        if (cid_bytes == 1) return f(tma_kernel_s<uint8_t, false, S>, tma_smem_s<uint8_t, false, S>());
+        if (cid_bytes == 2) return f(tma_kernel_s<uint16_t, false, S>, tma_smem_s<uint16_t, false, S>());
+        return f(tma_kernel_s<uint32_t, false, S>, tma_smem_s<uint32_t, false, S>());
     };
-    auto by_shape = [&](auto z) {
-        switch (shape) {
-            case 0: return go(std::integral_constant<int, 0>{}, z);
-            case 1: return go(std::integral_constant<int, 1>{}, z);
-            default: return go(std::integral_constant<int, 2>{}, z);
-        }
-    };
-    return zl ? by_shape(std::true_type{}) : by_shape(std::false_type{});
+    switch (shape) {
+        case 0: return go(std::integral_constant<int, 0>{});
+        case 1: return go(std::integral_constant<int, 1>{});
+        default: return go(std::integral_constant<int, 2>{});
+    }
 }
 
 // Tiles along k over [za, zb): when the range reaches n2 and spans 64t + 1 nodes, t tiles, the
@@ -240,7 +235,7 @@ inline int tma_ktiles(int za, int zb, int n2) {
 // k0 rounded down to 16 ids), and the first tile leaves its columns below the box unwritten. The shell around it (the layer and a one-node ring) goes to
 // the shell kernels. Blocks are (k0, j0, i0, i1): a TJ x TK tile over one x-segment.
 struct CleanPlan {
-    std::vector<int4> blocks;    // interior tiles first, then the zblocks tiles that reach the k layer
+    std::vector<int4> blocks;    // k0 | TMA_ZL_TILE for the zblocks tiles that reach the k layer
     int zblocks = 0;
     int seg = 0;                 // planes per block (at most)
     int lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
@@ -288,7 +283,6 @@ CleanPlan plan_clean(const HostSim& sim, const Geom& g, bool z_layer, int seg_fi
     out.seg = seg;
     const int ns = (xw + seg - 1) / seg;
     auto hot_k = [&](int k) { return sim.ax[2].node[size_t(k)].slot_e >= 0 || sim.ax[2].node[size_t(k)].slot_h >= 0; };
-    std::vector<int4> zl;
     for (int q = 0; q < ns; ++q) {
         const int i0 = out.lo[0] + int((long long)xw * q / ns), i1 = out.lo[0] + int((long long)xw * (q + 1) / ns);
         for (int by = 0; by < jt; ++by)
@@ -296,11 +290,10 @@ CleanPlan plan_clean(const HostSim& sim, const Geom& g, bool z_layer, int seg_fi
                 const int k0 = out.kbase + bx * TMA_TK;
                 bool edge = false;   // a column of the tile, its halo column or right-edge column is in the layer
                 for (int k = std::max(k0 - 1, 0); k <= std::min(k0 + TMA_TK, g.n2 - 1); ++k) edge = edge || hot_k(k);
-                (edge ? zl : out.blocks).push_back(make_int4(k0, out.lo[1] + by * TMA_TJ, i0, i1));
+                out.zblocks += edge;
+                out.blocks.push_back(make_int4(edge ? (k0 | TMA_ZL_TILE) : k0, out.lo[1] + by * TMA_TJ, i0, i1));
             }
     }
-    out.zblocks = int(zl.size());
-    out.blocks.insert(out.blocks.end(), zl.begin(), zl.end());
     // the shell rows around the clean box
     ShellRows& sr = out.shell;
     sr.xa = out.lo[0]; sr.xb = out.hi[0];
@@ -334,7 +327,7 @@ LocalClasses build_local(const HostSim& sim, const Geom& g, const CleanPlan& cp)
     for (long long r = 0; r < regions; ++r) {
         if (over) continue;
         const int4 b = blocks[size_t(r)];
-        const int k0 = b.x, j0 = b.y, i0 = b.z, i1 = b.w;
+        const int k0 = b.x & ~TMA_ZL_TILE, j0 = b.y, i0 = b.z, i1 = b.w;
         const int kbeg = std::max(k0, cp.lo[2]);
         int kend = std::min(k0 + TMA_TK, cp.hi[2]);
         if (cp.hi[2] == g.n2 && k0 + TMA_TK == g.n2 - 1) kend = g.n2;  // the owned right-edge column
@@ -414,17 +407,16 @@ void plan_tma(Session& s) {
     }
     cudaError_t ce = cudaSuccess;
     for (int sh = 0; sh < TMA_NSHAPES && ce == cudaSuccess; ++sh)
-        for (int z = 0; z < 2 && ce == cudaSuccess; ++z)
-            with_tma_kernel(b, s.local, sh, z != 0, [&](auto kern, int smem) {
-                ce = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-                if (sh == t.shape) t.smem = std::max(t.smem, smem);
-                return true;
-            });
+        with_tma_kernel(b, s.local, sh, [&](auto kern, int smem) {
+            ce = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+            if (sh == t.shape) t.smem = smem;
+            return true;
+        });
     if (ce != cudaSuccess) { t.why = std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(ce); return; }
     if (!s.tma_blocks) { t.why = "no block list"; return; }
     // every TMA box origin along k must sit on 16 bytes: k0 - 4 floats, and k0 & ~15 class ids
     for (const int4& bk : s.tma_plan_blocks)
-        if (bk.x % 8 != 0) { t.why = "internal: unaligned tile origin"; return; }
+        if ((bk.x & ~TMA_ZL_TILE) % 8 != 0) { t.why = "internal: unaligned tile origin"; return; }
     t.ok = true;
 }
 
@@ -432,23 +424,13 @@ int launch_tma(Session& s, int parity, float* e_out, float* h_out, float* psi_h_
     const TmaPlan& t = s.tma;
     TmaArgs a{s.geom, s.classes, e_out, h_out, s.sc.k_mu, s.clean_lo[2], s.clean_hi[1], s.clean_hi[2], s.tma_blocks,
               0, 1, s.psi, psi_h_out, s.tables, s.counter, s.error};
-    const int inner = t.blocks - t.zblocks;
     // without k-layer tiles the last two maps are never read
     const CUtensorMap& pze = t.pz ? t.pze : t.c;
     const CUtensorMap& pzh = t.pz ? t.pzh[parity] : t.c;
-    if (inner > 0)
-        with_tma_kernel(s.cid_bytes, s.local, t.shape, false, [&](auto kern, int smem) {
-            kern<<<unsigned(inner), TMA_CONSUMERS + 32, smem, s.stream>>>(t.e[parity], t.h[parity], t.c, pze, pzh, a);
-            return true;
-        });
-    if (t.zblocks > 0) {
-        a.block0 = inner;
-        a.bump = inner == 0;
-        with_tma_kernel(s.cid_bytes, s.local, t.shape, true, [&](auto kern, int smem) {
-            kern<<<unsigned(t.zblocks), TMA_CONSUMERS + 32, smem, s.stream>>>(t.e[parity], t.h[parity], t.c, pze, pzh, a);
-            return true;
-        });
-    }
+    with_tma_kernel(s.cid_bytes, s.local, t.shape, [&](auto kern, int smem) {
+        kern<<<unsigned(t.blocks), TMA_CONSUMERS + 32, smem, s.stream>>>(t.e[parity], t.h[parity], t.c, pze, pzh, a);
+        return true;
+    });
     return cudaPeekAtLastError() == cudaSuccess ? 0 : 1;
 }
 
@@ -548,7 +530,6 @@ int enqueue_step(Session& s, int parity, std::string& err) {
 uint64_t count_launches(const Session& s) {
     uint64_t n = 1;  // the field update (fused) or H update (separate)
     if (s.tma.ok && s.shell.ra + s.shell.rb + s.shell.rc > 0) n += 2;  // the CPML shell around the TMA march
-    if (s.tma.ok && s.tma.zblocks > 0 && s.tma.blocks > s.tma.zblocks) n++;  // the k-layer tiles
     if (!s.fused) n += 1 + (s.n_debye ? 1 : 0);
     if (s.n_wires) n++;
     if (s.n_sheets) n += 2;

@@ -262,16 +262,19 @@ __device__ __forceinline__ CoefRef coef_of(const TmaArgs& a, const float* lt, un
 // below kbeg; kbeg and kend are even (unless kend = n2), so a column pair is owned whole.
 // ZL = true: tiles that reach the k layer (in clean rows and planes): the producer also stages
 // the z-slab psi of every plane, and points inside the layer add their k-layer CPML terms.
-template <int TJ, int TK, typename CID, int STAGES, int SEGMAX, bool LOCAL, int MINB, bool ZL>
-__global__ void __launch_bounds__(TMA_CONSUMERS + 32, MINB)
-    k_tma_step(const __grid_constant__ CUtensorMap map_e, const __grid_constant__ CUtensorMap map_h,
-               const __grid_constant__ CUtensorMap map_c, const __grid_constant__ CUtensorMap map_pze,
-               const __grid_constant__ CUtensorMap map_pzh, TmaArgs a) {
+// A block descriptor's k0 carries this bit when the tile reaches the k layer.
+constexpr int TMA_ZL_TILE = 1 << 30;
+
+// One block's march; ZL: the tile reaches the k layer. The shared-memory layout is the ZL one for
+// both (the z boxes sit past the field boxes of each stage), so one launch runs both kinds of tile
+// in the block list's order: neighbouring tiles march together and share their halo columns in L2.
+template <int TJ, int TK, typename CID, int STAGES, int SEGMAX, bool LOCAL, bool ZL>
+__device__ __forceinline__ void tma_march(const CUtensorMap& map_e, const CUtensorMap& map_h, const CUtensorMap& map_c,
+                                          const CUtensorMap& map_pze, const CUtensorMap& map_pzh, const TmaArgs& a,
+                                          unsigned char* base) {
     static_assert(TJ + 1 == TMA_CONSUMERS / 32 && TK == 64, "one warp per row, one column pair per lane");
-    using L = TmaLayout<TJ, TK, CID, STAGES, SEGMAX, LOCAL, ZL>;
+    using L = TmaLayout<TJ, TK, CID, STAGES, SEGMAX, LOCAL, true>;
     static_assert(!LOCAL || sizeof(CID) == 1, "local class ids are 8-bit");
-    extern __shared__ __align__(128) unsigned char smem_raw[];
-    unsigned char* base = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
     unsigned char* stages = base;
     float* hn_all = reinterpret_cast<float*>(base + STAGES * L::STAGE);
     AxisNode* axj = reinterpret_cast<AxisNode*>(base + STAGES * L::STAGE + 2 * L::HN);  // rows j0-1 .. j0+TJ
@@ -285,7 +288,7 @@ __global__ void __launch_bounds__(TMA_CONSUMERS + 32, MINB)
     const int tid = threadIdx.x;
     const int bid = a.block0 + int(blockIdx.x);
     const int4 bd = a.blocks[bid];
-    const int k0 = bd.x, j0 = bd.y, i0 = bd.z, i1 = bd.w;
+    const int k0 = bd.x & ~TMA_ZL_TILE, j0 = bd.y, i0 = bd.z, i1 = bd.w;
     const int p_first = i0 > 0 ? i0 - 1 : 0;   // plane i0-1 supplies H(i0-1) for the first E update
     const int p_last = i1;                     // E(i1) for the last H update (zeros past the grid)
     const bool redge = a.kend == g.n2 && k0 + TK == g.n2 - 1;
@@ -499,6 +502,19 @@ __global__ void __launch_bounds__(TMA_CONSUMERS + 32, MINB)
         tma::mbar_arrive(&empty[s]);
     }
     // the last plane's stage (E(i1)) was waited on by the final iteration; nothing is in flight
+}
+
+template <int TJ, int TK, typename CID, int STAGES, int SEGMAX, bool LOCAL, int MINB>
+__global__ void __launch_bounds__(TMA_CONSUMERS + 32, MINB)
+    k_tma_step(const __grid_constant__ CUtensorMap map_e, const __grid_constant__ CUtensorMap map_h,
+               const __grid_constant__ CUtensorMap map_c, const __grid_constant__ CUtensorMap map_pze,
+               const __grid_constant__ CUtensorMap map_pzh, TmaArgs a) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    unsigned char* base = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
+    if (a.blocks[a.block0 + int(blockIdx.x)].x & TMA_ZL_TILE)
+        tma_march<TJ, TK, CID, STAGES, SEGMAX, LOCAL, true>(map_e, map_h, map_c, map_pze, map_pzh, a, base);
+    else
+        tma_march<TJ, TK, CID, STAGES, SEGMAX, LOCAL, false>(map_e, map_h, map_c, map_pze, map_pzh, a, base);
 }
 
 // Host side ---------------------------------------------------------------------------------

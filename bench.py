@@ -51,10 +51,14 @@ def parse():
     p.add_argument("--cpu-steps", type=int, default=8, help="full time steps the CPU baseline times")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
-    p.add_argument("--workload", choices=["throughput", "adjoint"], default="throughput",
+    p.add_argument("--workload", choices=["throughput", "adjoint", "batched"], default="throughput",
                    help="throughput: the 512^3 spheres step (the headline); adjoint: the flux-objective "
-                        "gradient over a 32x32x8 design block on 160x160x96 cells, 4000 steps")
+                        "gradient over a 32x32x8 design block on 160x160x96 cells, 4000 steps; batched: 192 "
+                        "grids of U{48..160}^3 cells stepped together vs one after another, 1500 steps")
+    p.add_argument("--count", type=int, default=192, help="batched: grids in the batch")
     p.add_argument("--checkpoints", type=int, default=64, help="adjoint: field checkpoints (0: keep the history)")
+    p.add_argument("--fd", type=int, default=32,
+                   help="adjoint: parameters checked against central differences of the FP64 device forward")
     return p.parse_args()
 
 
@@ -221,6 +225,32 @@ def run_adjoint(args):
             fwd.append((tf, f.forward_ms))
             grad.append((tg, r))
     clocks = sampler.stop()
+    # central differences (h = 1e-4) of the FP64 device forward on seeded parameters (seed 5)
+    fd = None
+    if args.fd > 0 and rank == 0:
+        r = grad[-1][1]
+        _, _, eps0, sig0 = W.flux_design(steps=spec.steps, checkpoints=args.checkpoints)
+        spec64 = fdtd.FluxSpec(spec.design_lo, spec.design_hi, spec.plane_k, spec.freq, spec.steps, precision=64)
+        rng = W.SplitMix64(5)
+        errs, t0 = [], time.perf_counter()
+        for q in range(args.fd):
+            at = tuple(rng.integer(0, n - 1) for n in spec.shape())
+            which = "eps" if q % 2 == 0 else "sigma"
+            base = eps0 if which == "eps" else sig0
+            up, dn = base.copy(), base.copy()
+            up[at] = np.float32(base[at] + 1e-4)
+            dn[at] = np.float32(base[at] - 1e-4)
+            h_eff = 0.5 * (float(up[at]) - float(dn[at]))   # the step the f32 materials carry
+            js = []
+            for arr in (up, dn):
+                s2 = scene(*((arr, sig0) if which == "eps" else (eps0, arr)))
+                js.append(fdtd.flux_gradient(g, fdtd.Sim.try_new(*s2.args()), 0, s2.pulse, spec64, grad=False).objective)
+            fdv = (js[0] - js[1]) / (2 * h_eff)
+            adj = float((r.grad_eps if which == "eps" else r.grad_sigma)[at])
+            errs.append(abs(adj - fdv) / max(abs(fdv), 1e-300))
+        fd = {"parameters": args.fd, "h": 1e-4, "reference": "FP64 forward on the device, central differences",
+              "max_rel_err": float(max(errs)), "median_rel_err": float(np.median(errs)),
+              "within_1e-3": int(sum(e <= 1e-3 for e in errs)), "seconds": time.perf_counter() - t0}
     if rank != 0:
         return 0
     dev_f = float(np.median([x[1] for x in fwd]))
@@ -241,7 +271,77 @@ def run_adjoint(args):
                 "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0,
                 "run": "fdtd.flux_gradient wall clock: setup of the session, the steps, read-back of the plane and "
                        "the gradient"},
-        "objective": r.objective, "clocks": clocks,
+        "objective": r.objective, "clocks": clocks, "fd_check": fd,
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def run_batched(args):
+    """The batched workload: the same grids stepped one after another (a session per grid, its
+    graphs, the TMA march where a clean box exists) and together (one batch); device-timed
+    (CUDA events on each stream) over all steps; value = sequential time / batched time."""
+    import numpy as np
+    import torch
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    from fieldgrid_b200 import fdtd
+    from fieldgrid_b200 import workloads as W
+    from fieldgrid_b200.gpu import Gpu, Options
+    g = Gpu.open(Options(device=torch.cuda.current_device()))
+    K = args.steps if args.steps != 2000 else 1500
+    scenes = W.batch_grids(count=args.count, steps=K)
+    t = time.perf_counter()
+    sims = [fdtd.Sim.try_new(*sc.args()) for sc in scenes]
+    t_setup = time.perf_counter() - t
+    nodes = [int(np.prod(sc.grid.dims())) for sc in scenes]
+    total = float(sum(nodes))
+    sampler = ClockSampler(device_id(int(os.environ.get("LOCAL_RANK", "0"))))
+    # one after another: each grid's own session and graphs
+    seq_ms = 0.0
+    for sc, sim in zip(scenes, sims):
+        s = fdtd.Session(g, sim, 0, sc.pulse, sc.extras)
+        s.step(2)
+        s.sync()
+        stream = torch.cuda.ExternalStream(s.stream)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        s.step(K)
+        e1.record(stream)
+        e1.synchronize()
+        seq_ms += e0.elapsed_time(e1)
+        s.close()
+    # together
+    t = time.perf_counter()
+    b = fdtd.Batch(g, sims, [sc.pulse for sc in scenes], K + 2, tune=True)
+    t_tune = time.perf_counter() - t
+    b.step(2)
+    b.sync()
+    t0 = time.perf_counter()
+    b.step(K)
+    b.sync()
+    bat_ms = (time.perf_counter() - t0) * 1e3
+    info = b.info()
+    series = [b.read(q, "series", (K + 2) * 2) for q in range(min(4, len(scenes)))]
+    b.close()
+    clocks = sampler.stop()
+    if rank != 0:
+        return 0
+    line = {
+        "metric": "batched speed-up over sequential per-grid runs", "value": seq_ms / bat_ms, "unit": "x",
+        "n_gpus": world, "steps": K, "warmup": 2, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"{len(scenes)} grids U{{48..160}}^3 cells (multiples of 8), 8-cell CPML, "
+                               f"random spheres (20% Debye), one point source each", "grids": len(scenes),
+                   "nodes_total": int(total), "nodes_min": min(nodes), "nodes_max": max(nodes)},
+        "batched_ms": bat_ms, "sequential_ms": seq_ms,
+        "batched_mcells": total * K / (bat_ms / 1e3) / 1e6, "sequential_mcells": total * K / (seq_ms / 1e3) / 1e6,
+        "tuned": info, "tune_s": t_tune, "setup_s": t_setup,
+        "timing": "sequential: CUDA events around each grid's steps on its stream, summed; batched: wall clock "
+                  "around the graph launches after a sync (one stream)",
+        "clocks": clocks,
+        "series_finite": bool(all(np.all(np.isfinite(x)) for x in series)),
     }
     print(json.dumps(line))
     return 0
@@ -253,6 +353,8 @@ def main():
         return run_reference(args)
     if args.workload == "adjoint":
         return run_adjoint(args)
+    if args.workload == "batched":
+        return run_batched(args)
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))

@@ -511,7 +511,9 @@ int fg_flux_gradient(fg_gpu* g, const fg_sim* sim, uint64_t driven, const fg_pul
     FluxResult r;
     std::string e;
     const bool want = grad_eps != nullptr;
-    int rc = flux_gradient(g->g, hs, driven, pulse->f0, pulse->fc, sp, want, r, e);
+    if (spec->precision == 64 && want) return fail(FG_ERR_INVALID, "the FP64 forward computes the objective alone", err, errlen);
+    int rc = spec->precision == 64 ? flux_objective64(g->g, hs, driven, pulse->f0, pulse->fc, sp, r, e)
+                                   : flux_gradient(g->g, hs, driven, pulse->f0, pulse->fc, sp, want, r, e);
     if (rc) return fail(rc, e, err, errlen);
     out->objective = r.J;
     out->flux_re = r.f_re;

@@ -1200,3 +1200,4 @@ uint64_t session_d2h_bytes(const Session* s) { return s->d2h_bytes; }
 
 #include "adjoint.cuh"
 #include "batch.cuh"
+#include "fp64_forward.cuh"

@@ -104,5 +104,8 @@ uint64_t batch_size(const Batch& b);
 
 int flux_gradient(Gpu* gpu, const HostSim& sim, uint64_t driven, double f0, double fc, const FluxSpec& sp,
                   bool want_grad, FluxResult& res, std::string& err);
+// The same objective from an FP64 forward on the device (fp64_forward.cuh).
+int flux_objective64(Gpu* gpu, const HostSim& sim, uint64_t driven, double f0, double fc, const FluxSpec& sp,
+                     FluxResult& res, std::string& err);
 
 }  // namespace fg

@@ -33,10 +33,17 @@ struct AxisNode {
     int32_t slot_e, slot_h;
 };
 
+// The same factors in f64 (before their rounding to f32), for the FP64 forward.
+struct AxisNode64 {
+    double inv_d, inv_dd, raw_inv_d, raw_inv_dd, be, ce, bh, ch;
+    int32_t slot_e, slot_h;
+};
+
 struct Axis {
     size_t n = 0;
     std::vector<double> d, dd;
     std::vector<AxisNode> node;
+    std::vector<AxisNode64> node64;
 };
 
 struct Edge {

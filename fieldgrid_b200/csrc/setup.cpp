@@ -56,6 +56,7 @@ Axis make_axis(const std::vector<double>& line, size_t pml, double dt) {
         a.dd[i] = (i == 0) ? a.d[0] : (i + 1 >= n ? a.d[n - 2] : 0.5 * (line[i + 1] - line[i - 1]));
     std::vector<double> ke(n, 1.0), kh(n, 1.0);
     a.node.assign(n, AxisNode{0, 0, 0, 0, 0, 0, 0, 0, -1, -1});
+    a.node64.assign(n, AxisNode64{0, 0, 0, 0, 0, 0, 0, 0, -1, -1});
     if (pml > 0 && n > 2 * pml + 2) {
         const double m = 3.0, kappa_max = 1.0, alpha_max = 0.05;
         const double left = line[pml], right = line[n - 1 - pml];
@@ -77,11 +78,19 @@ Axis make_axis(const std::vector<double>& line, size_t pml, double dt) {
         };
         for (size_t i = 0; i < n; ++i) {
             double k, b, c;
-            if (grade(line[i], k, b, c)) { ke[i] = k; a.node[i].be = float(b); a.node[i].ce = float(c); }
+            if (grade(line[i], k, b, c)) {
+                ke[i] = k;
+                a.node[i].be = float(b); a.node[i].ce = float(c);
+                a.node64[i].be = b; a.node64[i].ce = c;
+            }
             if (i < pml) a.node[i].slot_e = int32_t(i);
             else if (i > n - 1 - pml) a.node[i].slot_e = int32_t(i + 2 * pml - n);
             if (i + 1 < n) {
-                if (grade(0.5 * (line[i] + line[i + 1]), k, b, c)) { kh[i] = k; a.node[i].bh = float(b); a.node[i].ch = float(c); }
+                if (grade(0.5 * (line[i] + line[i + 1]), k, b, c)) {
+                    kh[i] = k;
+                    a.node[i].bh = float(b); a.node[i].ch = float(c);
+                    a.node64[i].bh = b; a.node64[i].ch = c;
+                }
                 if (i < pml) a.node[i].slot_h = int32_t(i);
                 else if (i >= n - 1 - pml) a.node[i].slot_h = int32_t(pml + i - (n - 1 - pml));
             }
@@ -92,6 +101,13 @@ Axis make_axis(const std::vector<double>& line, size_t pml, double dt) {
         a.node[i].inv_dd = float(1.0 / (ke[i] * a.dd[i]));
         a.node[i].raw_inv_d = float(1.0 / a.d[i]);
         a.node[i].raw_inv_dd = float(1.0 / a.dd[i]);
+        AxisNode64& w = a.node64[i];
+        w.inv_d = 1.0 / (kh[i] * a.d[i]);
+        w.inv_dd = 1.0 / (ke[i] * a.dd[i]);
+        w.raw_inv_d = 1.0 / a.d[i];
+        w.raw_inv_dd = 1.0 / a.dd[i];
+        w.slot_e = a.node[i].slot_e;
+        w.slot_h = a.node[i].slot_h;
     }
     return a;
 }

@@ -575,6 +575,7 @@ class FluxSpec:
     steps: int
     window: Optional[tuple] = None   # ((i0, j0), (i1, j1))
     checkpoints: int = 0
+    precision: int = 32              # 64: the objective alone, from an FP64 forward on the device
 
     def struct(self) -> A.fg_flux_spec:
         s = A.fg_flux_spec()
@@ -587,6 +588,7 @@ class FluxSpec:
         s.freq = float(self.freq)
         s.steps = int(self.steps)
         s.checkpoints = int(self.checkpoints)
+        s.precision = int(self.precision)
         return s
 
     def cells(self) -> int:

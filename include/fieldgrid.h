@@ -279,6 +279,9 @@ typedef struct fg_flux_spec {
     double freq;                          /* Hz */
     uint64_t steps;
     uint64_t checkpoints;
+    int32_t precision;                    /* 0 or 32: the f32 update; 64: the objective alone from an FP64
+                                             forward (f64 fields, psi, coefficients, pulse and DFT) */
+    int32_t reserved;
 } fg_flux_spec;
 
 typedef struct fg_flux_result {

@@ -77,6 +77,42 @@ def test_the_adjoint_gradient_matches_central_differences(gpu, small):
         assert abs(adj - fd) <= FD_TOL * max(abs(fd), floor), (which, at, adj, fd)
 
 
+def fp64(spec):
+    return fdtd.FluxSpec(spec.design_lo, spec.design_hi, spec.plane_k, spec.freq, spec.steps, precision=64)
+
+
+def test_the_fp64_device_forward_matches_the_fp64_oracle(gpu, small):
+    """The device's FP64 forward (the full-size FD reference) against the oracle's f64 run; they
+    differ only where setup overrode an edge (the port), kept at its f32 value on the device."""
+    scene, spec, eps0, sig0 = small
+    sc = scene()
+    r = fdtd.flux_gradient(gpu, fdtd.Sim.try_new(*sc.args()), 0, sc.pulse, fp64(spec), grad=False)
+    ref = flux_f64(sc, spec)
+    assert abs(r.objective - ref) <= 1e-5 * ref, (r.objective, ref)
+
+
+def test_the_adjoint_matches_differences_of_the_device_fp64_forward(gpu, small):
+    scene, spec, eps0, sig0 = small
+    sc = scene()
+    r = fdtd.flux_gradient(gpu, fdtd.Sim.try_new(*sc.args()), 0, sc.pulse, spec)
+    rng = W.SplitMix64(7)
+    for q in range(4):
+        at = tuple(rng.integer(0, s - 1) for s in spec.shape())
+        which = "eps" if q % 2 == 0 else "sig"
+        base = eps0 if which == "eps" else sig0
+        up, dn = base.copy(), base.copy()
+        up[at] = np.float32(base[at] + H)
+        dn[at] = np.float32(base[at] - H)
+        h_eff = 0.5 * (float(up[at]) - float(dn[at]))
+        j = []
+        for arr in (up, dn):
+            s2 = scene(*((arr, sig0) if which == "eps" else (eps0, arr)))
+            j.append(fdtd.flux_gradient(gpu, fdtd.Sim.try_new(*s2.args()), 0, s2.pulse, fp64(spec), grad=False).objective)
+        fd = (j[0] - j[1]) / (2 * h_eff)
+        adj = (r.grad_eps if which == "eps" else r.grad_sigma)[at]
+        assert abs(adj - fd) <= FD_TOL * abs(fd), (which, at, adj, fd)
+
+
 def test_checkpointed_sweep_equals_stored_history(gpu, small):
     scene, spec, eps0, sig0 = small
     sc = scene()

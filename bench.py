@@ -254,7 +254,7 @@ def run_adjoint(args):
     if rank != 0:
         return 0
     dev_f = float(np.median([x[1] for x in fwd]))
-    dev_g = float(np.median([x[1].forward_ms + x[1].recompute_ms + x[1].adjoint_ms for x in grad]))
+    dev_g = float(np.median([x[1].forward_ms + x[1].backward_ms for x in grad]))
     wall_f = float(np.median([x[0] for x in fwd]))
     wall_g = float(np.median([x[0] for x in grad]))
     r = grad[-1][1]
@@ -266,7 +266,8 @@ def run_adjoint(args):
                    "parameters": 2 * spec.cells(), "checkpoints": args.checkpoints, "segments": r.segments,
                    "segment_len": r.segment_len, "design_edges": r.design_edges, "freq_hz": spec.freq},
         "forward_ms": dev_f, "gradient_ms": dev_g,
-        "gradient_parts_ms": {"forward": r.forward_ms, "recompute": r.recompute_ms, "adjoint": r.adjoint_ms},
+        "gradient_parts_ms": {"forward": r.forward_ms, "backward": r.backward_ms, "recompute_device": r.recompute_ms,
+                              "sweep_device": r.adjoint_ms},
         "e2e": {"value": wall_g / wall_f, "unit": "x", "forward_s": wall_f, "gradient_s": wall_g,
                 "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0,
                 "run": "fdtd.flux_gradient wall clock: setup of the session, the steps, read-back of the plane and "

@@ -143,7 +143,7 @@ int flux_gradient(Gpu* gpu, const HostSim& sim, uint64_t driven, double f0, doub
     std::vector<int4> edges;
     for (const auto& e : info) edges.push_back(e.at);
     rs.design = want_grad ? &edges : nullptr;
-    rs.hist_cap = want_grad ? int(std::min<uint64_t>(L, N)) : 0;
+    rs.hist_cap = want_grad ? int(std::min<uint64_t>(S > 1 ? 2 * L : L, N)) : 0;   // checkpoints: a ring of two segments
     Session* s = nullptr;
     int rc = session_new(gpu, sim, rs, &s, err);
     if (rc) return rc;
@@ -238,13 +238,14 @@ int flux_gradient(Gpu* gpu, const HostSim& sim, uint64_t driven, double f0, doub
     // adjoint state and gradient accumulators
     const int nd = int(edges.size());
     float *lE[2] = {nullptr, nullptr}, *lH = nullptr, *lpsi[2] = {nullptr, nullptr}, *dw = nullptr;
+    float *cam = nullptr, *cbm = nullptr;
     double *ga = nullptr, *gb = nullptr;
     auto free_adj = [&] {
         cudaFree(lE[0]); cudaFree(lE[1]); cudaFree(lH); cudaFree(lpsi[0]); cudaFree(lpsi[1]);
-        cudaFree(dw); cudaFree(ga); cudaFree(gb);
+        cudaFree(dw); cudaFree(ga); cudaFree(gb); cudaFree(cam); cudaFree(cbm);
     };
     std::unique_ptr<void, std::function<void(void*)>> adj_guard((void*)1, [&](void*) { free_adj(); });
-    for (auto** p : {&lE[0], &lE[1], &lH}) FG_CUDA(cudaMalloc(p, fbytes));
+    for (auto** p : {&lE[0], &lE[1], &lH, &cam, &cbm}) FG_CUDA(cudaMalloc(p, fbytes));
     for (auto** p : {&lpsi[0], &lpsi[1]}) FG_CUDA(cudaMalloc(p, pbytes));
     FG_CUDA(cudaMalloc(&dw, wts.size() * 4));
     FG_CUDA(cudaMalloc(&ga, size_t(std::max(nd, 1)) * 8));
@@ -254,44 +255,94 @@ int flux_gradient(Gpu* gpu, const HostSim& sim, uint64_t driven, double f0, doub
     FG_CUDA(cudaMemsetAsync(ga, 0, size_t(std::max(nd, 1)) * 8, st));
     FG_CUDA(cudaMemsetAsync(gb, 0, size_t(std::max(nd, 1)) * 8, st));
     FG_CUDA(cudaMemcpyAsync(dw, wts.data(), wts.size() * 4, cudaMemcpyHostToDevice, st));
+    {
+        const dim3 blk(64, 4, 1), grd((g.n2 + 63) / 64, (g.n1 + 3) / 4, g.n0);
+        switch (s->cid_bytes) {
+            case 1: k_adj_coefs<uint8_t><<<grd, blk, 0, st>>>(g, (const uint8_t*)s->node_class, s->classes, cam, cbm); break;
+            case 2: k_adj_coefs<uint16_t><<<grd, blk, 0, st>>>(g, (const uint16_t*)s->node_class, s->classes, cam, cbm); break;
+            default: k_adj_coefs<uint32_t><<<grd, blk, 0, st>>>(g, (const uint32_t*)s->node_class, s->classes, cam, cbm); break;
+        }
+    }
 
-    // 4. backward sweep, segment by segment from the last
+    // 4. backward sweep, segment by segment from the last. With checkpoints the history is a ring of
+    // two segments: the re-run of segment q-1 (session stream) overlaps the sweep of segment q (a
+    // second stream); it waits only for the sweep of q+1, whose half of the ring it overwrites.
     const dim3 blk(64, 4, 1), grd((g.n2 + 63) / 64, (g.n1 + 3) / 4, g.n0);
     const unsigned wblocks = unsigned((wi * wj + 127) / 128), dblocks = unsigned((nd + 127) / 128);
+    cudaStream_t sw = nullptr;
+    std::vector<cudaEvent_t> evs;
+    std::unique_ptr<void, std::function<void(void*)>> sw_guard((void*)1, [&](void*) {
+        for (cudaEvent_t e : evs) cudaEventDestroy(e);
+        if (sw) cudaStreamDestroy(sw);
+    });
+    FG_CUDA(cudaStreamCreateWithFlags(&sw, cudaStreamNonBlocking));
+    auto event = [&](cudaEvent_t* e, bool timing) -> int {
+        FG_CUDA(cudaEventCreateWithFlags(e, timing ? cudaEventDefault : cudaEventDisableTiming));
+        evs.push_back(*e);
+        return FG_OK;
+    };
+    cudaEvent_t rec_done, swept[2];
+    if ((rc = event(&rec_done, false)) || (rc = event(&swept[0], false)) || (rc = event(&swept[1], false))) return rc;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> t_rec, t_sw;   // per segment, for the parts' times
+    auto recompute = [&](uint64_t q) -> int {
+        const uint64_t a = q * L, b = std::min<uint64_t>(N, a + L);
+        cudaEvent_t e0, e1;
+        int r = event(&e0, true);
+        if (!r) r = event(&e1, true);
+        if (r) return r;
+        FG_CUDA(cudaEventRecord(e0, st));
+        FG_CUDA(cudaMemcpyAsync(s->e, cks[q].e, fbytes, cudaMemcpyDeviceToDevice, st));
+        FG_CUDA(cudaMemcpyAsync(s->h, cks[q].h, fbytes, cudaMemcpyDeviceToDevice, st));
+        FG_CUDA(cudaMemcpyAsync(s->psi, cks[q].psi, pbytes, cudaMemcpyDeviceToDevice, st));
+        const unsigned cnt = unsigned(a);
+        FG_CUDA(cudaMemcpyAsync(s->counter, &cnt, sizeof(cnt), cudaMemcpyHostToDevice, st));
+        s->steps = a;
+        if ((r = set_base((long long)(a - (q & 1) * L)))) return r;   // slots of ring half q & 1
+        if ((r = session_step(s, b - a, err))) return r;
+        FG_CUDA(cudaEventRecord(e1, st));
+        FG_CUDA(cudaEventRecord(rec_done, st));
+        t_rec.push_back({e0, e1});
+        return FG_OK;
+    };
+    // the sweep stream starts after the adjoint buffers are cleared and the weights uploaded (on st)
+    cudaEvent_t ready;
+    if ((rc = event(&ready, false))) return rc;
+    FG_CUDA(cudaEventRecord(ready, st));
+    FG_CUDA(cudaStreamWaitEvent(sw, ready, 0));
+    auto b0 = now();
     int set = 0;
+    if (ckpt && (rc = recompute(S - 1))) return rc;
     for (uint64_t q = S; q-- > 0;) {
         const uint64_t a = q * L, b = std::min<uint64_t>(N, a + L);
-        if (ckpt) {
-            auto r0 = now();
-            FG_CUDA(cudaMemcpyAsync(s->e, cks[q].e, fbytes, cudaMemcpyDeviceToDevice, st));
-            FG_CUDA(cudaMemcpyAsync(s->h, cks[q].h, fbytes, cudaMemcpyDeviceToDevice, st));
-            FG_CUDA(cudaMemcpyAsync(s->psi, cks[q].psi, pbytes, cudaMemcpyDeviceToDevice, st));
-            const unsigned cnt = unsigned(a);
-            FG_CUDA(cudaMemcpyAsync(s->counter, &cnt, sizeof(cnt), cudaMemcpyHostToDevice, st));
-            s->steps = a;
-            if ((rc = set_base((long long)a))) return rc;
-            if ((rc = session_step(s, b - a, err))) return rc;
-            if ((rc = session_sync(s, err))) return rc;
-            res.recompute_ms += ms(r0, now());
-        }
-        auto a0 = now();
+        const long long half = ckpt ? (long long)((q & 1) * L) : 0;
+        cudaEvent_t e0, e1;
+        if ((rc = event(&e0, true)) || (rc = event(&e1, true))) return rc;
+        if (ckpt) FG_CUDA(cudaStreamWaitEvent(sw, rec_done, 0));
+        FG_CUDA(cudaEventRecord(e0, sw));
         for (uint64_t n = b; n-- > a;) {
-            k_adj_inject<<<wblocks, 128, 0, st>>>(g, int(sp.plane_k), int(sp.win_lo[0]), int(wi), int(sp.win_lo[1]),
+            k_adj_inject<<<wblocks, 128, 0, sw>>>(g, int(sp.plane_k), int(sp.win_lo[0]), int(wi), int(sp.win_lo[1]),
                                                   int(wj), dw, s->sc.dft, 1, (long long)n, lE[set], lH);
-            if (nd) k_adj_grad<<<dblocks, 128, 0, st>>>(g, s->design, nd, lE[set], s->hist_e, s->hist_s,
-                                                         (long long)(n - a), ga, gb);
-            switch (s->cid_bytes) {
-                case 1: k_adj_e<uint8_t><<<grd, blk, 0, st>>>(g, (const uint8_t*)s->node_class, s->classes, lE[set], lE[1 - set], lpsi[set], lpsi[1 - set], lH); break;
-                case 2: k_adj_e<uint16_t><<<grd, blk, 0, st>>>(g, (const uint16_t*)s->node_class, s->classes, lE[set], lE[1 - set], lpsi[set], lpsi[1 - set], lH); break;
-                default: k_adj_e<uint32_t><<<grd, blk, 0, st>>>(g, (const uint32_t*)s->node_class, s->classes, lE[set], lE[1 - set], lpsi[set], lpsi[1 - set], lH); break;
-            }
-            k_adj_h<<<grd, blk, 0, st>>>(g, lH, lpsi[set], lpsi[1 - set], lE[1 - set], s->sc.k_mu);
+            if (nd) k_adj_grad<<<dblocks, 128, 0, sw>>>(g, s->design, nd, lE[set], s->hist_e, s->hist_s,
+                                                         (long long)(n - a) + half, ga, gb);
+            k_adj_e<<<grd, blk, 0, sw>>>(g, cam, cbm, lE[set], lE[1 - set], lpsi[set], lpsi[1 - set], lH);
+            k_adj_h<<<grd, blk, 0, sw>>>(g, lH, lpsi[set], lpsi[1 - set], lE[1 - set], s->sc.k_mu);
             set = 1 - set;
         }
         FG_CUDA(cudaGetLastError());
-        FG_CUDA(cudaStreamSynchronize(st));
-        res.adjoint_ms += ms(a0, now());
+        FG_CUDA(cudaEventRecord(e1, sw));
+        FG_CUDA(cudaEventRecord(swept[q & 1], sw));
+        t_sw.push_back({e0, e1});
+        if (ckpt && q > 0) {
+            // segment q-1 goes to ring half (q-1) & 1, which the sweep of q+1 read
+            if (q + 1 < S) FG_CUDA(cudaStreamWaitEvent(st, swept[(q + 1) & 1], 0));
+            if ((rc = recompute(q - 1))) return rc;
+        }
     }
+    FG_CUDA(cudaStreamSynchronize(sw));
+    FG_CUDA(cudaStreamSynchronize(st));
+    res.backward_ms = ms(b0, now());
+    for (auto& pr : t_rec) { float x = 0; FG_CUDA(cudaEventElapsedTime(&x, pr.first, pr.second)); res.recompute_ms += x; }
+    for (auto& pr : t_sw) { float x = 0; FG_CUDA(cudaEventElapsedTime(&x, pr.first, pr.second)); res.adjoint_ms += x; }
 
     // 5. chain rule to the design voxels
     std::vector<double> hga, hgb;

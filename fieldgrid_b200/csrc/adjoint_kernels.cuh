@@ -44,22 +44,39 @@ __global__ void k_design_record(Geom g, const int4* __restrict__ edges, int n, c
     hist_s[slot * n + t] = t1 - t2;
 }
 
+// Each E edge's (ca, cb) where its update runs (cb != 0, off the low faces), else (1, 0): the
+// adjoint's per-step reads of the coefficients, formed once (k_adj_coefs) as flat arrays.
+template <typename CID>
+__global__ void k_adj_coefs(Geom g, const CID* __restrict__ node_class, const DevCoef* __restrict__ classes,
+                            float* __restrict__ cam, float* __restrict__ cbm) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int i = blockIdx.z;
+    if (k >= g.n2 || j >= g.n1) return;
+    const int p[3] = {i, j, k};
+    const long long id = ((long long)i * g.n1 + j) * g.p2 + k;
+    const DevCoef cf = classes[node_class[id]];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        const bool m = cf.cb[c] != 0.0f && p[(c + 1) % 3] > 0 && p[(c + 2) % 3] > 0;
+        cam[c * g.cs + id] = m ? cf.ca[c] : 1.0f;
+        cbm[c * g.cs + id] = m ? cf.cb[c] : 0.0f;
+    }
+}
+
 // The adjoints of the two H differences a, b that E edge c at p reads (cb lambda_E through the
 // inv_dd factors and the CPML terms); zero where the edge does not update or lies off the grid.
-template <typename CID>
-__device__ __forceinline__ void e_edge_lab(const Geom& g, const CID* __restrict__ node_class,
-                                           const DevCoef* __restrict__ classes, const float* __restrict__ lE,
+__device__ __forceinline__ void e_edge_lab(const Geom& g, const float* __restrict__ cbm, const float* __restrict__ lE,
                                            const float* __restrict__ lpsi, int c, int i, int j, int k, float& la,
                                            float& lb) {
     la = 0.f;
     lb = 0.f;
     if (i >= g.n0 || j >= g.n1 || k >= g.n2) return;
+    const long long id = ((long long)i * g.n1 + j) * g.p2 + k;
+    const float cb = cbm[c * g.cs + id];
+    if (cb == 0.0f) return;
     const int p[3] = {i, j, k};
     const int U = (c + 1) % 3, V = (c + 2) % 3;
-    if (p[U] == 0 || p[V] == 0) return;
-    const long long id = ((long long)i * g.n1 + j) * g.p2 + k;
-    const float cb = classes[node_class[id]].cb[c];
-    if (cb == 0.0f) return;
     const float gg = cb * lE[c * g.cs + id];
     const AxisNode& au = g.ax[U][p[U]];
     const AxisNode& av = g.ax[V][p[V]];
@@ -96,26 +113,25 @@ __device__ __forceinline__ void h_edge_lab(const Geom& g, const float* __restric
 }
 
 // Transpose of the E half of a step. Grid (ceil(n2/64), ceil(n1/4), n0), block (64, 4).
-template <typename CID>
-__global__ void __launch_bounds__(256) k_adj_e(Geom g, const CID* __restrict__ node_class,
-                                               const DevCoef* __restrict__ classes, const float* __restrict__ lE_in,
-                                               float* __restrict__ lE_out, const float* __restrict__ lpsi_in,
-                                               float* __restrict__ lpsi_out, float* __restrict__ lH) {
+__global__ void __launch_bounds__(256) k_adj_e(Geom g, const float* __restrict__ cam, const float* __restrict__ cbm,
+                                               const float* __restrict__ lE_in, float* __restrict__ lE_out,
+                                               const float* __restrict__ lpsi_in, float* __restrict__ lpsi_out,
+                                               float* __restrict__ lH) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
     const int i = blockIdx.z;
     if (k >= g.n2 || j >= g.n1) return;
     const int p[3] = {i, j, k};
     const long long id = ((long long)i * g.n1 + j) * g.p2 + k;
-    const DevCoef cf = classes[node_class[id]];
     float la[3], lb[3];
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
         const int U = (c + 1) % 3, V = (c + 2) % 3;
         const float l = lE_in[c * g.cs + id];
-        const bool m = cf.cb[c] != 0.0f && p[U] > 0 && p[V] > 0;
-        lE_out[c * g.cs + id] = m ? cf.ca[c] * l : l;
-        const float gg = m ? cf.cb[c] * l : 0.f;
+        const float cb = cbm[c * g.cs + id];
+        const bool m = cb != 0.0f;
+        lE_out[c * g.cs + id] = cam[c * g.cs + id] * l;
+        const float gg = cb * l;
         const AxisNode& au = g.ax[U][p[U]];
         const AxisNode& av = g.ax[V][p[V]];
         la[c] = gg * au.inv_dd;
@@ -135,14 +151,14 @@ __global__ void __launch_bounds__(256) k_adj_e(Geom g, const CID* __restrict__ n
     }
     // lambda_H_C += la(C+1, q) - la(C+1, q + e_(C+2)) + lb(C+2, q) - lb(C+2, q + e_(C+1))
     float na, nb, dummy;
-    e_edge_lab(g, node_class, classes, lE_in, lpsi_in, 1, i, j, k + 1, na, dummy);
-    e_edge_lab(g, node_class, classes, lE_in, lpsi_in, 2, i, j + 1, k, dummy, nb);
+    e_edge_lab(g, cbm, lE_in, lpsi_in, 1, i, j, k + 1, na, dummy);
+    e_edge_lab(g, cbm, lE_in, lpsi_in, 2, i, j + 1, k, dummy, nb);
     lH[id] += (la[1] - na) + (lb[2] - nb);
-    e_edge_lab(g, node_class, classes, lE_in, lpsi_in, 2, i + 1, j, k, na, dummy);
-    e_edge_lab(g, node_class, classes, lE_in, lpsi_in, 0, i, j, k + 1, dummy, nb);
+    e_edge_lab(g, cbm, lE_in, lpsi_in, 2, i + 1, j, k, na, dummy);
+    e_edge_lab(g, cbm, lE_in, lpsi_in, 0, i, j, k + 1, dummy, nb);
     lH[g.cs + id] += (la[2] - na) + (lb[0] - nb);
-    e_edge_lab(g, node_class, classes, lE_in, lpsi_in, 0, i, j + 1, k, na, dummy);
-    e_edge_lab(g, node_class, classes, lE_in, lpsi_in, 1, i + 1, j, k, dummy, nb);
+    e_edge_lab(g, cbm, lE_in, lpsi_in, 0, i, j + 1, k, na, dummy);
+    e_edge_lab(g, cbm, lE_in, lpsi_in, 1, i + 1, j, k, dummy, nb);
     lH[2 * g.cs + id] += (la[0] - na) + (lb[1] - nb);
 }
 

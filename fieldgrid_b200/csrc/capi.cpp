@@ -521,6 +521,7 @@ int fg_flux_gradient(fg_gpu* g, const fg_sim* sim, uint64_t driven, const fg_pul
     out->forward_ms = r.forward_ms;
     out->recompute_ms = r.recompute_ms;
     out->adjoint_ms = r.adjoint_ms;
+    out->backward_ms = r.backward_ms;
     out->segments = r.segments;
     out->segment_len = r.segment_len;
     out->design_edges = r.design_edges;

@@ -84,6 +84,7 @@ struct FluxSpec {
 struct FluxResult {
     double J = 0, f_re = 0, f_im = 0;
     double forward_ms = 0, recompute_ms = 0, adjoint_ms = 0;
+    double backward_ms = 0;             // the whole backward pass (re-runs and sweeps overlap)
     uint64_t segments = 0, segment_len = 0, design_edges = 0;
     std::vector<double> g_eps, g_sig;   // per design cell, k fastest
 };

@@ -607,6 +607,7 @@ class FluxResult:
     forward_ms: float
     recompute_ms: float
     adjoint_ms: float
+    backward_ms: float
     segments: int
     segment_len: int
     design_edges: int
@@ -633,7 +634,8 @@ def flux_gradient(g, sim: Sim, driven: int, pulse: Pulse, spec: FluxSpec, grad: 
     shp = spec.shape()
     return FluxResult(out.objective, complex(out.flux_re, out.flux_im),
                       None if ge is None else ge.reshape(shp), None if gs is None else gs.reshape(shp),
-                      out.forward_ms, out.recompute_ms, out.adjoint_ms, int(out.segments), int(out.segment_len),
+                      out.forward_ms, out.recompute_ms, out.adjoint_ms, out.backward_ms, int(out.segments),
+                      int(out.segment_len),
                       int(out.design_edges))
 
 

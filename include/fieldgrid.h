@@ -286,7 +286,8 @@ typedef struct fg_flux_spec {
 
 typedef struct fg_flux_result {
     double objective, flux_re, flux_im;   /* J, and F */
-    double forward_ms, recompute_ms, adjoint_ms;
+    double forward_ms, recompute_ms, adjoint_ms;   /* the parts' device times (re-runs and sweeps overlap) */
+    double backward_ms;                   /* the backward pass as a whole */
     uint64_t segments, segment_len, design_edges;
 } fg_flux_result;
 

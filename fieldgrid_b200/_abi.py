@@ -89,7 +89,7 @@ PROGRESS_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, u64, dbl)
 class fg_flux_spec(C.Structure):
     _fields_ = [("design_lo", C.c_uint64 * 3), ("design_hi", C.c_uint64 * 3), ("plane_k", C.c_uint64),
                 ("window_lo", C.c_uint64 * 2), ("window_hi", C.c_uint64 * 2), ("freq", C.c_double),
-                ("steps", C.c_uint64), ("checkpoints", C.c_uint64), ("precision", C.c_int32), ("reserved", C.c_int32)]
+                ("steps", C.c_uint64), ("checkpoints", C.c_uint64), ("precision", C.c_int32), ("transposes", C.c_int32)]
 
 
 class fg_flux_result(C.Structure):

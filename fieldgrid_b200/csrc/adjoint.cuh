@@ -237,25 +237,32 @@ int flux_gradient(Gpu* gpu, const HostSim& sim, uint64_t driven, double f0, doub
     for (size_t q = 0; q < wd.size(); ++q) wts[q] = float(wd[q] * scale);
     // adjoint state and gradient accumulators
     const int nd = int(edges.size());
-    float *lE[2] = {nullptr, nullptr}, *lH = nullptr, *lpsi[2] = {nullptr, nullptr}, *dw = nullptr;
-    float *cam = nullptr, *cbm = nullptr;
+    float *lE[2] = {nullptr, nullptr}, *lH[2] = {nullptr, nullptr}, *lpsi[2] = {nullptr, nullptr}, *dw = nullptr;
+    float *cam = nullptr, *cbm = nullptr;   // the separate transposes' masked coefficients
     double *ga = nullptr, *gb = nullptr;
     auto free_adj = [&] {
-        cudaFree(lE[0]); cudaFree(lE[1]); cudaFree(lH); cudaFree(lpsi[0]); cudaFree(lpsi[1]);
+        cudaFree(lE[0]); cudaFree(lE[1]); cudaFree(lH[0]); cudaFree(lH[1]); cudaFree(lpsi[0]); cudaFree(lpsi[1]);
         cudaFree(dw); cudaFree(ga); cudaFree(gb); cudaFree(cam); cudaFree(cbm);
     };
     std::unique_ptr<void, std::function<void(void*)>> adj_guard((void*)1, [&](void*) { free_adj(); });
-    for (auto** p : {&lE[0], &lE[1], &lH, &cam, &cbm}) FG_CUDA(cudaMalloc(p, fbytes));
+    const bool sep = sp.transposes == 1;
+    for (auto** p : {&lE[0], &lE[1], &lH[0]}) FG_CUDA(cudaMalloc(p, fbytes));
+    if (sep) {
+        for (auto** p : {&cam, &cbm}) FG_CUDA(cudaMalloc(p, fbytes));
+    } else {
+        FG_CUDA(cudaMalloc(&lH[1], fbytes));
+    }
     for (auto** p : {&lpsi[0], &lpsi[1]}) FG_CUDA(cudaMalloc(p, pbytes));
     FG_CUDA(cudaMalloc(&dw, wts.size() * 4));
     FG_CUDA(cudaMalloc(&ga, size_t(std::max(nd, 1)) * 8));
     FG_CUDA(cudaMalloc(&gb, size_t(std::max(nd, 1)) * 8));
-    for (float* p : {lE[0], lE[1], lH}) FG_CUDA(cudaMemsetAsync(p, 0, fbytes, st));
+    for (float* p : {lE[0], lE[1], lH[0], lH[1]})
+        if (p) FG_CUDA(cudaMemsetAsync(p, 0, fbytes, st));
     for (float* p : {lpsi[0], lpsi[1]}) FG_CUDA(cudaMemsetAsync(p, 0, pbytes, st));
     FG_CUDA(cudaMemsetAsync(ga, 0, size_t(std::max(nd, 1)) * 8, st));
     FG_CUDA(cudaMemsetAsync(gb, 0, size_t(std::max(nd, 1)) * 8, st));
     FG_CUDA(cudaMemcpyAsync(dw, wts.data(), wts.size() * 4, cudaMemcpyHostToDevice, st));
-    {
+    if (sep) {
         const dim3 blk(64, 4, 1), grd((g.n2 + 63) / 64, (g.n1 + 3) / 4, g.n0);
         switch (s->cid_bytes) {
             case 1: k_adj_coefs<uint8_t><<<grd, blk, 0, st>>>(g, (const uint8_t*)s->node_class, s->classes, cam, cbm); break;
@@ -268,6 +275,12 @@ int flux_gradient(Gpu* gpu, const HostSim& sim, uint64_t driven, double f0, doub
     // two segments: the re-run of segment q-1 (session stream) overlaps the sweep of segment q (a
     // second stream); it waits only for the sweep of q+1, whose half of the ring it overwrites.
     const dim3 blk(64, 4, 1), grd((g.n2 + 63) / 64, (g.n1 + 3) / 4, g.n0);
+    // the fused step: x-segments for about four waves of (32, 16) blocks on 148 SMs, 8 to 64 planes
+    const long long adj_tiles = (long long)((g.n2 + ADJ_KOWN - 1) / ADJ_KOWN) * ((g.n1 + ADJ_TJ - 1) / ADJ_TJ);
+    int adj_seg = 64;
+    while (adj_seg > 8 && adj_tiles * ((g.n0 + adj_seg - 1) / adj_seg) < 148 * 4) adj_seg /= 2;
+    const dim3 ablk(32, ADJ_ROWS, 1),
+        agrd((g.n2 + ADJ_KOWN - 1) / ADJ_KOWN, (g.n1 + ADJ_TJ - 1) / ADJ_TJ, (g.n0 + adj_seg - 1) / adj_seg);
     const unsigned wblocks = unsigned((wi * wj + 127) / 128), dblocks = unsigned((nd + 127) / 128);
     cudaStream_t sw = nullptr;
     std::vector<cudaEvent_t> evs;
@@ -320,12 +333,23 @@ int flux_gradient(Gpu* gpu, const HostSim& sim, uint64_t driven, double f0, doub
         if (ckpt) FG_CUDA(cudaStreamWaitEvent(sw, rec_done, 0));
         FG_CUDA(cudaEventRecord(e0, sw));
         for (uint64_t n = b; n-- > a;) {
+            float* lh = sep ? lH[0] : lH[set];
             k_adj_inject<<<wblocks, 128, 0, sw>>>(g, int(sp.plane_k), int(sp.win_lo[0]), int(wi), int(sp.win_lo[1]),
-                                                  int(wj), dw, s->sc.dft, 1, (long long)n, lE[set], lH);
+                                                  int(wj), dw, s->sc.dft, 1, (long long)n, lE[set], lh);
             if (nd) k_adj_grad<<<dblocks, 128, 0, sw>>>(g, s->design, nd, lE[set], s->hist_e, s->hist_s,
                                                          (long long)(n - a) + half, ga, gb);
-            k_adj_e<<<grd, blk, 0, sw>>>(g, cam, cbm, lE[set], lE[1 - set], lpsi[set], lpsi[1 - set], lH);
-            k_adj_h<<<grd, blk, 0, sw>>>(g, lH, lpsi[set], lpsi[1 - set], lE[1 - set], s->sc.k_mu);
+            if (sep) {
+                k_adj_e<<<grd, blk, 0, sw>>>(g, cam, cbm, lE[set], lE[1 - set], lpsi[set], lpsi[1 - set], lh);
+                k_adj_h<<<grd, blk, 0, sw>>>(g, lh, lpsi[set], lpsi[1 - set], lE[1 - set], s->sc.k_mu);
+            } else {
+                const AdjArgs aa{g, s->node_class, s->classes, lE[set], lE[1 - set], lH[set], lH[1 - set],
+                                 lpsi[set], lpsi[1 - set], s->sc.k_mu};
+                switch (s->cid_bytes) {
+                    case 1: k_adj_step<uint8_t><<<agrd, ablk, 0, sw>>>(aa, adj_seg); break;
+                    case 2: k_adj_step<uint16_t><<<agrd, ablk, 0, sw>>>(aa, adj_seg); break;
+                    default: k_adj_step<uint32_t><<<agrd, ablk, 0, sw>>>(aa, adj_seg); break;
+                }
+            }
             set = 1 - set;
         }
         FG_CUDA(cudaGetLastError());

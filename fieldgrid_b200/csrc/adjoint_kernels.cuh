@@ -208,6 +208,258 @@ __global__ void __launch_bounds__(256) k_adj_h(Geom g, const float* __restrict__
     lE[2 * g.cs + id] += (na - la[0]) + (nb - lb[1]);
 }
 
+// ---- the fused adjoint step: both transposes in one march ----
+//
+// The E transpose gives, per E edge c at p, the adjoints (la_E, lb_E) of the two H differences it
+// read; lambda_H'_C(p) = lambda_H_C(p) + la_E[C+1](p) - la_E[C+1](p + e_(C+2)) + lb_E[C+2](p)
+// - lb_E[C+2](p + e_(C+1)). The H transpose then gives, per H edge, (la_H, lb_H) from lambda_H',
+// and lambda_E_C(p) = ca lambda_E_C(p) + la_H[C+1](p - e_(C+2)) - la_H[C+1](p) + lb_H[C+2](p -
+// e_(C+1)) - lb_H[C+2](p). So lambda_H' of plane i needs E-edge terms of planes i and i + 1, and
+// lambda_E of plane i needs H-edge terms of planes i and i - 1: the forward's own data flow.
+//
+// A block marches along x over a tile of (j, k) nodes one node wider than it owns on every side:
+// warp w serves row j0 - 1 + w and lane l column k0 - 1 + l, and owns rows 1..ADJ_TJ and lanes
+// 1..30. Every thread forms the E-edge terms of its node (those of plane i + 1 one plane ahead,
+// carried in registers); all but the last row and lane form lambda_H' and the H-edge terms; the
+// owners form lambda_E. The k neighbours come by warp shuffles, the j neighbours through shared
+// memory, and x neighbours stay in registers, so no thread recomputes another's terms and the
+// warps do equal work. Every sum is formed in the order of k_adj_e and k_adj_h, so the fused step
+// equals that pair of launches bit for bit. lambda_E, lambda_H and lambda_psi all ping-pong.
+struct AdjArgs {
+    Geom g;
+    const void* node_class;
+    const DevCoef* classes;
+    const float* __restrict__ lE_in;
+    float* __restrict__ lE_out;
+    const float* __restrict__ lH_in;
+    float* __restrict__ lH_out;
+    const float* __restrict__ lpsi_in;
+    float* __restrict__ lpsi_out;
+    float k_mu;
+};
+
+// One axis node's factors as the adjoint reads them (from the axis tables, L1-resident).
+struct AdjAx {
+    float inv_dd, be, cer;   // E side; cer = ce raw_inv_dd
+    float inv_d, bh, chr;    // H side; chr = ch raw_inv_d
+    int slot_e, slot_h;
+};
+
+__device__ __forceinline__ AdjAx adj_ax(const AxisNode* n) {
+    AdjAx r;
+    r.inv_dd = __ldg(&n->inv_dd);
+    r.be = __ldg(&n->be);
+    r.cer = __ldg(&n->ce) * __ldg(&n->raw_inv_dd);
+    r.inv_d = __ldg(&n->inv_d);
+    r.bh = __ldg(&n->bh);
+    r.chr = __ldg(&n->ch) * __ldg(&n->raw_inv_d);
+    r.slot_e = __ldg(&n->slot_e);
+    r.slot_h = __ldg(&n->slot_h);
+    return r;
+}
+
+__device__ __forceinline__ AdjAx adj_axis(const Geom& g, int u, int i, int j, int k) {
+    return adj_ax(g.ax[u] + (u == 0 ? i : (u == 1 ? j : k)));
+}
+
+// E-edge c's terms at p given its coefficients: (la_E, lb_E) and ca lambda_E (le). `own` writes
+// the edge's lambda_psi.
+__device__ __forceinline__ void adj_e_terms(const AdjArgs& a, int c, int i, int j, int k, float l, float ca,
+                                            float cb, bool own, float& la, float& lb, float& le) {
+    const Geom& g = a.g;
+    const int p[3] = {i, j, k};
+    const int U = (c + 1) % 3, V = (c + 2) % 3;
+    const bool m = cb != 0.0f && p[U] > 0 && p[V] > 0;
+    le = m ? ca * l : l;
+    const float gg = m ? cb * l : 0.f;
+    const AdjAx au = adj_axis(g, U, i, j, k);
+    const AdjAx av = adj_axis(g, V, i, j, k);
+    la = gg * au.inv_dd;
+    lb = -gg * av.inv_dd;
+    if (au.slot_e >= 0) {
+        const long long q = g.psi_off[c * 3 + U] + psi_at(g, U, i, j, k, au.slot_e);
+        const float lp = a.lpsi_in[q];
+        if (own) a.lpsi_out[q] = m ? au.be * (gg + lp) : lp;
+        if (m) la += au.cer * (gg + lp);
+    }
+    if (av.slot_e >= 0) {
+        const long long q = g.psi_off[c * 3 + V] + psi_at(g, V, i, j, k, av.slot_e);
+        const float lp = a.lpsi_in[q];
+        if (own) a.lpsi_out[q] = m ? av.be * (-gg + lp) : lp;
+        if (m) lb += av.cer * (-gg + lp);
+    }
+}
+
+// All three E edges of node p from its lambda_E (l) and class id (cid); zero unless `ok`.
+__device__ __forceinline__ void adj_e_from(const AdjArgs& a, int i, int j, int k, bool ok, bool own,
+                                           const float (&l)[3], unsigned cid, float (&la)[3], float (&lb)[3],
+                                           float (&le)[3]) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) la[c] = lb[c] = le[c] = 0.f;
+    if (!ok) return;
+    const DevCoef cf = a.classes[cid];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) adj_e_terms(a, c, i, j, k, l[c], cf.ca[c], cf.cb[c], own, la[c], lb[c], le[c]);
+}
+
+// lambda_E and the class id of node p (zeros unless `ok`).
+template <typename CID>
+__device__ __forceinline__ void adj_e_load(const AdjArgs& a, long long id, bool ok, float (&l)[3], unsigned& cid) {
+    const Geom& g = a.g;
+    l[0] = l[1] = l[2] = 0.f;
+    cid = 0;
+    if (!ok) return;
+    l[0] = a.lE_in[id];
+    l[1] = a.lE_in[g.cs + id];
+    l[2] = a.lE_in[2 * g.cs + id];
+    cid = static_cast<const CID*>(a.node_class)[id];
+}
+
+// All three E edges of node p; zero where `in` is false (p off the grid) or past the last plane.
+template <typename CID>
+__device__ __forceinline__ void adj_e_all(const AdjArgs& a, int i, int j, int k, bool in, bool own, float (&la)[3],
+                                          float (&lb)[3], float (&le)[3]) {
+    const Geom& g = a.g;
+    const bool ok = in && i < g.n0;
+    float l[3];
+    unsigned cid;
+    adj_e_load<CID>(a, ((long long)i * g.n1 + j) * g.p2 + k, ok, l, cid);
+    adj_e_from(a, i, j, k, ok, own, l, cid, la, lb, le);
+}
+
+// H edge c's terms at p from its lambda_H' (lh): (la_H, lb_H); `own` writes its lambda_psi.
+__device__ __forceinline__ float2 adj_h_terms(const AdjArgs& a, int c, int i, int j, int k, float lh,
+                                              bool own) {
+    const Geom& g = a.g;
+    const int p[3] = {i, j, k};
+    const int n[3] = {g.n0, g.n1, g.n2};
+    const int U = (c + 1) % 3, V = (c + 2) % 3;
+    const bool r = p[U] + 1 < n[U] && p[V] + 1 < n[V];
+    const float gh = r ? -a.k_mu * lh : 0.f;
+    const AdjAx au = adj_axis(g, U, i, j, k);
+    const AdjAx av = adj_axis(g, V, i, j, k);
+    float la = gh * au.inv_d;
+    float lb = -gh * av.inv_d;
+    if (au.slot_h >= 0) {
+        const long long q = g.psi_off[9 + c * 3 + U] + psi_at(g, U, i, j, k, au.slot_h);
+        const float lp = a.lpsi_in[q];
+        if (own) a.lpsi_out[q] = r ? au.bh * (gh + lp) : lp;
+        if (r) la += au.chr * (gh + lp);
+    }
+    if (av.slot_h >= 0) {
+        const long long q = g.psi_off[9 + c * 3 + V] + psi_at(g, V, i, j, k, av.slot_h);
+        const float lp = a.lpsi_in[q];
+        if (own) a.lpsi_out[q] = r ? av.bh * (-gh + lp) : lp;
+        if (r) lb += av.chr * (-gh + lp);
+    }
+    return make_float2(la, lb);
+}
+
+constexpr int ADJ_TJ = 14;              // rows a block owns
+constexpr int ADJ_ROWS = ADJ_TJ + 2;    // warps: the owned rows and the j - 1 and j + ADJ_TJ rows
+constexpr int ADJ_KOWN = 30;            // columns a block owns (lanes 1..30)
+
+// Grid (ceil(n2 / 30), ceil(n1 / 14), ceil(n0 / seg)), block (32, 16). The loads of lambda_E and
+// the class id run two planes ahead and those of lambda_H one plane ahead of their use.
+template <typename CID>
+__global__ void __launch_bounds__(32 * ADJ_ROWS, 2) k_adj_step(AdjArgs a, int seg) {
+    __shared__ float es[2][ADJ_ROWS][32];   // la_E[0], lb_E[2] of each row (read by the row below)
+    __shared__ float hs[2][ADJ_ROWS][32];   // la_H[0], lb_H[2] of each row (read by the row above)
+    const Geom& g = a.g;
+    const int lane = threadIdx.x, w = threadIdx.y;
+    const int k = int(blockIdx.x) * ADJ_KOWN + lane - 1;
+    const int j = int(blockIdx.y) * ADJ_TJ + w - 1;
+    const int i0 = int(blockIdx.z) * seg, i1 = min(i0 + seg, g.n0);
+    const bool in = j >= 0 && k >= 0 && j < g.n1 && k < g.n2;
+    const bool own = in && lane >= 1 && lane <= ADJ_KOWN && w >= 1 && w <= ADJ_TJ;
+    const bool hrow = in && lane <= ADJ_KOWN && w <= ADJ_TJ;   // forms lambda_H' and the H-edge terms
+    const long long plane = (long long)g.n1 * g.p2, col = (long long)j * g.p2 + k;
+    constexpr unsigned FULL = 0xffffffffu;
+    float ea[3], eb[3], le[3];   // E-edge terms and ca lambda_E of plane i
+    adj_e_all<CID>(a, i0, j, k, in, own, ea, eb, le);
+    float pa2 = 0.f, pb1 = 0.f;  // la_H[2], lb_H[1] of plane i - 1
+    if (i0 > 0) {
+        // the H-edge terms of plane i0 - 1 that plane i0 reads, from the inputs
+        float qa[3], qb[3], ql[3];
+        adj_e_all<CID>(a, i0 - 1, j, k, in, false, qa, qb, ql);
+        es[0][w][lane] = qa[0];
+        const float sb0 = __shfl_down_sync(FULL, qb[0], 1);
+        __syncthreads();
+        if (hrow) {
+            const long long id = (i0 - 1) * plane + col;
+            const float h1 = a.lH_in[g.cs + id] + ((qa[2] - ea[2]) + (qb[0] - sb0));
+            const float h2 = a.lH_in[2 * g.cs + id] + ((qa[0] - es[0][w + 1][lane]) + (qb[1] - eb[1]));
+            pb1 = adj_h_terms(a, 1, i0 - 1, j, k, h1, false).y;
+            pa2 = adj_h_terms(a, 2, i0 - 1, j, k, h2, false).x;
+        }
+        __syncthreads();
+    }
+    float fe[3], fh[3] = {0.f, 0.f, 0.f};   // lambda_E of plane i + 1, lambda_H of plane i
+    unsigned fc;                            // class id of plane i + 1
+    adj_e_load<CID>(a, (i0 + 1) * plane + col, in && i0 + 1 < g.n0, fe, fc);
+    if (hrow) {
+        const long long id = i0 * plane + col;
+        fh[0] = a.lH_in[id];
+        fh[1] = a.lH_in[g.cs + id];
+        fh[2] = a.lH_in[2 * g.cs + id];
+    }
+    for (int i = i0; i < i1; ++i) {
+        const float l[3] = {fe[0], fe[1], fe[2]}, hc[3] = {fh[0], fh[1], fh[2]};
+        const unsigned cid = fc;
+        adj_e_load<CID>(a, (i + 2) * plane + col, in && i + 2 < g.n0, fe, fc);
+        if (hrow && i + 1 < i1) {
+            const long long id = (i + 1) * plane + col;
+            fh[0] = a.lH_in[id];
+            fh[1] = a.lH_in[g.cs + id];
+            fh[2] = a.lH_in[2 * g.cs + id];
+        }
+        float na[3], nb[3], nle[3];
+        adj_e_from(a, i + 1, j, k, in && i + 1 < g.n0, own && i + 1 < i1, l, cid, na, nb, nle);
+        es[0][w][lane] = ea[0];
+        es[1][w][lane] = eb[2];
+        const float sa1 = __shfl_down_sync(FULL, ea[1], 1);   // la_E[1] at k + 1
+        const float sb0 = __shfl_down_sync(FULL, eb[0], 1);   // lb_E[0] at k + 1
+        __syncthreads();
+        float ha[3] = {0.f, 0.f, 0.f}, hb[3] = {0.f, 0.f, 0.f};
+        if (hrow) {
+            const long long id = i * plane + col;
+            const float h0 = hc[0] + ((ea[1] - sa1) + (eb[2] - es[1][w + 1][lane]));
+            const float h1 = hc[1] + ((ea[2] - na[2]) + (eb[0] - sb0));
+            const float h2 = hc[2] + ((ea[0] - es[0][w + 1][lane]) + (eb[1] - nb[1]));
+            if (own) {
+                a.lH_out[id] = h0;
+                a.lH_out[g.cs + id] = h1;
+                a.lH_out[2 * g.cs + id] = h2;
+            }
+            const float2 t0 = adj_h_terms(a, 0, i, j, k, h0, own);
+            const float2 t1 = adj_h_terms(a, 1, i, j, k, h1, own);
+            const float2 t2 = adj_h_terms(a, 2, i, j, k, h2, own);
+            ha[0] = t0.x; hb[0] = t0.y;
+            ha[1] = t1.x; hb[1] = t1.y;
+            ha[2] = t2.x; hb[2] = t2.y;
+        }
+        hs[0][w][lane] = ha[0];
+        hs[1][w][lane] = hb[2];
+        const float ua1 = __shfl_up_sync(FULL, ha[1], 1);   // la_H[1] at k - 1
+        const float ub0 = __shfl_up_sync(FULL, hb[0], 1);   // lb_H[0] at k - 1
+        __syncthreads();
+        if (own) {
+            const long long id = i * plane + col;
+            a.lE_out[id] = le[0] + ((ua1 - ha[1]) + (hs[1][w - 1][lane] - hb[2]));
+            a.lE_out[g.cs + id] = le[1] + ((pa2 - ha[2]) + (ub0 - hb[0]));
+            a.lE_out[2 * g.cs + id] = le[2] + ((hs[0][w - 1][lane] - ha[0]) + (pb1 - hb[1]));
+        }
+        pa2 = ha[2];
+        pb1 = hb[1];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            ea[c] = na[c];
+            eb[c] = nb[c];
+            le[c] = nle[c];
+        }
+    }
+}
+
 // dJ/d(state after step n) of the flux objective on the plane window: per window node four
 // complex weights (Px, Py for Ex, Ey; Qx, Qy for Hx, Hy) times the step's DFT phase factors
 // (the same per-step table the forward DFT used, frequency 0).

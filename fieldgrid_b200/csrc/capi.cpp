@@ -508,6 +508,8 @@ int fg_flux_gradient(fg_gpu* g, const fg_sim* sim, uint64_t driven, const fg_pul
     sp.freq = spec->freq;
     sp.steps = spec->steps;
     sp.checkpoints = spec->checkpoints;
+    if (spec->transposes != 0 && spec->transposes != 1) return fail(FG_ERR_INVALID, "transposes must be 0 or 1", err, errlen);
+    sp.transposes = spec->transposes;
     FluxResult r;
     std::string e;
     const bool want = grad_eps != nullptr;

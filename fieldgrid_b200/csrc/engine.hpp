@@ -79,6 +79,7 @@ struct FluxSpec {
     double freq = 0;
     uint64_t steps = 0;
     uint64_t checkpoints = 0;                          // 0: keep every step's design history
+    int transposes = 0;     // 0: one fused adjoint step launch per step; 1: the E and H transposes apart
 };
 
 struct FluxResult {

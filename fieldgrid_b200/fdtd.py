@@ -576,6 +576,7 @@ class FluxSpec:
     window: Optional[tuple] = None   # ((i0, j0), (i1, j1))
     checkpoints: int = 0
     precision: int = 32              # 64: the objective alone, from an FP64 forward on the device
+    transposes: int = 0              # 1: the adjoint's E and H transposes as two launches per step
 
     def struct(self) -> A.fg_flux_spec:
         s = A.fg_flux_spec()
@@ -589,6 +590,7 @@ class FluxSpec:
         s.steps = int(self.steps)
         s.checkpoints = int(self.checkpoints)
         s.precision = int(self.precision)
+        s.transposes = int(self.transposes)
         return s
 
     def cells(self) -> int:

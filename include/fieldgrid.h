@@ -281,7 +281,8 @@ typedef struct fg_flux_spec {
     uint64_t checkpoints;
     int32_t precision;                    /* 0 or 32: the f32 update; 64: the objective alone from an FP64
                                              forward (f64 fields, psi, coefficients, pulse and DFT) */
-    int32_t reserved;
+    int32_t transposes;                   /* 0: each adjoint step one fused launch; 1: the E and H transposes
+                                             as two launches (slower; the same sums, bit for bit) */
 } fg_flux_spec;
 
 typedef struct fg_flux_result {

@@ -126,6 +126,22 @@ def test_checkpointed_sweep_equals_stored_history(gpu, small):
     assert np.array_equal(a.grad_sigma, b.grad_sigma)
 
 
+@pytest.mark.parametrize("dims", [(24, 24, 24), (40, 44, 70), (70, 37, 33)])
+def test_the_fused_adjoint_step_equals_the_separate_transposes(gpu, dims):
+    """One fused launch per adjoint step against the E and H transposes as two launches, on grids
+    whose (j, k) extents leave partial (8, 32) tiles and whose x extent spans several segments."""
+    scene, spec, _, _ = W.flux_design(*dims, pml=4, design=(4, 4, 3), steps=120, checkpoints=3)
+    sc = scene()
+    sim = fdtd.Sim.try_new(*sc.args())
+    a = fdtd.flux_gradient(gpu, sim, 0, sc.pulse, spec)
+    sep = fdtd.FluxSpec(spec.design_lo, spec.design_hi, spec.plane_k, spec.freq, spec.steps,
+                        checkpoints=spec.checkpoints, transposes=1)
+    b = fdtd.flux_gradient(gpu, sim, 0, sc.pulse, sep)
+    assert np.abs(a.grad_eps).max() > 0
+    assert np.array_equal(a.grad_eps, b.grad_eps)
+    assert np.array_equal(a.grad_sigma, b.grad_sigma)
+
+
 def test_the_autograd_function_returns_the_adjoint_gradient(gpu, small):
     import torch
     from fieldgrid_b200.autograd import FluxObjective

@@ -288,7 +288,11 @@ int flux_gradient(Gpu* gpu, const HostSim& sim, uint64_t driven, double f0, doub
         for (cudaEvent_t e : evs) cudaEventDestroy(e);
         if (sw) cudaStreamDestroy(sw);
     });
-    FG_CUDA(cudaStreamCreateWithFlags(&sw, cudaStreamNonBlocking));
+    // the sweep is the backward's critical path: its stream gets the highest priority, and the
+    // re-runs fill the SMs it leaves idle
+    int prio_lo = 0, prio_hi = 0;
+    FG_CUDA(cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi));
+    FG_CUDA(cudaStreamCreateWithPriority(&sw, cudaStreamNonBlocking, prio_hi));
     auto event = [&](cudaEvent_t* e, bool timing) -> int {
         FG_CUDA(cudaEventCreateWithFlags(e, timing ? cudaEventDefault : cudaEventDisableTiming));
         evs.push_back(*e);

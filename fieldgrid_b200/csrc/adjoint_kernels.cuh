@@ -238,7 +238,7 @@ struct AdjArgs {
     float k_mu;
 };
 
-// One axis node's factors as the adjoint reads them (from the axis tables, L1-resident).
+// One axis node's factors as the adjoint reads them.
 struct AdjAx {
     float inv_dd, be, cer;   // E side; cer = ce raw_inv_dd
     float inv_d, bh, chr;    // H side; chr = ch raw_inv_d
@@ -258,22 +258,67 @@ __device__ __forceinline__ AdjAx adj_ax(const AxisNode* n) {
     return r;
 }
 
-__device__ __forceinline__ AdjAx adj_axis(const Geom& g, int u, int i, int j, int k) {
-    return adj_ax(g.ax[u] + (u == 0 ? i : (u == 1 ? j : k)));
+constexpr int ADJ_TJ = 14;              // rows a block owns
+constexpr int ADJ_ROWS = ADJ_TJ + 2;    // warps: the owned rows and the j - 1 and j + ADJ_TJ rows
+constexpr int ADJ_KOWN = 30;            // columns a block owns (lanes 1..30)
+
+// A block's y and z axis factors in shared memory (field-major, slots as int bits): a thread's j
+// and k stay fixed along the march; the x factors are the plane's, one address for the block.
+struct AdjSm {
+    float y[8][ADJ_ROWS];
+    float z[8][32];
+};
+
+template <int N>
+__device__ __forceinline__ void adj_sm_fill(float (&t)[8][N], int at, const AxisNode* n) {
+    const AdjAx r = adj_ax(n);
+    t[0][at] = r.inv_dd;
+    t[1][at] = r.be;
+    t[2][at] = r.cer;
+    t[3][at] = r.inv_d;
+    t[4][at] = r.bh;
+    t[5][at] = r.chr;
+    t[6][at] = __int_as_float(r.slot_e);
+    t[7][at] = __int_as_float(r.slot_h);
+}
+
+template <int N>
+__device__ __forceinline__ AdjAx adj_sm_get(const float (&t)[8][N], int at) {
+    AdjAx r;
+    r.inv_dd = t[0][at];
+    r.be = t[1][at];
+    r.cer = t[2][at];
+    r.inv_d = t[3][at];
+    r.bh = t[4][at];
+    r.chr = t[5][at];
+    r.slot_e = __float_as_int(t[6][at]);
+    r.slot_h = __float_as_int(t[7][at]);
+    return r;
+}
+
+// Where a thread's axis factors are: the block's table and the thread's row (w) and lane.
+struct AdjAt {
+    const AdjSm* sm;
+    int w, lane;
+};
+
+__device__ __forceinline__ AdjAx adj_axis(const Geom& g, int u, int i, const AdjAt& at) {
+    if (u == 0) return adj_ax(g.ax[0] + i);
+    return u == 1 ? adj_sm_get(at.sm->y, at.w) : adj_sm_get(at.sm->z, at.lane);
 }
 
 // E-edge c's terms at p given its coefficients: (la_E, lb_E) and ca lambda_E (le). `own` writes
 // the edge's lambda_psi.
-__device__ __forceinline__ void adj_e_terms(const AdjArgs& a, int c, int i, int j, int k, float l, float ca,
-                                            float cb, bool own, float& la, float& lb, float& le) {
+__device__ __forceinline__ void adj_e_terms(const AdjArgs& a, const AdjAt& at, int c, int i, int j, int k, float l,
+                                            float ca, float cb, bool own, float& la, float& lb, float& le) {
     const Geom& g = a.g;
     const int p[3] = {i, j, k};
     const int U = (c + 1) % 3, V = (c + 2) % 3;
     const bool m = cb != 0.0f && p[U] > 0 && p[V] > 0;
     le = m ? ca * l : l;
     const float gg = m ? cb * l : 0.f;
-    const AdjAx au = adj_axis(g, U, i, j, k);
-    const AdjAx av = adj_axis(g, V, i, j, k);
+    const AdjAx au = adj_axis(g, U, i, at);
+    const AdjAx av = adj_axis(g, V, i, at);
     la = gg * au.inv_dd;
     lb = -gg * av.inv_dd;
     if (au.slot_e >= 0) {
@@ -291,7 +336,7 @@ __device__ __forceinline__ void adj_e_terms(const AdjArgs& a, int c, int i, int 
 }
 
 // All three E edges of node p from its lambda_E (l) and class id (cid); zero unless `ok`.
-__device__ __forceinline__ void adj_e_from(const AdjArgs& a, int i, int j, int k, bool ok, bool own,
+__device__ __forceinline__ void adj_e_from(const AdjArgs& a, const AdjAt& at, int i, int j, int k, bool ok, bool own,
                                            const float (&l)[3], unsigned cid, float (&la)[3], float (&lb)[3],
                                            float (&le)[3]) {
 #pragma unroll
@@ -299,7 +344,7 @@ __device__ __forceinline__ void adj_e_from(const AdjArgs& a, int i, int j, int k
     if (!ok) return;
     const DevCoef cf = a.classes[cid];
 #pragma unroll
-    for (int c = 0; c < 3; ++c) adj_e_terms(a, c, i, j, k, l[c], cf.ca[c], cf.cb[c], own, la[c], lb[c], le[c]);
+    for (int c = 0; c < 3; ++c) adj_e_terms(a, at, c, i, j, k, l[c], cf.ca[c], cf.cb[c], own, la[c], lb[c], le[c]);
 }
 
 // lambda_E and the class id of node p (zeros unless `ok`).
@@ -317,18 +362,18 @@ __device__ __forceinline__ void adj_e_load(const AdjArgs& a, long long id, bool 
 
 // All three E edges of node p; zero where `in` is false (p off the grid) or past the last plane.
 template <typename CID>
-__device__ __forceinline__ void adj_e_all(const AdjArgs& a, int i, int j, int k, bool in, bool own, float (&la)[3],
-                                          float (&lb)[3], float (&le)[3]) {
+__device__ __forceinline__ void adj_e_all(const AdjArgs& a, const AdjAt& at, int i, int j, int k, bool in, bool own,
+                                          float (&la)[3], float (&lb)[3], float (&le)[3]) {
     const Geom& g = a.g;
     const bool ok = in && i < g.n0;
     float l[3];
     unsigned cid;
     adj_e_load<CID>(a, ((long long)i * g.n1 + j) * g.p2 + k, ok, l, cid);
-    adj_e_from(a, i, j, k, ok, own, l, cid, la, lb, le);
+    adj_e_from(a, at, i, j, k, ok, own, l, cid, la, lb, le);
 }
 
 // H edge c's terms at p from its lambda_H' (lh): (la_H, lb_H); `own` writes its lambda_psi.
-__device__ __forceinline__ float2 adj_h_terms(const AdjArgs& a, int c, int i, int j, int k, float lh,
+__device__ __forceinline__ float2 adj_h_terms(const AdjArgs& a, const AdjAt& at, int c, int i, int j, int k, float lh,
                                               bool own) {
     const Geom& g = a.g;
     const int p[3] = {i, j, k};
@@ -336,8 +381,8 @@ __device__ __forceinline__ float2 adj_h_terms(const AdjArgs& a, int c, int i, in
     const int U = (c + 1) % 3, V = (c + 2) % 3;
     const bool r = p[U] + 1 < n[U] && p[V] + 1 < n[V];
     const float gh = r ? -a.k_mu * lh : 0.f;
-    const AdjAx au = adj_axis(g, U, i, j, k);
-    const AdjAx av = adj_axis(g, V, i, j, k);
+    const AdjAx au = adj_axis(g, U, i, at);
+    const AdjAx av = adj_axis(g, V, i, at);
     float la = gh * au.inv_d;
     float lb = -gh * av.inv_d;
     if (au.slot_h >= 0) {
@@ -355,20 +400,24 @@ __device__ __forceinline__ float2 adj_h_terms(const AdjArgs& a, int c, int i, in
     return make_float2(la, lb);
 }
 
-constexpr int ADJ_TJ = 14;              // rows a block owns
-constexpr int ADJ_ROWS = ADJ_TJ + 2;    // warps: the owned rows and the j - 1 and j + ADJ_TJ rows
-constexpr int ADJ_KOWN = 30;            // columns a block owns (lanes 1..30)
-
 // Grid (ceil(n2 / 30), ceil(n1 / 14), ceil(n0 / seg)), block (32, 16). The loads of lambda_E and
 // the class id run two planes ahead and those of lambda_H one plane ahead of their use.
 template <typename CID>
 __global__ void __launch_bounds__(32 * ADJ_ROWS, 2) k_adj_step(AdjArgs a, int seg) {
     __shared__ float es[2][ADJ_ROWS][32];   // la_E[0], lb_E[2] of each row (read by the row below)
     __shared__ float hs[2][ADJ_ROWS][32];   // la_H[0], lb_H[2] of each row (read by the row above)
+    __shared__ AdjSm sm;
     const Geom& g = a.g;
     const int lane = threadIdx.x, w = threadIdx.y;
     const int k = int(blockIdx.x) * ADJ_KOWN + lane - 1;
     const int j = int(blockIdx.y) * ADJ_TJ + w - 1;
+    if (w == 0) adj_sm_fill(sm.z, lane, g.ax[2] + min(max(k, 0), g.n2 - 1));
+    if (w == 1 && lane < ADJ_ROWS) {
+        const int jr = int(blockIdx.y) * ADJ_TJ + lane - 1;
+        adj_sm_fill(sm.y, lane, g.ax[1] + min(max(jr, 0), g.n1 - 1));
+    }
+    __syncthreads();
+    const AdjAt at{&sm, w, lane};
     const int i0 = int(blockIdx.z) * seg, i1 = min(i0 + seg, g.n0);
     const bool in = j >= 0 && k >= 0 && j < g.n1 && k < g.n2;
     const bool own = in && lane >= 1 && lane <= ADJ_KOWN && w >= 1 && w <= ADJ_TJ;
@@ -376,12 +425,12 @@ __global__ void __launch_bounds__(32 * ADJ_ROWS, 2) k_adj_step(AdjArgs a, int se
     const long long plane = (long long)g.n1 * g.p2, col = (long long)j * g.p2 + k;
     constexpr unsigned FULL = 0xffffffffu;
     float ea[3], eb[3], le[3];   // E-edge terms and ca lambda_E of plane i
-    adj_e_all<CID>(a, i0, j, k, in, own, ea, eb, le);
+    adj_e_all<CID>(a, at, i0, j, k, in, own, ea, eb, le);
     float pa2 = 0.f, pb1 = 0.f;  // la_H[2], lb_H[1] of plane i - 1
     if (i0 > 0) {
         // the H-edge terms of plane i0 - 1 that plane i0 reads, from the inputs
         float qa[3], qb[3], ql[3];
-        adj_e_all<CID>(a, i0 - 1, j, k, in, false, qa, qb, ql);
+        adj_e_all<CID>(a, at, i0 - 1, j, k, in, false, qa, qb, ql);
         es[0][w][lane] = qa[0];
         const float sb0 = __shfl_down_sync(FULL, qb[0], 1);
         __syncthreads();
@@ -389,8 +438,8 @@ __global__ void __launch_bounds__(32 * ADJ_ROWS, 2) k_adj_step(AdjArgs a, int se
             const long long id = (i0 - 1) * plane + col;
             const float h1 = a.lH_in[g.cs + id] + ((qa[2] - ea[2]) + (qb[0] - sb0));
             const float h2 = a.lH_in[2 * g.cs + id] + ((qa[0] - es[0][w + 1][lane]) + (qb[1] - eb[1]));
-            pb1 = adj_h_terms(a, 1, i0 - 1, j, k, h1, false).y;
-            pa2 = adj_h_terms(a, 2, i0 - 1, j, k, h2, false).x;
+            pb1 = adj_h_terms(a, at, 1, i0 - 1, j, k, h1, false).y;
+            pa2 = adj_h_terms(a, at, 2, i0 - 1, j, k, h2, false).x;
         }
         __syncthreads();
     }
@@ -414,7 +463,7 @@ __global__ void __launch_bounds__(32 * ADJ_ROWS, 2) k_adj_step(AdjArgs a, int se
             fh[2] = a.lH_in[2 * g.cs + id];
         }
         float na[3], nb[3], nle[3];
-        adj_e_from(a, i + 1, j, k, in && i + 1 < g.n0, own && i + 1 < i1, l, cid, na, nb, nle);
+        adj_e_from(a, at, i + 1, j, k, in && i + 1 < g.n0, own && i + 1 < i1, l, cid, na, nb, nle);
         es[0][w][lane] = ea[0];
         es[1][w][lane] = eb[2];
         const float sa1 = __shfl_down_sync(FULL, ea[1], 1);   // la_E[1] at k + 1
@@ -431,9 +480,9 @@ __global__ void __launch_bounds__(32 * ADJ_ROWS, 2) k_adj_step(AdjArgs a, int se
                 a.lH_out[g.cs + id] = h1;
                 a.lH_out[2 * g.cs + id] = h2;
             }
-            const float2 t0 = adj_h_terms(a, 0, i, j, k, h0, own);
-            const float2 t1 = adj_h_terms(a, 1, i, j, k, h1, own);
-            const float2 t2 = adj_h_terms(a, 2, i, j, k, h2, own);
+            const float2 t0 = adj_h_terms(a, at, 0, i, j, k, h0, own);
+            const float2 t1 = adj_h_terms(a, at, 1, i, j, k, h1, own);
+            const float2 t2 = adj_h_terms(a, at, 2, i, j, k, h2, own);
             ha[0] = t0.x; hb[0] = t0.y;
             ha[1] = t1.x; hb[1] = t1.y;
             ha[2] = t2.x; hb[2] = t2.y;

@@ -315,7 +315,7 @@ int flux_gradient(Gpu* gpu, const HostSim& sim, uint64_t driven, double f0, doub
         FG_CUDA(cudaMemcpyAsync(s->counter, &cnt, sizeof(cnt), cudaMemcpyHostToDevice, st));
         s->steps = a;
         if ((r = set_base((long long)(a - (q & 1) * L)))) return r;   // slots of ring half q & 1
-        if ((r = session_step(s, b - a, err))) return r;
+        if ((r = session_rerun(s, b - a, err))) return r;
         FG_CUDA(cudaEventRecord(e1, st));
         FG_CUDA(cudaEventRecord(rec_done, st));
         t_rec.push_back({e0, e1});

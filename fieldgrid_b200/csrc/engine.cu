@@ -134,6 +134,10 @@ struct Session {
     cudaGraphExec_t graph_many = nullptr;
     cudaGraphExec_t graph_two = nullptr;   // an even pair, for the ping-pong parity
     cudaGraphExec_t graph_one[2] = {nullptr, nullptr};
+    // re-runs (the adjoint's segment recomputation): the same steps without the outputs the run
+    // already holds (plane DFT, port series, NTFF), captured on first use
+    bool quiet = false;
+    cudaGraphExec_t quiet_many = nullptr, quiet_two = nullptr, quiet_one[2] = {nullptr, nullptr};
 };
 
 static constexpr int ENERGY_BLOCKS = 1024;
@@ -509,15 +513,15 @@ int enqueue_step(Session& s, int parity, std::string& err) {
     }
     if (s.n_sources || s.n_inductors) mark("lumped");
     if (s.n_sources || s.n_inductors) k_lumped<<<1, 256, 0, st>>>(s.sources, s.n_sources, s.inductors, s.n_inductors, s.sc, s.counter, e_now);
-    if (s.n_ports) mark("probe");
-    if (s.n_ports) k_probe<<<s.n_ports, 256, 0, st>>>(s.probes, s.port_edges, s.loops, g.cs, e_now, h_now, s.counter, s.sc, s.series);
-    if (s.plane_len) {
+    if (s.n_ports && !s.quiet) mark("probe");
+    if (s.n_ports && !s.quiet) k_probe<<<s.n_ports, 256, 0, st>>>(s.probes, s.port_edges, s.loops, g.cs, e_now, h_now, s.counter, s.sc, s.series);
+    if (s.plane_len && !s.quiet) {
         long long q = (long long)g.n0 * g.n1;
         mark("field_dft");
         k_field_dft<<<unsigned((q + 127) / 128), 128, 0, st>>>(g, s.plane_k, s.sc, s.counter, e_now, h_now, s.plane);
     }
-    if (s.ntff_len) mark("ntff");
-    if (s.ntff_len) k_ntff<<<(s.n_patches + 127) / 128, 128, 0, st>>>(s.patch, s.n_patches, g.cs, s.sc, s.counter, e_now, h_now, s.ntff);
+    if (s.ntff_len && !s.quiet) mark("ntff");
+    if (s.ntff_len && !s.quiet) k_ntff<<<(s.n_patches + 127) / 128, 128, 0, st>>>(s.patch, s.n_patches, g.cs, s.sc, s.counter, e_now, h_now, s.ntff);
     if (s.n_design && s.fused) {
         mark("design_record");
         k_design_record<<<(s.n_design + 127) / 128, 128, 0, st>>>(g, s.design, s.n_design, e_in, h_now, s.psi, s.counter,
@@ -1003,6 +1007,8 @@ void session_free(Session* s) {
     if (s->graph_two) cudaGraphExecDestroy(s->graph_two);
     for (auto& gx : s->graph_one)
         if (gx) cudaGraphExecDestroy(gx);
+    for (cudaGraphExec_t gx : {s->quiet_many, s->quiet_two, s->quiet_one[0], s->quiet_one[1]})
+        if (gx) cudaGraphExecDestroy(gx);
     if (s->arena) cudaFree(s->arena);
     cudaFree(s->design);
     cudaFree(s->hist_e);
@@ -1061,6 +1067,34 @@ int session_step(Session* s, uint64_t k, std::string& err) {
             done += 1;
             s->steps += 1;
         }
+    }
+    FG_CUDA(cudaGetLastError());
+    return FG_OK;
+}
+
+int session_rerun(Session* s, uint64_t k, std::string& err) {
+    if (!s->graph_many && !s->graph_one[0]) { err = "this session steps only as part of a batch"; return FG_ERR_INVALID; }
+    FG_CUDA(cudaSetDevice(s->gpu->device));
+    if (!s->quiet_many) {
+        s->quiet = true;
+        int rc = capture(*s, s->graph_steps, 0, &s->quiet_many, err);
+        if (!rc) rc = capture(*s, 2, 0, &s->quiet_two, err);
+        if (!rc) rc = capture(*s, 1, 0, &s->quiet_one[0], err);
+        if (!rc && s->fused) rc = capture(*s, 1, 1, &s->quiet_one[1], err);
+        s->quiet = false;
+        if (rc) return rc;
+    }
+    uint64_t done = 0;
+    while (done < k) {
+        const uint64_t left = k - done;
+        const int parity = s->fused ? int(s->steps & 1) : 0;
+        uint64_t n = 1;
+        cudaGraphExec_t gx = s->quiet_one[parity];
+        if (parity == 0 && left >= uint64_t(s->graph_steps)) { gx = s->quiet_many; n = s->graph_steps; }
+        else if (parity == 0 && left >= 2) { gx = s->quiet_two; n = 2; }
+        FG_CUDA(cudaGraphLaunch(gx, s->stream));
+        done += n;
+        s->steps += n;
     }
     FG_CUDA(cudaGetLastError());
     return FG_OK;

@@ -47,6 +47,9 @@ void gpu_close(Gpu* g);
 int session_new(Gpu* g, const HostSim& sim, const RunSpec& rs, Session** out, std::string& err);
 void session_free(Session* s);
 int session_step(Session* s, uint64_t k, std::string& err);
+// k steps without the outputs the run already holds (plane DFT, port series, NTFF): a re-run of
+// steps whose outputs were taken, for the state they leave (the adjoint's recomputation)
+int session_rerun(Session* s, uint64_t k, std::string& err);
 int session_sync(Session* s, std::string& err);
 int session_energy(Session* s, double* out, std::string& err);
 uint64_t session_steps(const Session* s);

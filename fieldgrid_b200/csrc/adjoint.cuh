@@ -19,6 +19,7 @@
 #include <complex>
 #include <functional>
 #include <memory>
+#include <unordered_set>
 
 namespace fg {
 
@@ -47,6 +48,8 @@ bool design_edges(const HostSim& sim, const FluxSpec& sp, std::vector<DesignEdge
         const size_t id = (ci * (n[1] - 1) + cj) * (n[2] - 1) + ck;
         return sim.cell_sig.empty() ? 0.0 : double(sim.cell_sig[id]);
     };
+    std::unordered_set<uint64_t> debye;   // (comp, node) of every Debye edge
+    for (const auto& q : sim.debye_edges) debye.insert(uint64_t(q.comp) * sim.nn + q.id);
     for (uint32_t c = 0; c < 3; ++c) {
         const uint32_t u = (c + 1) % 3, v = (c + 2) % 3;
         size_t lo[3], hi[3];   // edges whose averaging cells meet the box
@@ -87,7 +90,8 @@ bool design_edges(const HostSim& sim, const FluxSpec& sp, std::vector<DesignEdge
                     // the edge must carry exactly the plain coefficients (no PEC, lumped element,
                     // port or Debye override)
                     const size_t id = sim.idx(i, j, k);
-                    if (sim.ca(c, id) != float((1.0 - x) / (1.0 + x)) || sim.cb(c, id) != float(dt / eps / (1.0 + x))) {
+                    if (debye.count(uint64_t(c) * sim.nn + id) || sim.ca(c, id) != float((1.0 - x) / (1.0 + x)) ||
+                        sim.cb(c, id) != float(dt / eps / (1.0 + x))) {
                         err = "the design box overlaps an edge with a PEC, lumped, port or Debye override";
                         return false;
                     }
@@ -107,8 +111,8 @@ bool design_edges(const HostSim& sim, const FluxSpec& sp, std::vector<DesignEdge
 int flux_gradient(Gpu* gpu, const HostSim& sim, uint64_t driven, double f0, double fc, const FluxSpec& sp,
                   bool want_grad, FluxResult& res, std::string& err) {
     if (!gpu) { err = "no GPU: this engine has no CPU path"; return FG_ERR_NO_DEVICE; }
-    if (!sim.debye_edges.empty() || !sim.inductors.empty() || !sim.wires.empty() || !sim.sheets.empty()) {
-        err = "the adjoint supports dielectric, conducting, PEC and port media only (no Debye, inductor, wire or sheet)";
+    if (!sim.inductors.empty() || !sim.wires.empty() || !sim.sheets.empty()) {
+        err = "the adjoint supports dielectric, conducting, Debye, PEC and port media only (no inductor, wire or sheet)";
         return FG_ERR_INVALID;
     }
     if (sp.steps == 0 || sp.freq <= 0.0) { err = "the adjoint needs steps > 0 and a frequency > 0"; return FG_ERR_INVALID; }
@@ -158,20 +162,23 @@ int flux_gradient(Gpu* gpu, const HostSim& sim, uint64_t driven, double f0, doub
     auto now = [] { return std::chrono::steady_clock::now(); };
     auto ms = [](auto a, auto b) { return std::chrono::duration<double, std::milli>(b - a).count(); };
 
-    // checkpoints: E, H (buffer set 0 at even steps) and every psi slab
+    // checkpoints: E, H (buffer set 0 at even steps), every psi slab and the Debye state
     const size_t fbytes = size_t(3 * g.cs) * 4, pbytes = size_t(std::max<long long>(s->psi_total, 1)) * 4;
-    struct Ck { float *e = nullptr, *h = nullptr, *psi = nullptr; };
+    const size_t nd_s = size_t(s->n_debye) * size_t(s->n_poles);   // Debye state entries
+    const size_t dbytes = std::max<size_t>(nd_s, 1) * 4;
+    struct Ck { float *e = nullptr, *h = nullptr, *psi = nullptr, *deb = nullptr; };
     std::vector<Ck> cks;
     char* ck_mem = nullptr;   // all checkpoints in one allocation
     std::unique_ptr<void, std::function<void(void*)>> ck_guard((void*)1, [&](void*) { cudaFree(ck_mem); });
     const bool ckpt = want_grad && S > 1;
     if (ckpt) {
-        const size_t per = carve_size(fbytes) * 2 + carve_size(pbytes);
+        const size_t per = carve_size(fbytes) * 2 + carve_size(pbytes) + carve_size(dbytes);
         FG_CUDA(cudaMalloc(&ck_mem, per * S));
         for (uint64_t q = 0; q < S; ++q) {
             char* c = ck_mem + per * q;
             cks.push_back(Ck{reinterpret_cast<float*>(c), reinterpret_cast<float*>(c + carve_size(fbytes)),
-                             reinterpret_cast<float*>(c + 2 * carve_size(fbytes))});
+                             reinterpret_cast<float*>(c + 2 * carve_size(fbytes)),
+                             reinterpret_cast<float*>(c + 2 * carve_size(fbytes) + carve_size(pbytes))});
         }
     }
 
@@ -186,6 +193,7 @@ int flux_gradient(Gpu* gpu, const HostSim& sim, uint64_t driven, double f0, doub
             FG_CUDA(cudaMemcpyAsync(c.e, s->e, fbytes, cudaMemcpyDeviceToDevice, st));
             FG_CUDA(cudaMemcpyAsync(c.h, s->h, fbytes, cudaMemcpyDeviceToDevice, st));
             FG_CUDA(cudaMemcpyAsync(c.psi, s->psi, pbytes, cudaMemcpyDeviceToDevice, st));
+            if (nd_s) FG_CUDA(cudaMemcpyAsync(c.deb, s->debye_state, nd_s * 4, cudaMemcpyDeviceToDevice, st));
             if ((rc = session_step(s, std::min<uint64_t>(L, N - q * L), err))) return rc;
         }
     }
@@ -239,10 +247,11 @@ int flux_gradient(Gpu* gpu, const HostSim& sim, uint64_t driven, double f0, doub
     const int nd = int(edges.size());
     float *lE[2] = {nullptr, nullptr}, *lH[2] = {nullptr, nullptr}, *lpsi[2] = {nullptr, nullptr}, *dw = nullptr;
     float *cam = nullptr, *cbm = nullptr;   // the separate transposes' masked coefficients
+    float *lds = nullptr, *lold = nullptr;  // adjoint Debye state; each step's E_old term
     double *ga = nullptr, *gb = nullptr;
     auto free_adj = [&] {
         cudaFree(lE[0]); cudaFree(lE[1]); cudaFree(lH[0]); cudaFree(lH[1]); cudaFree(lpsi[0]); cudaFree(lpsi[1]);
-        cudaFree(dw); cudaFree(ga); cudaFree(gb); cudaFree(cam); cudaFree(cbm);
+        cudaFree(dw); cudaFree(ga); cudaFree(gb); cudaFree(cam); cudaFree(cbm); cudaFree(lds); cudaFree(lold);
     };
     std::unique_ptr<void, std::function<void(void*)>> adj_guard((void*)1, [&](void*) { free_adj(); });
     const bool sep = sp.transposes == 1;
@@ -253,6 +262,9 @@ int flux_gradient(Gpu* gpu, const HostSim& sim, uint64_t driven, double f0, doub
         FG_CUDA(cudaMalloc(&lH[1], fbytes));
     }
     for (auto** p : {&lpsi[0], &lpsi[1]}) FG_CUDA(cudaMalloc(p, pbytes));
+    FG_CUDA(cudaMalloc(&lds, dbytes));
+    FG_CUDA(cudaMalloc(&lold, std::max<size_t>(size_t(s->n_debye), 1) * 4));
+    FG_CUDA(cudaMemsetAsync(lds, 0, dbytes, st));
     FG_CUDA(cudaMalloc(&dw, wts.size() * 4));
     FG_CUDA(cudaMalloc(&ga, size_t(std::max(nd, 1)) * 8));
     FG_CUDA(cudaMalloc(&gb, size_t(std::max(nd, 1)) * 8));
@@ -311,6 +323,7 @@ int flux_gradient(Gpu* gpu, const HostSim& sim, uint64_t driven, double f0, doub
         FG_CUDA(cudaMemcpyAsync(s->e, cks[q].e, fbytes, cudaMemcpyDeviceToDevice, st));
         FG_CUDA(cudaMemcpyAsync(s->h, cks[q].h, fbytes, cudaMemcpyDeviceToDevice, st));
         FG_CUDA(cudaMemcpyAsync(s->psi, cks[q].psi, pbytes, cudaMemcpyDeviceToDevice, st));
+        if (nd_s) FG_CUDA(cudaMemcpyAsync(s->debye_state, cks[q].deb, nd_s * 4, cudaMemcpyDeviceToDevice, st));
         const unsigned cnt = unsigned(a);
         FG_CUDA(cudaMemcpyAsync(s->counter, &cnt, sizeof(cnt), cudaMemcpyHostToDevice, st));
         s->steps = a;
@@ -342,6 +355,14 @@ int flux_gradient(Gpu* gpu, const HostSim& sim, uint64_t driven, double f0, doub
                                                   int(wj), dw, s->sc.dft, 1, (long long)n, lE[set], lh);
             if (nd) k_adj_grad<<<dblocks, 128, 0, sw>>>(g, s->design, nd, lE[set], s->hist_e, s->hist_s,
                                                          (long long)(n - a) + half, ga, gb);
+            if (s->n_debye) {
+                const unsigned qb = unsigned((s->n_debye + 255) / 256);
+                switch (s->cid_bytes) {
+                    case 1: k_adj_debye_pre<uint8_t><<<qb, 256, 0, sw>>>(s->debye_f, s->debye_dd, s->n_debye, (const uint8_t*)s->node_class, s->classes, g.cs, s->debye_table, lds, lE[set], lold); break;
+                    case 2: k_adj_debye_pre<uint16_t><<<qb, 256, 0, sw>>>(s->debye_f, s->debye_dd, s->n_debye, (const uint16_t*)s->node_class, s->classes, g.cs, s->debye_table, lds, lE[set], lold); break;
+                    default: k_adj_debye_pre<uint32_t><<<qb, 256, 0, sw>>>(s->debye_f, s->debye_dd, s->n_debye, (const uint32_t*)s->node_class, s->classes, g.cs, s->debye_table, lds, lE[set], lold); break;
+                }
+            }
             if (sep) {
                 k_adj_e<<<grd, blk, 0, sw>>>(g, cam, cbm, lE[set], lE[1 - set], lpsi[set], lpsi[1 - set], lh);
                 k_adj_h<<<grd, blk, 0, sw>>>(g, lh, lpsi[set], lpsi[1 - set], lE[1 - set], s->sc.k_mu);
@@ -354,6 +375,9 @@ int flux_gradient(Gpu* gpu, const HostSim& sim, uint64_t driven, double f0, doub
                     default: k_adj_step<uint32_t><<<agrd, ablk, 0, sw>>>(aa, adj_seg); break;
                 }
             }
+            if (s->n_debye)
+                k_adj_debye_post<<<unsigned((s->n_debye + 255) / 256), 256, 0, sw>>>(s->debye_f, s->n_debye, lold,
+                                                                                     lE[1 - set]);
             set = 1 - set;
         }
         FG_CUDA(cudaGetLastError());

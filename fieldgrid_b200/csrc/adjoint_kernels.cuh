@@ -509,6 +509,42 @@ __global__ void __launch_bounds__(32 * ADJ_ROWS, 2) k_adj_step(AdjArgs a, int se
     }
 }
 
+// Transpose of the Debye ADE that follows the march (cpu.rs:239-260, debye_post_edge): per Debye
+// edge, E' = E* - cb sum_k (1 + b_k)/2 s_k and s_k' = b_k s_k + dd c_k (E' - E_old), E_old the
+// step's input. Given lambda_E' (in lE, in place) and lambda_s' (in ls, in place):
+//   d = sum_k dd c_k lambda_s'_k;  lambda_E* = lambda_E' + d;  lambda_s_k = b_k lambda_s'_k
+//   - cb (1 + b_k)/2 lambda_E*;  and lambda_E_old gains -d, kept in `old` for k_adj_debye_post,
+// which adds it to the march transpose's output (E_old is the step's input E).
+template <typename CID>
+__global__ void k_adj_debye_pre(const long long* __restrict__ f, const float* __restrict__ dd, int count,
+                                const CID* __restrict__ node_class, const DevCoef* __restrict__ classes, long long cs,
+                                const float* __restrict__ table, float* __restrict__ ls, float* __restrict__ lE,
+                                float* __restrict__ old) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= count) return;
+    const long long fi = f[q];
+    const int c = int(fi / cs);
+    const long long id = fi - c * cs;
+    const float cb = classes[node_class[id]].cb[c];
+    const int np = int(table[0]);
+    const float w = dd[q];
+    float d = 0.0f;
+    for (int k = 0; k < np; ++k) d += w * table[2 + 2 * k] * ls[(long long)k * count + q];
+    const float le = lE[fi] + d;
+    lE[fi] = le;
+    for (int k = 0; k < np; ++k) {
+        const long long p = (long long)k * count + q;
+        ls[p] = table[1 + 2 * k] * ls[p] - cb * (0.5f * (1.0f + table[1 + 2 * k])) * le;
+    }
+    old[q] = -d;
+}
+
+__global__ void k_adj_debye_post(const long long* __restrict__ f, int count, const float* __restrict__ old,
+                                 float* __restrict__ lE) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q < count) lE[f[q]] += old[q];
+}
+
 // dJ/d(state after step n) of the flux objective on the plane window: per window node four
 // complex weights (Px, Py for Ex, Ey; Qx, Qy for Hx, Hy) times the step's DFT phase factors
 // (the same per-step table the forward DFT used, frequency 0).

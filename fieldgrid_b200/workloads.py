@@ -267,11 +267,13 @@ def wire_cavity(radius: float, steps: int = 40000) -> Scene:
 
 def flux_design(nx: int = 160, ny: int = 160, nz: int = 96, dx: float = 1e-3, pml: int = 8,
                 design: tuple = (32, 32, 8), steps: int = 4000, checkpoints: int = 64, seed: int = 4,
-                freq: float = 10e9):
+                freq: float = 10e9, debye: bool = False):
     """Adjoint workload: an nx x ny x nz vacuum grid with a 50-ohm z-port source below a design
     block of per-voxel eps_r ~ U[1, 12] and sigma ~ U[0, 0.01] S/m (seed), and the flux objective
-    |F|^2 at `freq` on a z-plane above it. Returns (scene, spec, eps0, sig0): the scene built with
-    the initial design, the FluxSpec, and the design arrays (shaped like the block)."""
+    |F|^2 at `freq` on a z-plane above it. With `debye`, a one-pole Debye slab (eps_inf 2, delta
+    eps 3, tau 20 ps) stands beside the design block, between its low-x face and the CPML.
+    Returns (scene, spec, eps0, sig0): the scene built with the initial design, the FluxSpec, and
+    the design arrays (shaped like the block)."""
     from .fdtd import FluxSpec
     grid = Grid.uniform((0.0, 0.0, 0.0), (nx * dx, ny * dx, nz * dx), (nx, ny, nz), pml)
     rng = SplitMix64(seed)
@@ -289,14 +291,23 @@ def flux_design(nx: int = 160, ny: int = 160, nz: int = 96, dx: float = 1e-3, pm
                     freqs=[freq], plane_k=kp)
     spec = FluxSpec(design_lo=lo, design_hi=hi, plane_k=kp, freq=freq, steps=steps, checkpoints=checkpoints)
 
+    tau = 20e-12
+    media = Media(Sheets(), Debye([(1.0 / tau, 1.0)]), []) if debye else Media()
+
     def scene(eps=eps0, sig=sig0) -> Scene:
         mats = Materials.new(grid)
         e = mats.eps.reshape(nx, ny, nz)
         s = mats.sigma.reshape(nx, ny, nz)
         e[lo[0]:hi[0], lo[1]:hi[1], lo[2]:hi[2]] = np.asarray(eps, np.float32)
         s[lo[0]:hi[0], lo[1]:hi[1], lo[2]:hi[2]] = np.asarray(sig, np.float32)
+        if debye:
+            x0 = max(pml + 1, lo[0] - 6)
+            box = (slice(x0, lo[0] - 1), slice(lo[1], hi[1]), slice(lo[2] - 1, hi[2] + 1))
+            mats.inf.reshape(nx, ny, nz)[box] = 2.0
+            mats.debye.reshape(nx, ny, nz)[box] = 3.0
+            e[box] = 5.0
         sc = Scene(f"flux design {nx}x{ny}x{nz}, block {dw[0]}x{dw[1]}x{dw[2]}", grid, mats, None, [], ports, [],
-                   Media(), Pulse(freq, freq / 2), extras)
+                   media, Pulse(freq, freq / 2), extras)
         sc.info.update(dx=dx, pml=pml, design=dw, plane_k=kp)
         return sc
 

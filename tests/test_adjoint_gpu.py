@@ -113,6 +113,37 @@ def test_the_adjoint_matches_differences_of_the_device_fp64_forward(gpu, small):
         assert abs(adj - fd) <= FD_TOL * abs(fd), (which, at, adj, fd)
 
 
+@pytest.fixture(scope="module")
+def small_debye():
+    return W.flux_design(24, 24, 24, pml=4, design=(4, 4, 3), steps=400, checkpoints=0, debye=True)
+
+
+def test_the_adjoint_through_debye_media_matches_central_differences(gpu, small_debye):
+    """The Debye ADE transposed in the sweep: a one-pole slab beside the design block."""
+    scene, spec, eps0, sig0 = small_debye
+    sc = scene()
+    sim = fdtd.Sim.try_new(*sc.args())
+    r = fdtd.flux_gradient(gpu, sim, 0, sc.pulse, spec)
+    rng = W.SplitMix64(9)
+    for q in range(4):
+        at = tuple(rng.integer(0, s - 1) for s in spec.shape())
+        which = "eps" if q % 2 == 0 else "sig"
+        base = eps0 if which == "eps" else sig0
+        up, dn = base.copy(), base.copy()
+        up[at] = np.float32(base[at] + H)
+        dn[at] = np.float32(base[at] - H)
+        h_eff = 0.5 * (float(up[at]) - float(dn[at]))
+        jp = flux_f64(scene(*((up, sig0) if which == "eps" else (eps0, up))), spec)
+        jm = flux_f64(scene(*((dn, sig0) if which == "eps" else (eps0, dn))), spec)
+        fd = (jp - jm) / (2 * h_eff)
+        adj = (r.grad_eps if which == "eps" else r.grad_sigma)[at]
+        assert abs(adj - fd) <= FD_TOL * abs(fd), (which, at, adj, fd)
+    # checkpoints restore the Debye state: the same gradient bit for bit
+    spec4 = fdtd.FluxSpec(spec.design_lo, spec.design_hi, spec.plane_k, spec.freq, spec.steps, checkpoints=5)
+    b = fdtd.flux_gradient(gpu, sim, 0, sc.pulse, spec4)
+    assert np.array_equal(r.grad_eps, b.grad_eps) and np.array_equal(r.grad_sigma, b.grad_sigma)
+
+
 def test_checkpointed_sweep_equals_stored_history(gpu, small):
     scene, spec, eps0, sig0 = small
     sc = scene()
@@ -126,11 +157,12 @@ def test_checkpointed_sweep_equals_stored_history(gpu, small):
     assert np.array_equal(a.grad_sigma, b.grad_sigma)
 
 
-@pytest.mark.parametrize("dims", [(24, 24, 24), (40, 44, 70), (70, 37, 33)])
-def test_the_fused_adjoint_step_equals_the_separate_transposes(gpu, dims):
+@pytest.mark.parametrize("dims,debye", [((24, 24, 24), False), ((40, 44, 70), False), ((70, 37, 33), False),
+                                        ((40, 44, 70), True)])
+def test_the_fused_adjoint_step_equals_the_separate_transposes(gpu, dims, debye):
     """One fused launch per adjoint step against the E and H transposes as two launches, on grids
-    whose (j, k) extents leave partial (8, 32) tiles and whose x extent spans several segments."""
-    scene, spec, _, _ = W.flux_design(*dims, pml=4, design=(4, 4, 3), steps=120, checkpoints=3)
+    whose (j, k) extents leave partial (30, 14) tiles and whose x extent spans several segments."""
+    scene, spec, _, _ = W.flux_design(*dims, pml=4, design=(4, 4, 3), steps=120, checkpoints=3, debye=debye)
     sc = scene()
     sim = fdtd.Sim.try_new(*sc.args())
     a = fdtd.flux_gradient(gpu, sim, 0, sc.pulse, spec)
@@ -160,7 +192,7 @@ def test_the_autograd_function_returns_the_adjoint_gradient(gpu, small):
 def test_unsupported_media_are_refused(gpu):
     sc = W.everything(steps=20, fused=True)   # Debye slab, inductor, thin wires, sheets
     spec = fdtd.FluxSpec((8, 8, 8), (10, 10, 10), 12, 10e9, 20)
-    with pytest.raises(fdtd.FdtdError, match="no Debye"):
+    with pytest.raises(fdtd.FdtdError, match="no inductor"):
         fdtd.flux_gradient(gpu, fdtd.Sim.try_new(*sc.args()), 0, sc.pulse, spec)
     scene, spec, _, _ = W.flux_design(24, 24, 24, pml=4, design=(4, 4, 3), steps=20)
     edge = fdtd.FluxSpec((0, 10, 10), (4, 14, 13), spec.plane_k, spec.freq, 20)

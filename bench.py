@@ -51,11 +51,14 @@ def parse():
     p.add_argument("--cpu-steps", type=int, default=8, help="full time steps the CPU baseline times")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
-    p.add_argument("--workload", choices=["throughput", "adjoint", "batched"], default="throughput",
+    p.add_argument("--workload", choices=["throughput", "adjoint", "batched", "batched-adjoint"], default="throughput",
                    help="throughput: the 512^3 spheres step (the headline); adjoint: the flux-objective "
                         "gradient over a 32x32x8 design block on 160x160x96 cells, 4000 steps; batched: 192 "
-                        "grids of U{48..160}^3 cells stepped together vs one after another, 1500 steps")
+                        "grids of U{48..160}^3 cells stepped together vs one after another, 1500 steps; "
+                        "batched-adjoint: the same grids with a 16^3 design block each, their flux gradients "
+                        "together vs one after another")
     p.add_argument("--count", type=int, default=192, help="batched: grids in the batch")
+    p.add_argument("--group", type=int, default=16, help="batched-adjoint: gradients in flight together")
     p.add_argument("--checkpoints", type=int, default=64, help="adjoint: field checkpoints (0: keep the history)")
     p.add_argument("--fd", type=int, default=32,
                    help="adjoint: parameters checked against central differences of the FP64 device forward")
@@ -348,6 +351,62 @@ def run_batched(args):
     return 0
 
 
+def run_batched_adjoint(args):
+    """The batched workload's adjoint variant: each grid with a 16^3 design block and a flux
+    objective, its gradient taken one grid after another (fdtd.flux_gradient per grid) and for all
+    grids at once (fdtd.flux_gradient_batch, 16 runs in flight); wall clock around each, setup of
+    the device sessions included in both; value = sequential time / batched time."""
+    import numpy as np
+    import torch
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    from fieldgrid_b200 import fdtd
+    from fieldgrid_b200 import workloads as W
+    from fieldgrid_b200.gpu import Gpu, Options
+    g = Gpu.open(Options(device=torch.cuda.current_device()))
+    K = args.steps if args.steps != 2000 else 1500
+    ck = args.checkpoints if args.checkpoints != 64 else int(round(K ** 0.5))
+    jobs = W.batch_flux(count=args.count, steps=K, checkpoints=ck)
+    scenes = [j[0]() for j in jobs]
+    sims = [fdtd.Sim.try_new(*sc.args()) for sc in scenes]
+    specs = [j[1] for j in jobs]
+    pulses = [sc.pulse for sc in scenes]
+    nodes = [int(np.prod(sc.grid.dims())) for sc in scenes]
+    # warm-up: the first two runs both ways
+    fdtd.flux_gradient_batch(g, sims[:2], pulses[:2], specs[:2], group=args.group)
+    for q in range(2):
+        fdtd.flux_gradient(g, sims[q], 0, pulses[q], specs[q])
+    sampler = ClockSampler(device_id(int(os.environ.get("LOCAL_RANK", "0"))))
+    t = time.perf_counter()
+    seq = [fdtd.flux_gradient(g, sim, 0, p, spec) for sim, p, spec in zip(sims, pulses, specs)]
+    seq_s = time.perf_counter() - t
+    t = time.perf_counter()
+    bat = fdtd.flux_gradient_batch(g, sims, pulses, specs, group=args.group)
+    bat_s = time.perf_counter() - t
+    clocks = sampler.stop()
+    same = all(a.objective == b.objective and np.array_equal(a.grad_eps, b.grad_eps) and
+               np.array_equal(a.grad_sigma, b.grad_sigma) for a, b in zip(seq, bat))
+    if rank != 0:
+        return 0
+    line = {
+        "metric": "batched adjoint speed-up over sequential per-grid gradients", "value": seq_s / bat_s, "unit": "x",
+        "n_gpus": world, "steps": K, "warmup": 2, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"{len(jobs)} grids U{{48..160}}^3 cells (multiples of 8), 8-cell CPML, random "
+                               f"spheres (20% Debye), a 16^3 design block and a flux plane each", "grids": len(jobs),
+                   "nodes_total": int(sum(nodes)), "checkpoints": ck, "group": args.group},
+        "batched_s": bat_s, "sequential_s": seq_s, "results_equal": bool(same),
+        "sequential_setup_s": sum(r.setup_ms for r in seq) / 1e3,
+        "sequential_forward_backward_s": sum(r.forward_ms + r.backward_ms for r in seq) / 1e3,
+        "batched_setup_s": sum(r.setup_ms for r in bat) / 1e3,
+        "timing": "wall clock around all gradients (sessions set up inside both)",
+        "clocks": clocks,
+    }
+    print(json.dumps(line))
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -356,6 +415,8 @@ def main():
         return run_adjoint(args)
     if args.workload == "batched":
         return run_batched(args)
+    if args.workload == "batched-adjoint":
+        return run_batched_adjoint(args)
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))

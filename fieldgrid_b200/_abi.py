@@ -95,7 +95,7 @@ class fg_flux_spec(C.Structure):
 class fg_flux_result(C.Structure):
     _fields_ = [("objective", C.c_double), ("flux_re", C.c_double), ("flux_im", C.c_double),
                 ("forward_ms", C.c_double), ("recompute_ms", C.c_double), ("adjoint_ms", C.c_double),
-                ("backward_ms", C.c_double),
+                ("backward_ms", C.c_double), ("setup_ms", C.c_double),
                 ("segments", C.c_uint64), ("segment_len", C.c_uint64), ("design_edges", C.c_uint64)]
 
 

@@ -112,7 +112,8 @@ __global__ void __launch_bounds__(256) k_batch_probe(const BatchInstance* __rest
 }
 
 struct BatchShape {
-    int tile = 0;             // 0: 32 x 8, 1: 64 x 4, 2: 32 x 4 (TK x TJ); 3: graph branches
+    int tile = 0;             // 0: 32 x 8, 1: 64 x 4, 2: 32 x 4 (TK x TJ); 3: graph branches; 4: the same
+                              // with the direct-load march
     int blocks_per_sm = 0;    // persistent blocks per SM; 0: the occupancy limit
     int seg = 32;             // x-planes per work item
 };
@@ -120,7 +121,8 @@ struct BatchShape {
 // tile 3 is the other execution mode: one graph branch per grid, each running that grid's own
 // step (TMA march where it has a clean box, CPML shell, Debye, sources, probes) on its stream;
 // branches run concurrently
-constexpr int BATCH_BRANCHES = 3;
+constexpr int BATCH_BRANCHES = 3;          // graph branches, each grid's own step (TMA march + shell)
+constexpr int BATCH_BRANCHES_DIRECT = 4;   // graph branches with the direct-load fused march
 
 constexpr int BATCH_TILES[3][2] = {{32, 8}, {64, 4}, {32, 4}};
 
@@ -164,7 +166,12 @@ bool with_batch_march(int cid_bytes, int tile, F&& f) {
 
 // Work items of every grid for a shape; uploads the per-grid tiling and the prefix sums.
 int batch_apply_shape(Batch& B, const BatchShape& sh, std::string& err) {
-    if (sh.tile == BATCH_BRANCHES) {
+    for (Session* s : B.s) {
+        s->direct = sh.tile == BATCH_BRANCHES_DIRECT;
+        // the other grids fill the GPU: long x-segments, few halo planes
+        if (s->direct) s->shape.seg = 64;
+    }
+    if (sh.tile >= BATCH_BRANCHES) {
         B.shape = sh;
         return FG_OK;
     }
@@ -198,7 +205,7 @@ int batch_apply_shape(Batch& B, const BatchShape& sh, std::string& err) {
 int batch_enqueue_step(Batch& B, int parity, std::string& err) {
     cudaStream_t st = B.stream;
     const int n = int(B.s.size());
-    if (B.shape.tile == BATCH_BRANCHES) {
+    if (B.shape.tile >= BATCH_BRANCHES) {
         // fork every grid's stream from the batch stream, step it there, join back
         FG_CUDA(cudaEventRecord(B.fork, st));
         for (int b = 0; b < n; ++b) {
@@ -254,7 +261,7 @@ int batch_capture(Batch& B, int steps, int parity0, cudaGraphExec_t* out, std::s
     cudaGraph_t graph;
     FG_CUDA(cudaStreamBeginCapture(B.stream, cudaStreamCaptureModeThreadLocal));
     int rc = FG_OK;
-    if (B.shape.tile == BATCH_BRANCHES) {
+    if (B.shape.tile >= BATCH_BRANCHES) {
         // the grids are independent: each branch runs all the graph's steps, one join at the end
         FG_CUDA(cudaEventRecord(B.fork, B.stream));
         for (size_t b = 0; b < B.s.size() && rc == FG_OK; ++b) {
@@ -265,7 +272,7 @@ int batch_capture(Batch& B, int steps, int parity0, cudaGraphExec_t* out, std::s
             FG_CUDA(cudaStreamWaitEvent(B.stream, B.join[b], 0));
         }
     }
-    for (int q = 0; q < steps && rc == FG_OK && B.shape.tile != BATCH_BRANCHES; ++q)
+    for (int q = 0; q < steps && rc == FG_OK && B.shape.tile < BATCH_BRANCHES; ++q)
         rc = batch_enqueue_step(B, (parity0 + q) & 1, err);
     cudaError_t ce = cudaStreamEndCapture(B.stream, &graph);
     if (rc) return rc;
@@ -389,6 +396,7 @@ int batch_new(Gpu* gpu, const std::vector<const HostSim*>& sims, const std::vect
             for (int seg : {16, 32, 64})
                 for (int bps : {0, 2}) cands.push_back(BatchShape{tile, bps, seg});
         cands.push_back(BatchShape{BATCH_BRANCHES, 0, 0});
+        cands.push_back(BatchShape{BATCH_BRANCHES_DIRECT, 0, 0});
         for (const BatchShape& sh : cands) {
             if ((rc = batch_apply_shape(*B, sh, err))) break;
             // each candidate is timed as captured graphs of `timed` steps (launch costs included)
@@ -423,7 +431,7 @@ int batch_new(Gpu* gpu, const std::vector<const HostSim*>& sims, const std::vect
 int batch_new_c(Gpu* gpu, const std::vector<const HostSim*>& sims, const std::vector<RunSpec>& specs, bool tune,
                 int tile, int blocks_per_sm, int seg, int graph_steps, Batch** out, std::string& err) {
     BatchShape sh;
-    sh.tile = std::min(std::max(tile, 0), BATCH_BRANCHES);
+    sh.tile = std::min(std::max(tile, 0), BATCH_BRANCHES_DIRECT);
     sh.blocks_per_sm = std::max(blocks_per_sm, 0);
     sh.seg = seg > 0 ? seg : 32;
     return batch_new(gpu, sims, specs, tune, sh, graph_steps > 0 ? graph_steps : 10, out, err);

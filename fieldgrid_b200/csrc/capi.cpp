@@ -486,14 +486,8 @@ int fg_far_radiated(fg_gpu* g, const fg_far* f, uint64_t steps, double* total, d
     return FG_OK;
 }
 
-int fg_flux_gradient(fg_gpu* g, const fg_sim* sim, uint64_t driven, const fg_pulse* pulse, const fg_flux_spec* spec,
-                     fg_flux_result* out, double* grad_eps, double* grad_sigma, char* err, size_t errlen) {
-    if (!g) return fail(FG_ERR_NO_DEVICE, "no GPU: this engine has no CPU path", err, errlen);
-    if (!sim || !pulse || !spec || !out) return fail(FG_ERR_INVALID, "null argument", err, errlen);
-    if ((grad_eps == nullptr) != (grad_sigma == nullptr))
-        return fail(FG_ERR_INVALID, "grad_eps and grad_sigma are both given or both NULL", err, errlen);
-    const HostSim& hs = *sim->s;
-    FluxSpec sp;
+// fg_flux_spec -> FluxSpec (the default window: the nodes inside the CPML)
+static int flux_spec(const HostSim& hs, const fg_flux_spec* spec, FluxSpec& sp, std::string& e) {
     for (int a = 0; a < 3; ++a) { sp.lo[a] = spec->design_lo[a]; sp.hi[a] = spec->design_hi[a]; }
     sp.plane_k = spec->plane_k;
     for (int a = 0; a < 2; ++a) {
@@ -508,15 +502,12 @@ int fg_flux_gradient(fg_gpu* g, const fg_sim* sim, uint64_t driven, const fg_pul
     sp.freq = spec->freq;
     sp.steps = spec->steps;
     sp.checkpoints = spec->checkpoints;
-    if (spec->transposes != 0 && spec->transposes != 1) return fail(FG_ERR_INVALID, "transposes must be 0 or 1", err, errlen);
+    if (spec->transposes != 0 && spec->transposes != 1) { e = "transposes must be 0 or 1"; return FG_ERR_INVALID; }
     sp.transposes = spec->transposes;
-    FluxResult r;
-    std::string e;
-    const bool want = grad_eps != nullptr;
-    if (spec->precision == 64 && want) return fail(FG_ERR_INVALID, "the FP64 forward computes the objective alone", err, errlen);
-    int rc = spec->precision == 64 ? flux_objective64(g->g, hs, driven, pulse->f0, pulse->fc, sp, r, e)
-                                   : flux_gradient(g->g, hs, driven, pulse->f0, pulse->fc, sp, want, r, e);
-    if (rc) return fail(rc, e, err, errlen);
+    return FG_OK;
+}
+
+static void flux_out(const FluxResult& r, fg_flux_result* out) {
     out->objective = r.J;
     out->flux_re = r.f_re;
     out->flux_im = r.f_im;
@@ -524,12 +515,62 @@ int fg_flux_gradient(fg_gpu* g, const fg_sim* sim, uint64_t driven, const fg_pul
     out->recompute_ms = r.recompute_ms;
     out->adjoint_ms = r.adjoint_ms;
     out->backward_ms = r.backward_ms;
+    out->setup_ms = r.setup_ms;
     out->segments = r.segments;
     out->segment_len = r.segment_len;
     out->design_edges = r.design_edges;
+}
+
+int fg_flux_gradient(fg_gpu* g, const fg_sim* sim, uint64_t driven, const fg_pulse* pulse, const fg_flux_spec* spec,
+                     fg_flux_result* out, double* grad_eps, double* grad_sigma, char* err, size_t errlen) {
+    if (!g) return fail(FG_ERR_NO_DEVICE, "no GPU: this engine has no CPU path", err, errlen);
+    if (!sim || !pulse || !spec || !out) return fail(FG_ERR_INVALID, "null argument", err, errlen);
+    if ((grad_eps == nullptr) != (grad_sigma == nullptr))
+        return fail(FG_ERR_INVALID, "grad_eps and grad_sigma are both given or both NULL", err, errlen);
+    const HostSim& hs = *sim->s;
+    FluxSpec sp;
+    std::string e;
+    if (int rc = flux_spec(hs, spec, sp, e)) return fail(rc, e, err, errlen);
+    FluxResult r;
+    const bool want = grad_eps != nullptr;
+    if (spec->precision == 64 && want) return fail(FG_ERR_INVALID, "the FP64 forward computes the objective alone", err, errlen);
+    int rc = spec->precision == 64 ? flux_objective64(g->g, hs, driven, pulse->f0, pulse->fc, sp, r, e)
+                                   : flux_gradient(g->g, hs, driven, pulse->f0, pulse->fc, sp, want, r, e);
+    if (rc) return fail(rc, e, err, errlen);
+    flux_out(r, out);
     if (want) {
         std::copy(r.g_eps.begin(), r.g_eps.end(), grad_eps);
         std::copy(r.g_sig.begin(), r.g_sig.end(), grad_sigma);
+    }
+    return FG_OK;
+}
+
+int fg_flux_gradient_batch(fg_gpu* g, const fg_sim* const* sims, const uint64_t* driven, const fg_pulse* pulses,
+                           const fg_flux_spec* specs, uint64_t count, int group, fg_flux_result* out,
+                           double* const* grad_eps, double* const* grad_sigma, char* err, size_t errlen) {
+    if (!g) return fail(FG_ERR_NO_DEVICE, "no GPU: this engine has no CPU path", err, errlen);
+    if (count == 0) return fail(FG_ERR_INVALID, "an empty batch", err, errlen);
+    if (!sims || !driven || !pulses || !specs || !out || !grad_eps || !grad_sigma)
+        return fail(FG_ERR_INVALID, "null argument", err, errlen);
+    std::vector<const HostSim*> hs(count);
+    std::vector<uint64_t> dv(driven, driven + count);
+    std::vector<std::pair<double, double>> pv(count);
+    std::vector<FluxSpec> sv(count);
+    std::string e;
+    for (uint64_t q = 0; q < count; ++q) {
+        if (!sims[q] || !grad_eps[q] || !grad_sigma[q]) return fail(FG_ERR_INVALID, "null argument", err, errlen);
+        if (specs[q].precision == 64) return fail(FG_ERR_INVALID, "the FP64 forward computes the objective alone", err, errlen);
+        hs[q] = sims[q]->s;
+        pv[q] = {pulses[q].f0, pulses[q].fc};
+        if (int rc = flux_spec(*hs[q], &specs[q], sv[q], e)) return fail(rc, "job " + std::to_string(q) + ": " + e, err, errlen);
+    }
+    std::vector<FluxResult> rs;
+    int rc = flux_gradient_batch(g->g, hs, dv, pv, sv, group, rs, e);
+    if (rc) return fail(rc, e, err, errlen);
+    for (uint64_t q = 0; q < count; ++q) {
+        flux_out(rs[q], &out[q]);
+        std::copy(rs[q].g_eps.begin(), rs[q].g_eps.end(), grad_eps[q]);
+        std::copy(rs[q].g_sig.begin(), rs[q].g_sig.end(), grad_sigma[q]);
     }
     return FG_OK;
 }

@@ -137,6 +137,9 @@ struct Session {
     // re-runs (the adjoint's segment recomputation): the same steps without the outputs the run
     // already holds (plane DFT, port series, NTFF), captured on first use
     bool quiet = false;
+    // march with the direct-load fused kernel even where a TMA plan exists (a batch's graph
+    // branches of small grids: one launch instead of march + shell)
+    bool direct = false;
     cudaGraphExec_t quiet_many = nullptr, quiet_two = nullptr, quiet_one[2] = {nullptr, nullptr};
 };
 
@@ -473,14 +476,15 @@ int enqueue_step(Session& s, int parity, std::string& err) {
             k_wire_h<<<(s.n_wires + 127) / 128, 128, 0, st>>>(s.wires, s.n_wires, e_in, h_in);
         }
         mark("fused_step");
-        int rc = s.tma.ok
+        const bool tma = s.tma.ok && !s.direct;
+        int rc = tma
                      ? launch_tma(s, parity, e_out, h_out, parity ? s.psi : s.psi_h2)
                      : launch_fused(s.shape, s.cid_bytes, g, s.node_class, s.classes, e_in, h_in, e_out, h_out, s.psi,
                                     parity ? s.psi_h2 : s.psi, parity ? s.psi : s.psi_h2, s.sc.k_mu, s.counter,
                                     s.n_wires > 0, st);
         if (rc) { err = "fused step launch failed"; return FG_ERR_CUDA; }
         const unsigned shell_rows = s.shell.ra + s.shell.rb + s.shell.rc;
-        if (s.tma.ok && shell_rows > 0) {
+        if (tma && shell_rows > 0) {
             // the CPML shell around the march's clean box, one warp per row
             const unsigned gb = (shell_rows + SHELL_THREADS / 32 - 1) / (SHELL_THREADS / 32);
             mark("shell_h");
@@ -511,10 +515,18 @@ int enqueue_step(Session& s, int parity, std::string& err) {
             default: k_debye_post<uint32_t><<<(s.n_debye + 255) / 256, 256, 0, st>>>(s.debye_f, s.debye_dd, s.n_debye, saved, e_in, (const uint32_t*)s.node_class, s.classes, g.cs, s.debye_table, s.debye_state, e_now); break;
         }
     }
-    if (s.n_sources || s.n_inductors) mark("lumped");
-    if (s.n_sources || s.n_inductors) k_lumped<<<1, 256, 0, st>>>(s.sources, s.n_sources, s.inductors, s.n_inductors, s.sc, s.counter, e_now);
-    if (s.n_ports && !s.quiet) mark("probe");
-    if (s.n_ports && !s.quiet) k_probe<<<s.n_ports, 256, 0, st>>>(s.probes, s.port_edges, s.loops, g.cs, e_now, h_now, s.counter, s.sc, s.series);
+    const bool lumped = s.n_sources || s.n_inductors, probes = s.n_ports && !s.quiet;
+    if (lumped && probes && s.n_ports == 1) {
+        // one port: its source and its probe in one launch
+        mark("lumped_probe");
+        k_lumped_probe<<<1, 256, 0, st>>>(s.sources, s.n_sources, s.inductors, s.n_inductors, s.sc, s.counter, e_now,
+                                          s.probes, s.port_edges, s.loops, g.cs, h_now, s.series);
+    } else {
+        if (lumped) mark("lumped");
+        if (lumped) k_lumped<<<1, 256, 0, st>>>(s.sources, s.n_sources, s.inductors, s.n_inductors, s.sc, s.counter, e_now);
+        if (probes) mark("probe");
+        if (probes) k_probe<<<s.n_ports, 256, 0, st>>>(s.probes, s.port_edges, s.loops, g.cs, e_now, h_now, s.counter, s.sc, s.series);
+    }
     if (s.plane_len && !s.quiet) {
         long long q = (long long)g.n0 * g.n1;
         mark("field_dft");
@@ -533,13 +545,14 @@ int enqueue_step(Session& s, int parity, std::string& err) {
 
 uint64_t count_launches(const Session& s) {
     uint64_t n = 1;  // the field update (fused) or H update (separate)
-    if (s.tma.ok && s.shell.ra + s.shell.rb + s.shell.rc > 0) n += 2;  // the CPML shell around the TMA march
+    if (s.tma.ok && !s.direct && s.shell.ra + s.shell.rb + s.shell.rc > 0) n += 2;  // the CPML shell around the TMA march
     if (!s.fused) n += 1 + (s.n_debye ? 1 : 0);
     if (s.n_wires) n++;
     if (s.n_sheets) n += 2;
     if (s.n_debye) n++;
-    if (s.n_sources || s.n_inductors) n++;
-    if (s.n_ports) n++;
+    const bool lumped = s.n_sources || s.n_inductors;
+    if (lumped) n++;
+    if (s.n_ports && !(lumped && s.n_ports == 1)) n++;   // one port: with the source in one launch
     if (s.plane_len) n++;
     if (s.ntff_len) n++;
     if (s.n_design && s.fused) n++;

@@ -89,6 +89,7 @@ struct FluxResult {
     double J = 0, f_re = 0, f_im = 0;
     double forward_ms = 0, recompute_ms = 0, adjoint_ms = 0;
     double backward_ms = 0;             // the whole backward pass (re-runs and sweeps overlap)
+    double setup_ms = 0;                // checks, session, checkpoint and adjoint buffers
     uint64_t segments = 0, segment_len = 0, design_edges = 0;
     std::vector<double> g_eps, g_sig;   // per design cell, k fastest
 };
@@ -109,6 +110,10 @@ uint64_t batch_size(const Batch& b);
 
 int flux_gradient(Gpu* gpu, const HostSim& sim, uint64_t driven, double f0, double fc, const FluxSpec& sp,
                   bool want_grad, FluxResult& res, std::string& err);
+// count flux gradients on one GPU, `group` at a time with their phases enqueued together
+int flux_gradient_batch(Gpu* gpu, const std::vector<const HostSim*>& sims, const std::vector<uint64_t>& driven,
+                        const std::vector<std::pair<double, double>>& pulses, const std::vector<FluxSpec>& specs,
+                        int group, std::vector<FluxResult>& out, std::string& err);
 // The same objective from an FP64 forward on the device (fp64_forward.cuh).
 int flux_objective64(Gpu* gpu, const HostSim& sim, uint64_t driven, double f0, double fc, const FluxSpec& sp,
                      FluxResult& res, std::string& err);

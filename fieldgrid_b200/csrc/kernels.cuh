@@ -263,6 +263,18 @@ __global__ void k_probe(const DevProbe* __restrict__ defs, const DevPortEdge* __
     probe_block(blockIdx.x, defs, pe, lp, cs, e, h, counter, sc, series);
 }
 
+// The driven port's source (and inductors) then the probe of a Sim's single port, in one block:
+// lumped_block's writes are visible to probe_block after the block barrier.
+__global__ void k_lumped_probe(const DevSource* __restrict__ src, int ns, DevInductor* __restrict__ ind, int ni,
+                               StepConst sc, const unsigned* __restrict__ counter, float* __restrict__ e,
+                               const DevProbe* __restrict__ defs, const DevPortEdge* __restrict__ pe,
+                               const DevLoop* __restrict__ lp, long long cs, const float* __restrict__ h,
+                               float* __restrict__ series) {
+    lumped_block(src, ns, ind, ni, sc, counter, e);
+    __syncthreads();
+    probe_block(0, defs, pe, lp, cs, e, h, counter, sc, series);
+}
+
 // cpu.rs:336-361: running DFT of Ex, Ey, Ez (at (n+1) dt) and Hx, Hy (at (n+1/2) dt) on the
 // z-plane k = plane_k; phases formed in f32 like the CPU path.
 __global__ void k_field_dft(Geom g, int plane_k, StepConst sc, const unsigned* __restrict__ counter,

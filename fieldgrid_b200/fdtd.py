@@ -613,6 +613,7 @@ class FluxResult:
     segments: int
     segment_len: int
     design_edges: int
+    setup_ms: float = 0.0
 
 
 def flux_gradient(g, sim: Sim, driven: int, pulse: Pulse, spec: FluxSpec, grad: bool = True) -> FluxResult:
@@ -637,8 +638,39 @@ def flux_gradient(g, sim: Sim, driven: int, pulse: Pulse, spec: FluxSpec, grad: 
     return FluxResult(out.objective, complex(out.flux_re, out.flux_im),
                       None if ge is None else ge.reshape(shp), None if gs is None else gs.reshape(shp),
                       out.forward_ms, out.recompute_ms, out.adjoint_ms, out.backward_ms, int(out.segments),
-                      int(out.segment_len),
-                      int(out.design_edges))
+                      int(out.segment_len), int(out.design_edges), out.setup_ms)
+
+
+def flux_gradient_batch(g, sims, pulses, specs, driven=None, group: int = 16) -> list:
+    """Many flux gradients on one GPU (fg_flux_gradient_batch): `group` runs at a time, their
+    forwards, objectives and backward sweeps enqueued together on per-run streams. Each result
+    equals flux_gradient of that run alone."""
+    if g is None:
+        raise FdtdError("no GPU: this engine has no CPU path", 3)
+    n = len(sims)
+    L = lib()
+    driven = [0] * n if driven is None else list(driven)
+    hs = (C.c_void_p * n)(*[s._h for s in sims])
+    dv = (C.c_uint64 * n)(*driven)
+    pl = (A.fg_pulse * n)(*[A.pulse_struct(p) for p in pulses])
+    st = (A.fg_flux_spec * n)(*[s.struct() for s in specs])
+    out = (A.fg_flux_result * n)()
+    ge = [np.zeros(s.cells(), np.float64) for s in specs]
+    gs = [np.zeros(s.cells(), np.float64) for s in specs]
+    P = C.POINTER(C.c_double)
+    pe = (P * n)(*[a.ctypes.data_as(P) for a in ge])
+    ps = (P * n)(*[a.ctypes.data_as(P) for a in gs])
+    err = C.create_string_buffer(ERRLEN)
+    code = L.fg_flux_gradient_batch(g._h, hs, dv, pl, st, n, int(group), out, pe, ps, err, ERRLEN)
+    _check(code, err)
+    res = []
+    for q in range(n):
+        o = out[q]
+        shp = specs[q].shape()
+        res.append(FluxResult(o.objective, complex(o.flux_re, o.flux_im), ge[q].reshape(shp), gs[q].reshape(shp),
+                              o.forward_ms, o.recompute_ms, o.adjoint_ms, o.backward_ms, int(o.segments),
+                              int(o.segment_len), int(o.design_edges), o.setup_ms))
+    return res
 
 
 # ---- batches of independent grids (no counterpart in the reference) ----
@@ -686,7 +718,7 @@ class Batch:
         o = A.fg_batch_options()
         pb, tm, st = C.c_int(), C.c_double(), C.c_uint64()
         lib().fg_batch_info(self._h, C.byref(o), C.byref(pb), C.byref(tm), C.byref(st))
-        tiles = ["32x8", "64x4", "32x4", "graph branches"]
+        tiles = ["32x8", "64x4", "32x4", "graph branches", "graph branches, direct march"]
         return {"tile": tiles[o.tile], "blocks_per_sm": o.blocks_per_sm, "seg": o.seg,
                 "persistent_blocks": pb.value, "tuned_ms_per_step": tm.value, "steps": st.value}
 

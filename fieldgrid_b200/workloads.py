@@ -337,3 +337,54 @@ def batch_grids(count: int = 192, lo: int = 48, hi: int = 160, pml: int = 8, ste
         sc.info.update(dims=dims, pml=pml, spheres=nsph)
         scenes.append(sc)
     return scenes
+
+
+def batch_flux(count: int = 192, lo: int = 48, hi: int = 160, pml: int = 8, steps: int = 1500, seed: int = 6,
+               dx: float = 1e-3, design: int = 16, checkpoints: int = 39, freq: float = 10e9):
+    """Batched adjoint workload: the grids of batch_grids (same seed, so the same dims, spheres and
+    Debye pole), each with a centred design^3 block of per-voxel eps_r ~ U[1, 12] and sigma ~ U[0,
+    0.01] S/m (cleared of the spheres with a one-cell margin, so no Debye edge reaches it), the
+    flux objective at `freq` on a z-plane two nodes above the block, and the point source moved
+    below the block when it fell inside the cleared region. Returns [(scene, spec, eps0, sig0)]
+    with scene(eps, sig) -> Scene as in flux_design."""
+    from .fdtd import FluxSpec
+    base = batch_grids(count, lo, hi, pml, steps, seed, dx)
+    rng = SplitMix64(seed ^ 0x5EED)
+    out = []
+    for b, sc0 in enumerate(base):
+        dims = sc0.info["dims"]
+        d = min(design, min(dims) - 2 * pml - 8)
+        blo = tuple(dims[a] // 2 - d // 2 for a in range(3))
+        bhi = tuple(v + d for v in blo)
+        plane_k = bhi[2] + 2
+        eps0 = np.array([rng.uniform(1.0, 12.0) for _ in range(d ** 3)], np.float32).reshape(d, d, d)
+        sig0 = np.array([rng.uniform(0.0, 0.01) for _ in range(d ** 3)], np.float32).reshape(d, d, d)
+        at = sc0.ports[0].columns[0][0].at
+        clear = tuple(slice(blo[a] - 1, bhi[a] + 1) for a in range(3))
+        inside = all(blo[a] - 2 <= at[a] <= bhi[a] + 1 for a in range(3))
+        src = (blo[0] + d // 2, blo[1] + d // 2, max(pml + 2, blo[2] - 4)) if inside else at
+        ports = [_point_port("source", src)]
+        extras = Extras(max_steps=steps, decay_db=math.inf, fused_e=True, check_every=min(steps, 1000) or 1000,
+                        freqs=[freq], plane_k=plane_k)
+        spec = FluxSpec(design_lo=blo, design_hi=bhi, plane_k=plane_k, freq=freq, steps=steps, checkpoints=checkpoints)
+
+        def scene(eps=eps0, sig=sig0, sc0=sc0, dims=dims, blo=blo, bhi=bhi, clear=clear, ports=ports, extras=extras,
+                  b=b, plane_k=plane_k) -> Scene:
+            m0 = sc0.mats
+            shp = tuple(dims)
+            e = m0.eps.reshape(shp).copy()
+            s = m0.sigma.reshape(shp).copy()
+            inf = m0.inf.reshape(shp).copy()
+            deb = m0.debye.reshape(shp).copy()
+            e[clear], s[clear], inf[clear], deb[clear] = 1.0, 0.0, 1.0, 0.0
+            box = tuple(slice(blo[a], bhi[a]) for a in range(3))
+            e[box] = np.asarray(eps, np.float32)
+            s[box] = np.asarray(sig, np.float32)
+            mats = Materials(e, s, inf, deb)
+            sc = Scene(f"batch flux {b}: {dims[0]}x{dims[1]}x{dims[2]}", sc0.grid, mats, None, [], ports, [],
+                       sc0.media, Pulse(freq, freq / 2), extras)
+            sc.info.update(dims=dims, design=(blo, bhi), plane_k=plane_k)
+            return sc
+
+        out.append((scene, spec, eps0, sig0))
+    return out

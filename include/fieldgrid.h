@@ -289,6 +289,7 @@ typedef struct fg_flux_result {
     double objective, flux_re, flux_im;   /* J, and F */
     double forward_ms, recompute_ms, adjoint_ms;   /* the parts' device times (re-runs and sweeps overlap) */
     double backward_ms;                   /* the backward pass as a whole */
+    double setup_ms;                      /* checks, device session, checkpoint and adjoint buffers */
     uint64_t segments, segment_len, design_edges;
 } fg_flux_result;
 
@@ -297,6 +298,17 @@ typedef struct fg_flux_result {
 int fg_flux_gradient(fg_gpu* g, const fg_sim* sim, uint64_t driven, const fg_pulse* pulse,
                      const fg_flux_spec* spec, fg_flux_result* out, double* grad_eps, double* grad_sigma,
                      char* err, size_t errlen);
+
+/* Many flux gradients on one GPU: no counterpart in the reference. count independent runs, each a
+ * Sim with its own driven port, pulse and flux spec (precision 32), in groups of `group` runs (0:
+ * 16) whose phases are enqueued together, each run on its own streams: the forwards, then each
+ * objective as its forward ends, then the backward sweeps (the next group's set-up and forwards
+ * overlap them). Each run's results (out[q], and the gradients over spec q's design cells in
+ * grad_eps[q], grad_sigma[q]) are those of running it alone with fg_flux_gradient. The first
+ * failing run ends the call; its error names the run. */
+int fg_flux_gradient_batch(fg_gpu* g, const fg_sim* const* sims, const uint64_t* driven, const fg_pulse* pulses,
+                           const fg_flux_spec* specs, uint64_t count, int group, fg_flux_result* out,
+                           double* const* grad_eps, double* const* grad_sigma, char* err, size_t errlen);
 
 /* ---- batches: many independent grids stepped together ----
  * No counterpart in the reference (it runs one Sim per run() call). Each grid is a Sim with its
@@ -307,12 +319,13 @@ int fg_flux_gradient(fg_gpu* g, const fg_sim* sim, uint64_t driven, const fg_pul
  * grid's results are those of stepping it alone (fused step). Grids with thin wires or resistive
  * sheets, or that ask for a plane DFT or NTFF, are refused. With tune = 1 the batch times each
  * candidate (work-list tile 32x8, 64x4 or 32x4 with its persistent blocks per SM and x-planes per
- * work item, and the graph branches) as a captured graph of a few steps, keeps the fastest and
+ * work item, and both kinds of graph branches) as a captured graph of a few steps, keeps the fastest and
  * resets every grid to step 0; with tune = 0 it uses the shape given. */
 typedef struct fg_batch fg_batch;
 typedef struct fg_batch_options {
     int tune;
-    int tile;                /* work-list march 0: 32x8, 1: 64x4, 2: 32x4 (k x j); 3: graph branches */
+    int tile;                /* work-list march 0: 32x8, 1: 64x4, 2: 32x4 (k x j); 3: graph branches;
+                                4: graph branches with the direct-load march (one launch per grid) */
     int blocks_per_sm;       /* 0: the occupancy limit */
     int seg;                 /* x-planes per work item; 0: 32 */
     int graph_steps;         /* steps per captured graph; 0: 10 */

@@ -199,3 +199,28 @@ def test_unsupported_media_are_refused(gpu):
     sc = scene()
     with pytest.raises(fdtd.FdtdError, match="grid boundary"):
         fdtd.flux_gradient(gpu, fdtd.Sim.try_new(*sc.args()), 0, sc.pulse, edge)
+
+
+def test_a_batch_of_flux_gradients_equals_running_each_alone(gpu):
+    """fg_flux_gradient_batch: uneven grids with Debye spheres, in groups of 3 (two groups); every
+    run's objective and gradients equal flux_gradient of that run alone, bit for bit."""
+    jobs = W.batch_flux(count=5, lo=32, hi=48, pml=4, steps=120, checkpoints=4, design=8)
+    scenes = [j[0]() for j in jobs]
+    sims = [fdtd.Sim.try_new(*sc.args()) for sc in scenes]
+    specs = [j[1] for j in jobs]
+    got = fdtd.flux_gradient_batch(gpu, sims, [sc.pulse for sc in scenes], specs, group=3)
+    assert len(got) == 5
+    for sc, sim, spec, r in zip(scenes, sims, specs, got):
+        a = fdtd.flux_gradient(gpu, sim, 0, sc.pulse, spec)
+        assert r.objective == a.objective and r.objective > 0
+        assert np.array_equal(r.grad_eps, a.grad_eps) and np.abs(a.grad_eps).max() > 0
+        assert np.array_equal(r.grad_sigma, a.grad_sigma)
+
+
+def test_a_batch_names_the_run_it_refuses(gpu):
+    jobs = W.batch_flux(count=2, lo=32, hi=48, pml=4, steps=20, checkpoints=2, design=8)
+    scenes = [j[0]() for j in jobs]
+    sims = [fdtd.Sim.try_new(*sc.args()) for sc in scenes]
+    bad = fdtd.FluxSpec((0, 10, 10), (4, 14, 13), jobs[1][1].plane_k, 10e9, 20)
+    with pytest.raises(fdtd.FdtdError, match="job 1: the design box touches the grid boundary"):
+        fdtd.flux_gradient_batch(gpu, sims, [sc.pulse for sc in scenes], [jobs[0][1], bad])

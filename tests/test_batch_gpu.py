@@ -44,10 +44,11 @@ def test_a_batch_steps_each_grid_as_alone(gpu, scenes):
     b.close()
 
 
-def test_graph_branches_step_each_grid_as_alone(gpu, scenes):
+@pytest.mark.parametrize("tile,name", [(3, "graph branches"), (4, "graph branches, direct march")])
+def test_graph_branches_step_each_grid_as_alone(gpu, scenes, tile, name):
     sims = [fdtd.Sim.try_new(*sc.args()) for sc in scenes]
-    b = fdtd.Batch(gpu, sims, [sc.pulse for sc in scenes], 64, tune=False, tile=3, graph_steps=4)
-    assert b.info()["tile"] == "graph branches"
+    b = fdtd.Batch(gpu, sims, [sc.pulse for sc in scenes], 64, tune=False, tile=tile, graph_steps=4)
+    assert b.info()["tile"] == name
     b.step(9)
     check(gpu, b, scenes, 9)
     b.close()

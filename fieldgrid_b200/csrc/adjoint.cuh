@@ -224,6 +224,7 @@ struct FluxJob {
         for (const auto& e : info) edges.push_back(e.at);
         rs.design = want_grad ? &edges : nullptr;
         rs.hist_cap = want_grad ? int(std::min<uint64_t>(S > 1 ? 2 * L : L, N)) : 0;   // checkpoints: a ring of two segments
+        rs.design_in_steps = !(want_grad && S > 1);   // with checkpoints only the re-runs record
         int rc = session_new(gpu, *sim, rs, &s, err);
         if (rc) return rc;
         const Geom& g = s->geom;
@@ -369,6 +370,11 @@ struct FluxJob {
         const dim3 ablk(32, ADJ_ROWS, 1),
             agrd((g.n2 + ADJ_KOWN - 1) / ADJ_KOWN, (g.n1 + ADJ_TJ - 1) / ADJ_TJ, (g.n0 + adj_seg - 1) / adj_seg);
         const unsigned wblocks = unsigned((wi * wj + 127) / 128), dblocks = unsigned((nd + 127) / 128);
+        // the source and the gradient share a launch unless a design edge is a window node
+        bool apart = sep;
+        for (const int4& e : edges)
+            apart = apart || (e.x < 2 && uint64_t(e.w) == sp.plane_k && uint64_t(e.y) >= sp.win_lo[0] &&
+                              uint64_t(e.y) < sp.win_hi[0] && uint64_t(e.z) >= sp.win_lo[1] && uint64_t(e.z) < sp.win_hi[1]);
         int rc;
         cudaEvent_t rec_done, swept[2];
         if ((rc = event(&rec_done, false)) || (rc = event(&swept[0], false)) || (rc = event(&swept[1], false))) return rc;
@@ -408,10 +414,17 @@ struct FluxJob {
             FG_CUDA(cudaEventRecord(e0, sw));
             for (uint64_t n = b; n-- > a;) {
                 float* lh = sep ? lH[0] : lH[set];
-                k_adj_inject<<<wblocks, 128, 0, sw>>>(g, int(sp.plane_k), int(sp.win_lo[0]), int(wi), int(sp.win_lo[1]),
-                                                      int(wj), dw, s->sc.dft, 1, (long long)n, lE[set], lh);
-                if (nd) k_adj_grad<<<dblocks, 128, 0, sw>>>(g, s->design, nd, lE[set], s->hist_e, s->hist_s,
-                                                             (long long)(n - a) + half, ga, gb);
+                if (apart) {
+                    k_adj_inject<<<wblocks, 128, 0, sw>>>(g, int(sp.plane_k), int(sp.win_lo[0]), int(wi), int(sp.win_lo[1]),
+                                                          int(wj), dw, s->sc.dft, 1, (long long)n, lE[set], lh);
+                    if (nd) k_adj_grad<<<dblocks, 128, 0, sw>>>(g, s->design, nd, lE[set], s->hist_e, s->hist_s,
+                                                                 (long long)(n - a) + half, ga, gb);
+                } else {
+                    k_adj_source_grad<<<wblocks + dblocks, 128, 0, sw>>>(
+                        g, int(sp.plane_k), int(sp.win_lo[0]), int(wi), int(sp.win_lo[1]), int(wj), dw, s->sc.dft, 1,
+                        (long long)n, lE[set], lh, wblocks, s->design, nd, s->hist_e, s->hist_s,
+                        (long long)(n - a) + half, ga, gb);
+                }
                 if (s->n_debye) {
                     const unsigned qb = unsigned((s->n_debye + 255) / 256);
                     switch (s->cid_bytes) {

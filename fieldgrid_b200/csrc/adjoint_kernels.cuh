@@ -548,10 +548,9 @@ __global__ void k_adj_debye_post(const long long* __restrict__ f, int count, con
 // dJ/d(state after step n) of the flux objective on the plane window: per window node four
 // complex weights (Px, Py for Ex, Ey; Qx, Qy for Hx, Hy) times the step's DFT phase factors
 // (the same per-step table the forward DFT used, frequency 0).
-__global__ void k_adj_inject(Geom g, int plane_k, int i0, int wi, int j0, int wj, const float* __restrict__ w,
-                             const float* __restrict__ dft, int nf, long long n, float* __restrict__ lE,
-                             float* __restrict__ lH) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void adj_inject(const Geom& g, int t, int plane_k, int i0, int wi, int j0, int wj,
+                                           const float* __restrict__ w, const float* __restrict__ dft, int nf,
+                                           long long n, float* __restrict__ lE, float* __restrict__ lH) {
     if (t >= wi * wj) return;
     const int i = i0 + t / wj, j = j0 + t % wj;
     const float* d = dft + (n * nf) * 4;
@@ -563,17 +562,43 @@ __global__ void k_adj_inject(Geom g, int plane_k, int i0, int wi, int j0, int wj
     lH[g.cs + id] += 2.0f * (c[6] * d[2] + c[7] * d[3]);
 }
 
+__global__ void k_adj_inject(Geom g, int plane_k, int i0, int wi, int j0, int wj, const float* __restrict__ w,
+                             const float* __restrict__ dft, int nf, long long n, float* __restrict__ lE,
+                             float* __restrict__ lH) {
+    adj_inject(g, blockIdx.x * blockDim.x + threadIdx.x, plane_k, i0, wi, j0, wj, w, dft, nf, n, lE, lH);
+}
+
 // dJ/dca and dJ/dcb of every design edge: the adjoint of E^n+1 times E^n and S^n, summed in f64.
-__global__ void k_adj_grad(Geom g, const int4* __restrict__ edges, int n, const float* __restrict__ lE,
-                           const float* __restrict__ hist_e, const float* __restrict__ hist_s, long long slot,
-                           double* __restrict__ ga, double* __restrict__ gb) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void adj_grad(const Geom& g, int t, const int4* __restrict__ edges, int n,
+                                         const float* __restrict__ lE, const float* __restrict__ hist_e,
+                                         const float* __restrict__ hist_s, long long slot, double* __restrict__ ga,
+                                         double* __restrict__ gb) {
     if (t >= n) return;
     const int4 d = edges[t];
     const long long id = ((long long)d.y * g.n1 + d.z) * g.p2 + d.w;
     const double l = lE[d.x * g.cs + id];
     ga[t] += l * double(hist_e[slot * n + t]);
     gb[t] += l * double(hist_s[slot * n + t]);
+}
+
+__global__ void k_adj_grad(Geom g, const int4* __restrict__ edges, int n, const float* __restrict__ lE,
+                           const float* __restrict__ hist_e, const float* __restrict__ hist_s, long long slot,
+                           double* __restrict__ ga, double* __restrict__ gb) {
+    adj_grad(g, blockIdx.x * blockDim.x + threadIdx.x, edges, n, lE, hist_e, hist_s, slot, ga, gb);
+}
+
+// Both of a sweep step's small parts in one launch, where no design edge is a window node of the
+// plane (so the gradient reads no lambda_E the source writes): blocks [0, wblocks) add the
+// source (k_adj_inject), the rest accumulate the gradient (k_adj_grad). 128 threads per block.
+__global__ void k_adj_source_grad(Geom g, int plane_k, int i0, int wi, int j0, int wj, const float* __restrict__ w,
+                                  const float* __restrict__ dft, int nf, long long n_step, float* __restrict__ lE,
+                                  float* __restrict__ lH, unsigned wblocks, const int4* __restrict__ edges, int nd,
+                                  const float* __restrict__ hist_e, const float* __restrict__ hist_s, long long slot,
+                                  double* __restrict__ ga, double* __restrict__ gb) {
+    if (blockIdx.x < wblocks)
+        adj_inject(g, blockIdx.x * blockDim.x + threadIdx.x, plane_k, i0, wi, j0, wj, w, dft, nf, n_step, lE, lH);
+    else
+        adj_grad(g, (blockIdx.x - wblocks) * blockDim.x + threadIdx.x, edges, nd, lE, hist_e, hist_s, slot, ga, gb);
 }
 
 }  // namespace fg

@@ -137,6 +137,7 @@ struct Session {
     // re-runs (the adjoint's segment recomputation): the same steps without the outputs the run
     // already holds (plane DFT, port series, NTFF), captured on first use
     bool quiet = false;
+    bool design_in_steps = true;   // the normal steps record the design history too
     // march with the direct-load fused kernel even where a TMA plan exists (a batch's graph
     // branches of small grids: one launch instead of march + shell)
     bool direct = false;
@@ -534,7 +535,7 @@ int enqueue_step(Session& s, int parity, std::string& err) {
     }
     if (s.ntff_len && !s.quiet) mark("ntff");
     if (s.ntff_len && !s.quiet) k_ntff<<<(s.n_patches + 127) / 128, 128, 0, st>>>(s.patch, s.n_patches, g.cs, s.sc, s.counter, e_now, h_now, s.ntff);
-    if (s.n_design && s.fused) {
+    if (s.n_design && s.fused && (s.quiet || s.design_in_steps)) {
         mark("design_record");
         k_design_record<<<(s.n_design + 127) / 128, 128, 0, st>>>(g, s.design, s.n_design, e_in, h_now, s.psi, s.counter,
                                                                    s.hist_base, s.hist_cap, s.hist_e, s.hist_s);
@@ -555,7 +556,7 @@ uint64_t count_launches(const Session& s) {
     if (s.n_ports && !(lumped && s.n_ports == 1)) n++;   // one port: with the source in one launch
     if (s.plane_len) n++;
     if (s.ntff_len) n++;
-    if (s.n_design && s.fused) n++;
+    if (s.n_design && s.fused && s.design_in_steps) n++;
     return n;
 }
 
@@ -972,6 +973,7 @@ int session_new(Gpu* gpu, const HostSim& sim, const RunSpec& rs, Session** out, 
     if (rs.design && !rs.design->empty()) {
         if (!s->fused) { err = "design recording needs the fused step"; return FG_ERR_INVALID; }
         s->n_design = int(rs.design->size());
+        s->design_in_steps = rs.design_in_steps;
         s->hist_cap = std::max(rs.hist_cap, 1);
         const size_t hb = size_t(s->hist_cap) * size_t(s->n_design) * 4;
         FG_CUDA(cudaMalloc(&s->design, rs.design->size() * sizeof(int4)));

@@ -26,6 +26,7 @@ struct RunSpec {               // pack() inputs that are not part of the Sim (ru
     // into a ring of hist_cap slots (slot = step - base)
     const std::vector<int4>* design = nullptr;
     int hist_cap = 0;
+    bool design_in_steps = true;   // false: only re-runs (session_rerun) record the design history
     // batched use: the direct-load march only, no captured graphs, and a class-id width of at
     // least cid_bytes (so instances share one kernel instantiation)
     bool tma = true;

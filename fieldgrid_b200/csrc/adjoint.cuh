@@ -268,6 +268,35 @@ struct FluxJob {
         return FG_OK;
     }
 
+    // The re-run of steps [a, b) for the design history, inside its dependency cone: one step moves
+    // information one node along each axis (E^n+1 at p reads E^n and H^n-1/2 no further than one
+    // node away), so of T steps the t-th marches only the nodes within T - 1 - t + 2 of the design
+    // edges' nodes (the direct-load march over that box, no shell, no outputs) and the rest of the
+    // grid is left stale. The recorded history equals that of the full step, bit for bit.
+    int rerun_cone(uint64_t a, uint64_t b) {
+        const uint64_t T = b - a;
+        const int n[3] = {int(sim->n[0]), int(sim->n[1]), int(sim->n[2])};
+        int base_lo[3], base_hi[3];   // nodes of the design edges and of the H they read, + 1
+        for (int ax = 0; ax < 3; ++ax) {
+            base_lo[ax] = std::max(0, int(sp.lo[ax]) - 2);
+            base_hi[ax] = std::min(n[ax], int(sp.hi[ax]) + 3);
+        }
+        s->quiet = s->direct = s->boxed = true;
+        int rc = FG_OK;
+        for (uint64_t t = 0; t < T && !rc; ++t) {
+            const int r = int(T - 1 - t);
+            for (int ax = 0; ax < 3; ++ax) {
+                s->box_lo[ax] = std::max(0, base_lo[ax] - r);
+                s->box_hi[ax] = std::min(n[ax], base_hi[ax] + r);
+            }
+            rc = enqueue_step(*s, int((a + t) & 1), err);
+            s->steps += 1;
+        }
+        s->quiet = s->direct = s->boxed = false;
+        FG_CUDA(cudaGetLastError());
+        return rc;
+    }
+
     // the forward run, enqueued (checkpoints at the start of every segment)
     int forward() {
         FG_CUDA(cudaSetDevice(gpu->device));
@@ -392,7 +421,7 @@ struct FluxJob {
             s->steps = a;
             // the step counter at a, the history slots of ring half q & 1
             if ((r = set_base((long long)(a - (q & 1) * L), true, unsigned(a)))) return r;
-            if ((r = session_rerun(s, b - a, err))) return r;
+            if ((r = rerun_cone(a, b))) return r;
             FG_CUDA(cudaEventRecord(e1, st));
             FG_CUDA(cudaEventRecord(rec_done, st));
             t_rec.push_back({e0, e1});

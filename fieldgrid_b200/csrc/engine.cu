@@ -134,14 +134,17 @@ struct Session {
     cudaGraphExec_t graph_many = nullptr;
     cudaGraphExec_t graph_two = nullptr;   // an even pair, for the ping-pong parity
     cudaGraphExec_t graph_one[2] = {nullptr, nullptr};
-    // re-runs (the adjoint's segment recomputation): the same steps without the outputs the run
-    // already holds (plane DFT, port series, NTFF), captured on first use
+    // re-runs (the adjoint's segment recomputation): steps without the outputs the run already
+    // holds (plane DFT, port series, NTFF)
     bool quiet = false;
     bool design_in_steps = true;   // the normal steps record the design history too
     // march with the direct-load fused kernel even where a TMA plan exists (a batch's graph
     // branches of small grids: one launch instead of march + shell)
     bool direct = false;
-    cudaGraphExec_t quiet_many = nullptr, quiet_two = nullptr, quiet_one[2] = {nullptr, nullptr};
+    // with `direct`: march only the tiles over the box [box_lo, box_hi) (the adjoint's re-runs
+    // inside the design history's dependency cone)
+    bool boxed = false;
+    int box_lo[3] = {0, 0, 0}, box_hi[3] = {0, 0, 0};
 };
 
 static constexpr int ENERGY_BLOCKS = 1024;
@@ -478,7 +481,11 @@ int enqueue_step(Session& s, int parity, std::string& err) {
         }
         mark("fused_step");
         const bool tma = s.tma.ok && !s.direct;
-        int rc = tma
+        int rc = s.direct && s.boxed
+                     ? launch_fused_box(s.cid_bytes, g, s.node_class, s.classes, e_in, h_in, e_out, h_out, s.psi,
+                                        parity ? s.psi_h2 : s.psi, parity ? s.psi : s.psi_h2, s.sc.k_mu, s.counter,
+                                        s.box_lo, s.box_hi, st)
+                 : tma
                      ? launch_tma(s, parity, e_out, h_out, parity ? s.psi : s.psi_h2)
                      : launch_fused(s.shape, s.cid_bytes, g, s.node_class, s.classes, e_in, h_in, e_out, h_out, s.psi,
                                     parity ? s.psi_h2 : s.psi, parity ? s.psi : s.psi_h2, s.sc.k_mu, s.counter,
@@ -1022,8 +1029,6 @@ void session_free(Session* s) {
     if (s->graph_two) cudaGraphExecDestroy(s->graph_two);
     for (auto& gx : s->graph_one)
         if (gx) cudaGraphExecDestroy(gx);
-    for (cudaGraphExec_t gx : {s->quiet_many, s->quiet_two, s->quiet_one[0], s->quiet_one[1]})
-        if (gx) cudaGraphExecDestroy(gx);
     if (s->arena) cudaFree(s->arena);
     cudaFree(s->design);
     cudaFree(s->hist_e);
@@ -1082,34 +1087,6 @@ int session_step(Session* s, uint64_t k, std::string& err) {
             done += 1;
             s->steps += 1;
         }
-    }
-    FG_CUDA(cudaGetLastError());
-    return FG_OK;
-}
-
-int session_rerun(Session* s, uint64_t k, std::string& err) {
-    if (!s->graph_many && !s->graph_one[0]) { err = "this session steps only as part of a batch"; return FG_ERR_INVALID; }
-    FG_CUDA(cudaSetDevice(s->gpu->device));
-    if (!s->quiet_many) {
-        s->quiet = true;
-        int rc = capture(*s, s->graph_steps, 0, &s->quiet_many, err);
-        if (!rc) rc = capture(*s, 2, 0, &s->quiet_two, err);
-        if (!rc) rc = capture(*s, 1, 0, &s->quiet_one[0], err);
-        if (!rc && s->fused) rc = capture(*s, 1, 1, &s->quiet_one[1], err);
-        s->quiet = false;
-        if (rc) return rc;
-    }
-    uint64_t done = 0;
-    while (done < k) {
-        const uint64_t left = k - done;
-        const int parity = s->fused ? int(s->steps & 1) : 0;
-        uint64_t n = 1;
-        cudaGraphExec_t gx = s->quiet_one[parity];
-        if (parity == 0 && left >= uint64_t(s->graph_steps)) { gx = s->quiet_many; n = s->graph_steps; }
-        else if (parity == 0 && left >= 2) { gx = s->quiet_two; n = 2; }
-        FG_CUDA(cudaGraphLaunch(gx, s->stream));
-        done += n;
-        s->steps += n;
     }
     FG_CUDA(cudaGetLastError());
     return FG_OK;

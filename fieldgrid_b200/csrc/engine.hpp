@@ -26,7 +26,7 @@ struct RunSpec {               // pack() inputs that are not part of the Sim (ru
     // into a ring of hist_cap slots (slot = step - base)
     const std::vector<int4>* design = nullptr;
     int hist_cap = 0;
-    bool design_in_steps = true;   // false: only re-runs (session_rerun) record the design history
+    bool design_in_steps = true;   // false: only quiet re-runs (the adjoint's) record the design history
     // batched use: the direct-load march only, no captured graphs, and a class-id width of at
     // least cid_bytes (so instances share one kernel instantiation)
     bool tma = true;
@@ -48,9 +48,6 @@ void gpu_close(Gpu* g);
 int session_new(Gpu* g, const HostSim& sim, const RunSpec& rs, Session** out, std::string& err);
 void session_free(Session* s);
 int session_step(Session* s, uint64_t k, std::string& err);
-// k steps without the outputs the run already holds (plane DFT, port series, NTFF): a re-run of
-// steps whose outputs were taken, for the state they leave (the adjoint's recomputation)
-int session_rerun(Session* s, uint64_t k, std::string& err);
 int session_sync(Session* s, std::string& err);
 int session_energy(Session* s, double* out, std::string& err);
 uint64_t session_steps(const Session* s);

@@ -182,6 +182,17 @@ __global__ void __launch_bounds__(TK* TJ) k_fused_step(FusedArgs a, int seg) {
     fused_tile<CID, TK, TJ>(a, hs, blockIdx.x, blockIdx.y, i0, min(i0 + seg, a.g.n0));
 }
 
+// The fused step over the tiles that cover a box of nodes only: tiles (bx0 + x, by0 + y), planes
+// [i_lo, i_hi) in segments of `seg`. Nodes outside the box keep whatever the output buffers held
+// (the caller reads only nodes whose inputs the box kept correct: a dependency cone).
+template <typename CID, int TK, int TJ>
+__global__ void __launch_bounds__(TK* TJ) k_fused_box(FusedArgs a, int seg, int bx0, int by0, int i_lo, int i_hi) {
+    __shared__ float hs[2][3][TJ + 1][TK + 1];
+    if ((blockIdx.x | blockIdx.y | blockIdx.z | threadIdx.x | threadIdx.y) == 0) *a.counter += 1u;
+    const int i0 = i_lo + int(blockIdx.z) * seg;
+    fused_tile<CID, TK, TJ>(a, hs, bx0 + int(blockIdx.x), by0 + int(blockIdx.y), i0, min(i0 + seg, i_hi));
+}
+
 inline FusedShape choose_shape(const Geom& g, int /*cid_bytes*/, bool /*wires*/) {
     FusedShape s;
     s.tk = 32;
@@ -211,6 +222,29 @@ inline int launch_fused(const FusedShape& s, int cid_bytes, const Geom& g, const
         case 1: k_fused_step<uint8_t, TK, TJ><<<grd, blk, 0, st>>>(a, s.seg); break;
         case 2: k_fused_step<uint16_t, TK, TJ><<<grd, blk, 0, st>>>(a, s.seg); break;
         default: k_fused_step<uint32_t, TK, TJ><<<grd, blk, 0, st>>>(a, s.seg); break;
+    }
+    return cudaPeekAtLastError() == cudaSuccess ? 0 : 1;
+}
+
+// launch_fused over the box of nodes [lo, hi) (each lo < hi, inside the grid).
+inline int launch_fused_box(int cid_bytes, const Geom& g, const void* node_class, const DevCoef* classes,
+                            const float* e_in, const float* h_in, float* e_out, float* h_out, float* psi_e,
+                            const float* psi_h_in, float* psi_h_out, float k_mu, unsigned* counter, const int lo[3],
+                            const int hi[3], cudaStream_t st) {
+    FusedArgs a{g, node_class, classes, e_in, h_in, e_out, h_out, psi_e, psi_h_in, psi_h_out, k_mu, counter};
+    constexpr int TK = 32, TJ = 8;
+    const int bx0 = lo[2] / TK, bx1 = (hi[2] + TK - 1) / TK, by0 = lo[1] / TJ, by1 = (hi[1] + TJ - 1) / TJ;
+    const int planes = hi[0] - lo[0];
+    const long long tiles = (long long)(bx1 - bx0) * (by1 - by0);
+    // x-segments for several waves of blocks on 148 SMs, 8 to 64 planes
+    int seg = 64;
+    while (seg > 8 && tiles * ((planes + seg - 1) / seg) < 148 * 8) seg /= 2;
+    dim3 blk(TK, TJ, 1);
+    dim3 grd(unsigned(bx1 - bx0), unsigned(by1 - by0), unsigned((planes + seg - 1) / seg));
+    switch (cid_bytes) {
+        case 1: k_fused_box<uint8_t, TK, TJ><<<grd, blk, 0, st>>>(a, seg, bx0, by0, lo[0], hi[0]); break;
+        case 2: k_fused_box<uint16_t, TK, TJ><<<grd, blk, 0, st>>>(a, seg, bx0, by0, lo[0], hi[0]); break;
+        default: k_fused_box<uint32_t, TK, TJ><<<grd, blk, 0, st>>>(a, seg, bx0, by0, lo[0], hi[0]); break;
     }
     return cudaPeekAtLastError() == cudaSuccess ? 0 : 1;
 }

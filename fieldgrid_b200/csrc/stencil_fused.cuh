@@ -236,9 +236,10 @@ inline int launch_fused_box(int cid_bytes, const Geom& g, const void* node_class
     const int bx0 = lo[2] / TK, bx1 = (hi[2] + TK - 1) / TK, by0 = lo[1] / TJ, by1 = (hi[1] + TJ - 1) / TJ;
     const int planes = hi[0] - lo[0];
     const long long tiles = (long long)(bx1 - bx0) * (by1 - by0);
-    // x-segments for several waves of blocks on 148 SMs, 8 to 64 planes
+    // x-segments for several waves of blocks on 148 SMs, 2 to 64 planes: a small box runs short
+    // segments, since a block's march is a chain of per-plane latencies
     int seg = 64;
-    while (seg > 8 && tiles * ((planes + seg - 1) / seg) < 148 * 8) seg /= 2;
+    while (seg > 2 && tiles * ((planes + seg - 1) / seg) < 148 * 8) seg /= 2;
     dim3 blk(TK, TJ, 1);
     dim3 grd(unsigned(bx1 - bx0), unsigned(by1 - by0), unsigned((planes + seg - 1) / seg));
     switch (cid_bytes) {

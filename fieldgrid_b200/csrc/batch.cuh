@@ -113,9 +113,10 @@ __global__ void __launch_bounds__(256) k_batch_probe(const BatchInstance* __rest
 
 struct BatchShape {
     int tile = 0;             // 0: 32 x 8, 1: 64 x 4, 2: 32 x 4 (TK x TJ); 3: graph branches; 4: the same
-                              // with the direct-load march
+                              // with the direct-load march for the small grids
     int blocks_per_sm = 0;    // persistent blocks per SM; 0: the occupancy limit
-    int seg = 32;             // x-planes per work item
+    int seg = 32;             // x-planes per work item; tile 4: the grids of fewer than seg thousand
+                              // nodes march direct (0: all)
 };
 
 // tile 3 is the other execution mode: one graph branch per grid, each running that grid's own
@@ -167,7 +168,7 @@ bool with_batch_march(int cid_bytes, int tile, F&& f) {
 // Work items of every grid for a shape; uploads the per-grid tiling and the prefix sums.
 int batch_apply_shape(Batch& B, const BatchShape& sh, std::string& err) {
     for (Session* s : B.s) {
-        s->direct = sh.tile == BATCH_BRANCHES_DIRECT;
+        s->direct = sh.tile == BATCH_BRANCHES_DIRECT && (sh.seg <= 0 || s->geom.nn < 1000LL * sh.seg);
         // the other grids fill the GPU: long x-segments, few halo planes
         if (s->direct) s->shape.seg = 64;
     }
@@ -396,7 +397,7 @@ int batch_new(Gpu* gpu, const std::vector<const HostSim*>& sims, const std::vect
             for (int seg : {16, 32, 64})
                 for (int bps : {0, 2}) cands.push_back(BatchShape{tile, bps, seg});
         cands.push_back(BatchShape{BATCH_BRANCHES, 0, 0});
-        cands.push_back(BatchShape{BATCH_BRANCHES_DIRECT, 0, 0});
+        for (int below : {0, 300, 1000}) cands.push_back(BatchShape{BATCH_BRANCHES_DIRECT, 0, below});
         for (const BatchShape& sh : cands) {
             if ((rc = batch_apply_shape(*B, sh, err))) break;
             // each candidate is timed as captured graphs of `timed` steps (launch costs included)

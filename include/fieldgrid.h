@@ -325,7 +325,8 @@ typedef struct fg_batch fg_batch;
 typedef struct fg_batch_options {
     int tune;
     int tile;                /* work-list march 0: 32x8, 1: 64x4, 2: 32x4 (k x j); 3: graph branches;
-                                4: graph branches with the direct-load march (one launch per grid) */
+                                4: graph branches, the grids of fewer than seg thousand nodes (all: seg 0)
+                                with the direct-load march (one launch per grid-step) */
     int blocks_per_sm;       /* 0: the occupancy limit */
     int seg;                 /* x-planes per work item; 0: 32 */
     int graph_steps;         /* steps per captured graph; 0: 10 */

@@ -44,10 +44,13 @@ def test_a_batch_steps_each_grid_as_alone(gpu, scenes):
     b.close()
 
 
-@pytest.mark.parametrize("tile,name", [(3, "graph branches"), (4, "graph branches, direct march")])
-def test_graph_branches_step_each_grid_as_alone(gpu, scenes, tile, name):
+@pytest.mark.parametrize("tile,seg,name", [(3, 0, "graph branches"), (4, 0, "graph branches, direct march"),
+                                          (4, 50, "graph branches, direct march")])
+def test_graph_branches_step_each_grid_as_alone(gpu, scenes, tile, seg, name):
+    """Branches of each grid's own step: the TMA march, the direct-load march for all grids, and
+    the direct-load march for the grids under 50 thousand nodes only (a mix)."""
     sims = [fdtd.Sim.try_new(*sc.args()) for sc in scenes]
-    b = fdtd.Batch(gpu, sims, [sc.pulse for sc in scenes], 64, tune=False, tile=tile, graph_steps=4)
+    b = fdtd.Batch(gpu, sims, [sc.pulse for sc in scenes], 64, tune=False, tile=tile, seg=seg, graph_steps=4)
     assert b.info()["tile"] == name
     b.step(9)
     check(gpu, b, scenes, 9)

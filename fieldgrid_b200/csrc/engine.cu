@@ -91,6 +91,7 @@ struct Session {
     float* currents = nullptr;
     long long* debye_f = nullptr;
     float* debye_dd = nullptr;
+    float* debye_cb = nullptr;      // each Debye edge's cb
     float* debye_old = nullptr;
     float* debye_state = nullptr;
     float* debye_table = nullptr;
@@ -517,11 +518,8 @@ int enqueue_step(Session& s, int parity, std::string& err) {
     if (s.n_debye) {
         mark("debye_post");
         const float* saved = s.fused ? nullptr : s.debye_old;
-        switch (s.cid_bytes) {
-            case 1: k_debye_post<uint8_t><<<(s.n_debye + 255) / 256, 256, 0, st>>>(s.debye_f, s.debye_dd, s.n_debye, saved, e_in, (const uint8_t*)s.node_class, s.classes, g.cs, s.debye_table, s.debye_state, e_now); break;
-            case 2: k_debye_post<uint16_t><<<(s.n_debye + 255) / 256, 256, 0, st>>>(s.debye_f, s.debye_dd, s.n_debye, saved, e_in, (const uint16_t*)s.node_class, s.classes, g.cs, s.debye_table, s.debye_state, e_now); break;
-            default: k_debye_post<uint32_t><<<(s.n_debye + 255) / 256, 256, 0, st>>>(s.debye_f, s.debye_dd, s.n_debye, saved, e_in, (const uint32_t*)s.node_class, s.classes, g.cs, s.debye_table, s.debye_state, e_now); break;
-        }
+        k_debye_post_cb<<<(s.n_debye + 255) / 256, 256, 0, st>>>(s.debye_f, s.debye_dd, s.debye_cb, s.n_debye, saved,
+                                                                 e_in, s.debye_table, s.debye_state, e_now);
     }
     const bool lumped = s.n_sources || s.n_inductors, probes = s.n_ports && !s.quiet;
     if (lumped && probes && s.n_ports == 1) {
@@ -663,10 +661,11 @@ int session_new(Gpu* gpu, const HostSim& sim, const RunSpec& rs, Session** out, 
         sheets.push_back(d);
     }
     std::vector<long long> debye_f;
-    std::vector<float> debye_dd;
+    std::vector<float> debye_dd, debye_cb;
     for (auto& q : sim.debye_edges) {
         debye_f.push_back((long long)q.comp * cs + dev(q.id));
         debye_dd.push_back(float(q.dd));
+        debye_cb.push_back(sim.cb(q.comp, q.id));
     }
     std::vector<float> debye_table{float(sim.poles.size())};
     for (auto& [x, a] : sim.poles) {
@@ -819,7 +818,7 @@ int session_new(Gpu* gpu, const HostSim& sim, const RunSpec& rs, Session** out, 
     need += carve_size(std::max<size_t>(sim.sheet_table.size(), 1) * 4);
     need += carve_size(std::max<size_t>(sheets.size() * nr_nc, 1) * 4);
     need += carve_size(std::max<size_t>(debye_f.size(), 1) * 8);
-    need += carve_size(std::max<size_t>(debye_f.size(), 1) * 4) * 2;
+    need += carve_size(std::max<size_t>(debye_f.size(), 1) * 4) * 3;
     need += carve_size(std::max<size_t>(debye_f.size() * sim.poles.size(), 1) * 4);
     need += carve_size(debye_table.size() * 4);
     need += carve_size(std::max<size_t>(t_pulse.size(), 1) * 4);
@@ -867,6 +866,7 @@ int session_new(Gpu* gpu, const HostSim& sim, const RunSpec& rs, Session** out, 
     s->currents = carve<float>(cur, std::max<size_t>(sheets.size() * nr_nc, 1));
     s->debye_f = carve<long long>(cur, std::max<size_t>(debye_f.size(), 1));
     s->debye_dd = carve<float>(cur, std::max<size_t>(debye_f.size(), 1));
+    s->debye_cb = carve<float>(cur, std::max<size_t>(debye_f.size(), 1));
     s->debye_old = carve<float>(cur, std::max<size_t>(debye_f.size(), 1));
     s->debye_state = carve<float>(cur, std::max<size_t>(debye_f.size() * sim.poles.size(), 1));
     s->debye_table = carve<float>(cur, debye_table.size());
@@ -965,6 +965,7 @@ int session_new(Gpu* gpu, const HostSim& sim, const RunSpec& rs, Session** out, 
     rc |= up(s->branch, sim.sheet_table.data(), sim.sheet_table.size() * 4);
     rc |= up(s->debye_f, debye_f.data(), debye_f.size() * 8);
     rc |= up(s->debye_dd, debye_dd.data(), debye_dd.size() * 4);
+    rc |= up(s->debye_cb, debye_cb.data(), debye_cb.size() * 4);
     rc |= up(s->debye_table, debye_table.data(), debye_table.size() * 4);
     rc |= up(d_pulse, t_pulse.data(), t_pulse.size() * 4);
     if (s->local) {

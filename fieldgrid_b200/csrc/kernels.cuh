@@ -181,14 +181,30 @@ __device__ __forceinline__ void debye_post_edge(int q, const long long* __restri
     }
 }
 
-template <typename CID>
-__global__ void k_debye_post(const long long* __restrict__ f, const float* __restrict__ dd, int count,
-                             const float* __restrict__ eold_saved, const float* __restrict__ eold_field,
-                             const CID* __restrict__ node_class, const DevCoef* __restrict__ classes, long long cs,
-                             const float* __restrict__ table, float* __restrict__ state, float* __restrict__ e) {
-    int q = blockIdx.x * blockDim.x + threadIdx.x;
-    if (q < count) debye_post_edge(q, f, dd, count, eold_saved, eold_field, node_class, classes, cs, table, state, e);
+// debye_post_edge with each edge's cb given (cbq, formed once at set-up): no class-id lookup
+// between the edge list and the arithmetic, so every load of an edge issues at once.
+__global__ void k_debye_post_cb(const long long* __restrict__ f, const float* __restrict__ dd,
+                                const float* __restrict__ cbq, int count, const float* __restrict__ eold_saved,
+                                const float* __restrict__ eold_field, const float* __restrict__ table,
+                                float* __restrict__ state, float* __restrict__ e) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= count) return;
+    const long long fi = f[q];
+    const float cb = cbq[q];
+    const float old = eold_saved ? eold_saved[q] : eold_field[fi];
+    const int np = int(table[0]);
+    float s0 = 0.0f;
+    for (int k = 0; k < np; ++k) s0 += 0.5f * (1.0f + table[1 + 2 * k]) * state[(long long)k * count + q];
+    const float next = e[fi] - cb * s0;
+    e[fi] = next;
+    const float de = next - old;
+    const float w = dd[q];
+    for (int k = 0; k < np; ++k) {
+        long long p = (long long)k * count + q;
+        state[p] = table[1 + 2 * k] * state[p] + w * table[2 + 2 * k] * de;
+    }
 }
+
 
 // cpu.rs:262-265
 __device__ __forceinline__ float pulse_at(const StepConst& sc, float t) {

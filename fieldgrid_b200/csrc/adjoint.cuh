@@ -10,7 +10,9 @@
 // otherwise it keeps the full state at the start of about `checkpoints` segments of an even number
 // of steps, and the backward sweep re-runs each segment from its checkpoint (recording that
 // segment's history) before sweeping it: segment recomputation with O(sqrt(N)) field checkpoints
-// when checkpoints ~ sqrt(N).
+// when checkpoints ~ sqrt(N). A re-run marches only the shrinking box of nodes that can still
+// reach the design edges within the segment (FluxJob::rerun_cone), on a second stream while the
+// sweep of the following segment runs.
 //
 // Included at the end of engine.cu (it uses the Session internals).
 #pragma once

@@ -35,6 +35,21 @@ if ROOT not in sys.path:
 BYTES_PER_NODE = 48  # read + write of Ex Ey Ez Hx Hy Hz, f32
 
 
+def max_over_ranks(x: float, world: int, device: str = "cuda") -> float:
+    """The largest of every rank's x (a job's time is its slowest rank's); x itself at N = 1."""
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], device=device, dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_rate(nodes_per_rank: int, steps: int, world: int, ms_max: float) -> float:
+    """Whole-job Mcell-updates/s of replicas: every rank's nodes x steps over the slowest rank's time."""
+    return world * nodes_per_rank * steps / (ms_max / 1e3) / 1e6
+
+
 def log(*a):
     print(*a, file=sys.stderr, flush=True)
 
@@ -470,11 +485,8 @@ def main():
     if world > 1:
         dist.barrier()
     ms = ev0.elapsed_time(ev1)
-    t_max = torch.tensor([ms], device="cuda", dtype=torch.float64)
-    if world > 1:
-        dist.all_reduce(t_max, op=dist.ReduceOp.MAX)
-    ms_max = float(t_max.item())
-    value = world * nn * K / (ms_max / 1e3) / 1e6
+    ms_max = max_over_ranks(ms, world)
+    value = job_rate(nn, K, world, ms_max)
 
     # per-kernel device times of the same step (events between eager launches)
     kt = s.kernel_times(kt_steps)
@@ -504,11 +516,8 @@ def main():
         rec = fdtd.run(g, sim, 0, sc.pulse, ex)
         torch.cuda.synchronize()
         t_e2e = time.perf_counter() - t0
-        te = torch.tensor([t_e2e], device="cuda", dtype=torch.float64)
-        if world > 1:
-            dist.all_reduce(te, op=dist.ReduceOp.MAX)
-        t_e2e = float(te.item())
-        e2e = {"value": world * nn * K / t_e2e / 1e6, "unit": "Mcell/s",
+        t_e2e = max_over_ranks(t_e2e, world)
+        e2e = {"value": job_rate(nn, K, world, t_e2e * 1e3), "unit": "Mcell/s",
                "h2d_bytes_per_step": rec.h2d / K, "d2h_bytes_per_step": rec.d2h / K,
                "run": f"one fg_run of {K} steps on host buffers: pack + upload of the grid, the steps, energy checks "
                       f"every {ex.check_every or 1000}, read-back of the series; wall clock, max over ranks",

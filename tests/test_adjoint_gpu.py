@@ -144,6 +144,24 @@ def test_the_adjoint_through_debye_media_matches_central_differences(gpu, small_
     assert np.array_equal(r.grad_eps, b.grad_eps) and np.array_equal(r.grad_sigma, b.grad_sigma)
 
 
+def test_cone_reruns_reproduce_the_tma_march_history(gpu):
+    """On a grid the forward marches with the TMA kernel (k-layer tiles, CPML shell), re-runs that
+    march only the dependency cone with the direct-load kernel record the same history: the
+    checkpointed gradient equals the stored-history one bit for bit, with Debye media present."""
+    scene, spec, _, _ = W.flux_design(64, 60, 72, pml=8, design=(8, 6, 4), steps=160, checkpoints=0, debye=True)
+    sc = scene()
+    sim = fdtd.Sim.try_new(*sc.args())
+    s = fdtd.Session(gpu, sim, 0, sc.pulse, sc.extras)
+    assert "TMA" in s.variant
+    s.close()
+    a = fdtd.flux_gradient(gpu, sim, 0, sc.pulse, spec)
+    ck = fdtd.FluxSpec(spec.design_lo, spec.design_hi, spec.plane_k, spec.freq, spec.steps, checkpoints=6)
+    b = fdtd.flux_gradient(gpu, sim, 0, sc.pulse, ck)
+    assert b.segments > 2 and np.abs(a.grad_eps).max() > 0
+    assert np.array_equal(a.grad_eps, b.grad_eps)
+    assert np.array_equal(a.grad_sigma, b.grad_sigma)
+
+
 def test_checkpointed_sweep_equals_stored_history(gpu, small):
     scene, spec, eps0, sig0 = small
     sc = scene()

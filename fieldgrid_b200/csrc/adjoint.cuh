@@ -551,7 +551,10 @@ int flux_gradient(Gpu* gpu, const HostSim& sim, uint64_t driven, double f0, doub
 // Many flux gradients on one GPU, in groups of up to `group` jobs: a group's jobs are prepared
 // and their forwards enqueued together; each objective is formed as its forward ends; the
 // backwards are enqueued together, and while they run the next group is prepared and its
-// forwards enqueued, before the group is finished in turn. Each job's results are those of
+// forwards enqueued, before the group is finished in turn. A group also stops growing when the
+// device's free memory would not hold the next job (estimated from the bytes per node the jobs
+// prepared so far took, with half again to spare): its jobs then wait for a later group, and a
+// group that cannot open beside the running one opens after it. Each job's results are those of
 // running it alone. The first error stops the batch (its message names the job).
 int flux_gradient_batch(Gpu* gpu, const std::vector<const HostSim*>& sims, const std::vector<uint64_t>& driven,
                         const std::vector<std::pair<double, double>>& pulses, const std::vector<FluxSpec>& specs,
@@ -559,18 +562,28 @@ int flux_gradient_batch(Gpu* gpu, const std::vector<const HostSim*>& sims, const
     const size_t count = sims.size();
     out.assign(count, FluxResult{});
     if (group <= 0) group = 16;
+    FG_CUDA(cudaSetDevice(gpu->device));
     using Group = std::vector<std::unique_ptr<FluxJob>>;
     int rc = FG_OK;
     size_t bad = 0;
     std::string bad_err;
+    double per_node = 0.0;   // device bytes per node a prepared job took, at most
     auto fail = [&](size_t q, const FluxJob& j) {
         bad = q;
         bad_err = j.err;
     };
-    // prepare jobs [g0, g1) and enqueue their forwards
-    auto open = [&](size_t g0, Group& G) {
-        const size_t g1 = std::min(count, g0 + size_t(group));
-        for (size_t q = g0; q < g1 && !rc; ++q) {
+    auto free_bytes = [] {
+        size_t f = 0, t = 0;
+        return cudaMemGetInfo(&f, &t) == cudaSuccess ? double(f) : 0.0;
+    };
+    // prepare jobs from g0 while they fit (and, with `holding`, the first one only if it fits
+    // beside the running group) and enqueue their forwards; returns the first job left out
+    auto open = [&](size_t g0, Group& G, bool holding) -> size_t {
+        size_t q = g0;
+        for (; q < count && q < g0 + size_t(group) && !rc; ++q) {
+            const double need = 1.5 * per_node * double(sims[q]->nn);
+            const double before = free_bytes();
+            if ((!G.empty() || holding) && per_node > 0.0 && before < need) break;
             auto j = std::make_unique<FluxJob>();
             j->gpu = gpu;
             j->sim = sims[q];
@@ -580,25 +593,33 @@ int flux_gradient_batch(Gpu* gpu, const std::vector<const HostSim*>& sims, const
             j->sp = specs[q];
             j->want_grad = true;
             if ((rc = j->prepare())) fail(q, *j);
+            const double after = free_bytes();
+            if (before > after) per_node = std::max(per_node, (before - after) / double(sims[q]->nn));
             G.push_back(std::move(j));
         }
-        for (size_t q = 0; q < G.size() && !rc; ++q)
-            if ((rc = G[q]->forward())) fail(g0 + q, *G[q]);
+        for (size_t t = 0; t < G.size() && !rc; ++t)
+            if ((rc = G[t]->forward())) fail(g0 + t, *G[t]);
+        return q;
     };
     Group cur, next;
-    open(0, cur);
-    for (size_t g0 = 0; g0 < count && !rc; g0 += size_t(group)) {
+    size_t g0 = 0, g1 = open(0, cur, false);
+    while (!rc && g0 < count) {
         for (size_t q = 0; q < cur.size() && !rc; ++q)
             if ((rc = cur[q]->objective())) fail(g0 + q, *cur[q]);
         for (size_t q = 0; q < cur.size() && !rc; ++q)
             if ((rc = cur[q]->backward())) fail(g0 + q, *cur[q]);
-        if (!rc && g0 + size_t(group) < count) open(g0 + size_t(group), next);
+        size_t g2 = g1;
+        if (!rc && g1 < count) g2 = open(g1, next, true);
         for (size_t q = 0; q < cur.size() && !rc; ++q)
             if ((rc = cur[q]->finish())) fail(g0 + q, *cur[q]);
         if (rc) break;
         for (size_t q = 0; q < cur.size(); ++q) out[g0 + q] = std::move(cur[q]->res);
+        cur.clear();   // the group's memory goes back before a deferred group opens
+        if (next.empty() && g1 < count) g2 = open(g1, next, false);
         cur = std::move(next);
         next.clear();
+        g0 = g1;
+        g1 = g2;
     }
     if (rc) {
         err = "job " + std::to_string(bad) + ": " + bad_err;

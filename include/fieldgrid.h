@@ -303,7 +303,7 @@ int fg_flux_gradient(fg_gpu* g, const fg_sim* sim, uint64_t driven, const fg_pul
  * Sim with its own driven port, pulse and flux spec (precision 32), in groups of `group` runs (0:
  * 16) whose phases are enqueued together, each run on its own streams: the forwards, then each
  * objective as its forward ends, then the backward sweeps (the next group's set-up and forwards
- * overlap them). Each run's results (out[q], and the gradients over spec q's design cells in
+ * overlap them). A group holds fewer runs when the free device memory would not hold the next. Each run's results (out[q], and the gradients over spec q's design cells in
  * grad_eps[q], grad_sigma[q]) are those of running it alone with fg_flux_gradient. The first
  * failing run ends the call; its error names the run. */
 int fg_flux_gradient_batch(fg_gpu* g, const fg_sim* const* sims, const uint64_t* driven, const fg_pulse* pulses,

@@ -22,6 +22,7 @@ static __device__ __align__(256) double g_energy_partials[FG_ENERGY_NOALLOC_MAX_
 namespace {
 
 constexpr int NOALLOC_THREADS = 256;
+constexpr unsigned long long MIN_CHUNK = 2048;   // elements per block at least
 
 // First pass: block b sums E^2 + (376.73 H)^2 over elements [b*chunk, min((b+1)*chunk, n)) of
 // both arrays into g_energy_partials[b] (every slot the second pass reads is written here first,
@@ -88,18 +89,23 @@ int scratch_of(int device, double** out, std::string& err) {
 }  // namespace
 
 extern "C" int fg_energy_noalloc(const float* e, const float* h, uint64_t n, double* out, void* stream) {
-    if (!e || !h || !out) {
+    if (!out || (n > 0 && (!e || !h))) {   // an empty array may come as a null pointer
         fg::set_last_error("fg_energy_noalloc: null pointer");
         return FG_ERR_INVALID;
     }
-    const unsigned long long chunk = FG_ENERGY_NOALLOC_CHUNK;
-    const unsigned long long blocks = (n + chunk - 1) / chunk;
-    if (blocks > FG_ENERGY_NOALLOC_MAX_BLOCKS) {
+    const unsigned long long limit = (unsigned long long)FG_ENERGY_NOALLOC_MAX_BLOCKS * FG_ENERGY_NOALLOC_CHUNK;
+    if (n > limit) {
         fg::set_last_error("fg_energy_noalloc: " + std::to_string(n) + " elements exceed the maximum of " +
-                           std::to_string((unsigned long long)FG_ENERGY_NOALLOC_MAX_BLOCKS * chunk) +
-                           " this entry point's fixed scratch covers");
+                           std::to_string(limit) + " this entry point's fixed scratch covers");
         return FG_ERR_INVALID;
     }
+    // Elements per block, chosen per call so that small and large arrays both spread over the
+    // GPU: n split over at most FG_ENERGY_NOALLOC_MAX_BLOCKS blocks, at least MIN_CHUNK elements
+    // each, a multiple of the block size. At the limit this is FG_ENERGY_NOALLOC_CHUNK.
+    unsigned long long chunk = (n + FG_ENERGY_NOALLOC_MAX_BLOCKS - 1) / FG_ENERGY_NOALLOC_MAX_BLOCKS;
+    if (chunk < MIN_CHUNK) chunk = MIN_CHUNK;
+    chunk = (chunk + NOALLOC_THREADS - 1) / NOALLOC_THREADS * NOALLOC_THREADS;
+    const unsigned long long blocks = (n + chunk - 1) / chunk;
     int device = 0;
     cudaError_t ce = cudaGetDevice(&device);
     if (ce != cudaSuccess) {

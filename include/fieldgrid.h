@@ -227,16 +227,18 @@ void fg_session_free(fg_session* s);
  * No counterpart in the reference. For callers that cannot allocate device memory when they need
  * the energy of a field (e.g. an operator callback running while a host framework's caching
  * allocator owns the device memory, or a loop that must avoid the device-wide synchronisation of
- * cudaMalloc/cudaFree): sum over q < n of e[q]^2 + (376.73 h[q])^2 in f64 (the quantity of
- * cpu.rs:417-421), written to *out. e, h and out are device pointers owned by the caller; the
- * call allocates nothing. Its per-block partial sums live in one fixed array of
- * FG_ENERGY_NOALLOC_MAX_BLOCKS doubles (32 KB) per device, held from the library's load until
- * process exit; each block covers FG_ENERGY_NOALLOC_CHUNK elements, so n is limited to
- * FG_ENERGY_NOALLOC_MAX_BLOCKS * FG_ENERGY_NOALLOC_CHUNK (2^32) and larger n is refused with
- * FG_ERR_INVALID. The first call on a device looks up that array's device address (make it before
- * any stream capture). Every call uses the same array: calls that overlap on the GPU (different
- * streams, or host threads on one device) race; calls ordered on one stream are safe. Work is
- * enqueued on `stream` (NULL = the default stream); read *out after that stream is synchronised. */
+ * cudaMalloc/cudaFree): sum over q < n of e[q]^2 + (376.73 h[q])^2, each term and the sum in f64,
+ * written to *out; n = 0 gives 0, and e and h may then be NULL. e, h and out are device pointers
+ * owned by the caller; the call allocates nothing. Its per-block partial sums live in one fixed
+ * array of FG_ENERGY_NOALLOC_MAX_BLOCKS doubles (32 KB) per device, held from the library's load
+ * until process exit; each call splits its n elements over at most that many blocks, and n is
+ * limited to FG_ENERGY_NOALLOC_MAX_BLOCKS * FG_ENERGY_NOALLOC_CHUNK (2^32): larger n is refused
+ * with FG_ERR_INVALID. The first call on a device looks up that array's device address and keeps
+ * it (make that call before any stream capture); after cudaDeviceReset on that device the kept
+ * address is stale, so do not call this entry point again in that process. Every call uses the
+ * same array: calls that overlap on the GPU (different streams, or host threads on one device)
+ * race; calls ordered on one stream are safe. Work is enqueued on `stream` (NULL = the default
+ * stream); read *out after that stream is synchronised. */
 #define FG_ENERGY_NOALLOC_MAX_BLOCKS 4096
 #define FG_ENERGY_NOALLOC_CHUNK (1u << 20)
 int fg_energy_noalloc(const float* e, const float* h, uint64_t n, double* out, void* stream);
@@ -271,7 +273,8 @@ int fg_far_radiated(fg_gpu* g, const fg_far* f, uint64_t steps, double* total, d
  * design edges; checkpoints = c keeps the full field state at the start of about c segments and
  * re-runs each segment before sweeping it (sqrt(steps) checkpoints: segment recomputation).
  * The design box must stay off the grid boundary and off PEC, lumped, port and Debye edges; the
- * Sim must hold no Debye media, inductors, thin wires or resistive sheets. */
+ * Sim may hold Debye media outside the design box (their ADE is transposed in the backward sweep
+ * and carried by the checkpoints), but no inductors, thin wires or resistive sheets. */
 typedef struct fg_flux_spec {
     uint64_t design_lo[3], design_hi[3];  /* design cells [lo, hi), cell indices as in Materials */
     uint64_t plane_k;                     /* node index of the flux plane along z */

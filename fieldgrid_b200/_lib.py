@@ -93,6 +93,7 @@ def _declare(L):
         "fg_flux_gradient": (C.c_int, [vp, vp, u64, P(A.fg_pulse), P(A.fg_flux_spec), P(A.fg_flux_result), P(dbl),
                                        P(dbl), cp, sz]),
         "fg_energy_noalloc": (C.c_int, [vp, vp, u64, vp, vp]),
+        "fg_port_spectra": (C.c_int, [P(C.c_float), u64, u64, u64, dbl, P(dbl), u64, P(dbl), P(dbl)]),
         "fg_flux_gradient_batch": (C.c_int, [vp, vp, P(u64), P(A.fg_pulse), P(A.fg_flux_spec), u64, C.c_int,
                                              P(A.fg_flux_result), vp, vp, cp, sz]),
     }

@@ -459,6 +459,42 @@ int fg_far_intensity(fg_gpu* g, const fg_far* f, const double* dirs, uint64_t n,
     return FG_OK;
 }
 
+// The port's voltage and current spectra of sims-antenna's finish (sims-antenna/src/fdtd/mod.rs:
+// 229-266): per frequency f, V = sum_n V_n dt e^{-j w (n+1) dt} and I = sum_n I_n dt e^{-j w (n+1/2) dt}
+// (E is sampled at (n+1) dt, H at (n+1/2) dt), w = 2 pi f, with each phase factor advanced by one
+// complex multiplication per step in f64 as the reference does (not re-evaluated per step).
+int fg_port_spectra(const float* series, uint64_t steps, uint64_t ports, uint64_t port, double dt,
+                    const double* freqs, uint64_t nf, double* v, double* i) {
+    if ((steps && !series) || (nf && (!freqs || !v || !i)) || port >= ports || !(dt > 0.0)) {
+        g_last_error = "fg_port_spectra: invalid arguments";
+        return FG_ERR_INVALID;
+    }
+#pragma omp parallel for schedule(static)
+    for (long long q = 0; q < (long long)nf; ++q) {
+        const double w = 2.0 * PI * freqs[q];
+        // C64::from_polar(r, t) = (r cos t, r sin t)
+        const double re_rot = std::cos(-w * dt), im_rot = std::sin(-w * dt);
+        double pe_re = dt * std::cos(-w * dt), pe_im = dt * std::sin(-w * dt);
+        double ph_re = dt * std::cos(-w * 0.5 * dt), ph_im = dt * std::sin(-w * 0.5 * dt);
+        double vr = 0.0, vi = 0.0, ir = 0.0, ii = 0.0;
+        for (uint64_t n = 0; n < steps; ++n) {
+            const double vn = double(series[(n * ports + port) * 2]), in = double(series[(n * ports + port) * 2 + 1]);
+            vr += pe_re * vn;
+            vi += pe_im * vn;
+            ir += ph_re * in;
+            ii += ph_im * in;
+            // (a + bj)(c + dj) = (ac - bd) + (ad + bc)j
+            const double per = pe_re * re_rot - pe_im * im_rot, pei = pe_re * im_rot + pe_im * re_rot;
+            const double phr = ph_re * re_rot - ph_im * im_rot, phi = ph_re * im_rot + ph_im * re_rot;
+            pe_re = per; pe_im = pei;
+            ph_re = phr; ph_im = phi;
+        }
+        v[2 * q] = vr; v[2 * q + 1] = vi;
+        i[2 * q] = ir; i[2 * q + 1] = ii;
+    }
+    return FG_OK;
+}
+
 // Far::radiated (ntff.rs:122-136)
 int fg_far_radiated(fg_gpu* g, const fg_far* f, uint64_t steps, double* total, double* peak) {
     if (!f || !total || !peak || steps == 0) return FG_ERR_INVALID;

@@ -146,6 +146,10 @@ struct Session {
     // inside the design history's dependency cone)
     bool boxed = false;
     int box_lo[3] = {0, 0, 0}, box_hi[3] = {0, 0, 0};
+    // the march's mbarrier wait limit and its test knob (TmaArgs::stall_plane); set at creation
+    // from FIELDGRID_TEST_WAIT_NS / FIELDGRID_TEST_STALL_PLANE, which only the failure-path test sets
+    unsigned long long wait_ns = tma::WAIT_LIMIT_NS;
+    int stall_plane = -1;
 };
 
 static constexpr int ENERGY_BLOCKS = 1024;
@@ -435,7 +439,7 @@ void plan_tma(Session& s) {
 int launch_tma(Session& s, int parity, float* e_out, float* h_out, float* psi_h_out) {
     const TmaPlan& t = s.tma;
     TmaArgs a{s.geom, s.classes, e_out, h_out, s.sc.k_mu, s.clean_lo[2], s.clean_hi[1], s.clean_hi[2], s.tma_blocks,
-              0, 1, s.psi, psi_h_out, s.tables, s.counter, s.error};
+              0, 1, s.psi, psi_h_out, s.tables, s.counter, s.error, s.wait_ns, s.stall_plane};
     // without k-layer tiles the last two maps are never read
     const CUtensorMap& pze = t.pz ? t.pze : t.c;
     const CUtensorMap& pzh = t.pz ? t.pzh[parity] : t.c;
@@ -992,6 +996,10 @@ int session_new(Gpu* gpu, const HostSim& sim, const RunSpec& rs, Session** out, 
         FG_CUDA(cudaMemset(s->hist_base, 0, sizeof(long long)));
     }
     s->shape = choose_shape(g, s->cid_bytes, s->n_wires > 0);
+    if (const char* v = std::getenv("FIELDGRID_TEST_WAIT_NS"))
+        s->wait_ns = std::min<unsigned long long>(std::max<unsigned long long>(std::strtoull(v, nullptr, 10),
+                                                                               tma::WAIT_LIMIT_MIN_NS), tma::WAIT_LIMIT_NS);
+    if (const char* v = std::getenv("FIELDGRID_TEST_STALL_PLANE")) s->stall_plane = std::atoi(v);
     plan_tma(*s);
     if (s->tma.ok)
         s->variant = "TMA fused march, tile " + std::to_string(s->tma.tj) + "x" + std::to_string(s->tma.tk) + ", " +

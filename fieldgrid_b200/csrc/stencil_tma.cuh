@@ -100,6 +100,7 @@ __device__ __forceinline__ bool consumers_sync_or(bool flag, int count) {
 }
 
 constexpr uint64_t WAIT_LIMIT_NS = 2000000000ull;  // 2 s: far beyond any legitimate copy
+constexpr uint64_t WAIT_LIMIT_MIN_NS = 1000000ull;  // the shortest limit a run may ask for (1 ms)
 
 }  // namespace tma
 
@@ -148,6 +149,10 @@ struct TmaArgs {
     const float* tables;                 // LOCAL: per block (entry of `blocks`), LOCAL_CLASSES x (ca[3], cb[3])
     unsigned* counter;
     int* error;
+    unsigned long long wait_ns;          // the limit of every mbarrier wait (2 s in normal runs)
+    int stall_plane;                     // test knob, -1 in normal runs: the full barrier of this
+                                         // plane expects 16 bytes more than its copies deliver, so
+                                         // the waits on it run out (the failure path under test)
 };
 
 // The E values around one point that its H update needs (own, +j, +k, +i neighbours).
@@ -320,17 +325,18 @@ __device__ __forceinline__ void tma_march(const CUtensorMap& map_e, const CUtens
         if (tid != TMA_CONSUMERS) return;
         for (int p = p_first; p <= p_last; ++p) {
             const int u = p - p_first, s = u % STAGES, n = u / STAGES;
-            if (!tma::mbar_wait(&empty[s], uint32_t((n & 1) ^ 1), tma::WAIT_LIMIT_NS)) {
+            if (!tma::mbar_wait(&empty[s], uint32_t((n & 1) ^ 1), a.wait_ns)) {
                 atomicExch(a.error, 1);
+                // the copies already issued land before the block leaves (bounded waits)
                 for (int q = max(p_first, p - STAGES); q < p; ++q) {
                     const int uq = q - p_first;
-                    tma::mbar_wait(&full[uq % STAGES], uint32_t((uq / STAGES) & 1), tma::WAIT_LIMIT_NS);
+                    tma::mbar_wait(&full[uq % STAGES], uint32_t((uq / STAGES) & 1), a.wait_ns);
                 }
                 return;
             }
             unsigned char* st = stages + s * L::STAGE;
             const bool zp = ZL && p < i1;   // plane i1 supplies E only
-            tma::mbar_expect_tx(&full[s], L::TX + (zp ? 2 * 2 * zc * 4 : 0));
+            tma::mbar_expect_tx(&full[s], L::TX + (zp ? 2 * 2 * zc * 4 : 0) + (p == a.stall_plane ? 16 : 0));
             tma::load_4d(st, &map_e, &full[s], k0 - 4, j0 - 1, p, 0);
             tma::load_4d(st + L::al(L::E_BYTES), &map_h, &full[s], k0 - 4, j0 - 1, p, 0);
             tma::load_3d(st + L::al(L::E_BYTES) + L::al(L::H_BYTES), &map_c, &full[s], k0 & ~15, j0, p);
@@ -374,8 +380,8 @@ __device__ __forceinline__ void tma_march(const CUtensorMap& map_e, const CUtens
         const int u = p - p_first;
         const int s = u % STAGES, s1 = (u + 1) % STAGES;
         const bool pre = p < i0;  // the plane before the segment: H only, nothing written
-        if (!tma::mbar_wait(&full[s], uint32_t((u / STAGES) & 1), tma::WAIT_LIMIT_NS)) bad = true;
-        if (!tma::mbar_wait(&full[s1], uint32_t(((u + 1) / STAGES) & 1), tma::WAIT_LIMIT_NS)) bad = true;
+        if (!tma::mbar_wait(&full[s], uint32_t((u / STAGES) & 1), a.wait_ns)) bad = true;
+        if (!tma::mbar_wait(&full[s1], uint32_t(((u + 1) / STAGES) & 1), a.wait_ns)) bad = true;
         const float* E = reinterpret_cast<const float*>(stages + s * L::STAGE);
         const float* E1 = reinterpret_cast<const float*>(stages + s1 * L::STAGE);
         const float* H = reinterpret_cast<const float*>(stages + s * L::STAGE + L::al(L::E_BYTES));

@@ -262,6 +262,14 @@ int fg_far_intensity(fg_gpu* g, const fg_far* f, const double* dirs, uint64_t n,
 /* Far::radiated (ntff.rs:122-136): total radiated power and peak intensity. */
 int fg_far_radiated(fg_gpu* g, const fg_far* f, uint64_t steps, double* total, double* peak);
 
+/* ---- port spectra (sims-antenna/src/fdtd/mod.rs:229-266, finish) -------------------------
+ * The running DFT of one port's V/I series at nf frequencies, in f64: V(f) = sum_n V_n dt
+ * e^{-j w (n+1) dt}, I(f) = sum_n I_n dt e^{-j w (n+1/2) dt}, w = 2 pi f. series is the record's
+ * (steps * ports * 2) floats; v and i receive nf (re, im) pairs. The caller forms Z = V/I,
+ * S11 = (Z - 50)/(Z + 50) and P_in = Re(V conj(I))/2 from them, as finish does. Host code. */
+int fg_port_spectra(const float* series, uint64_t steps, uint64_t ports, uint64_t port, double dt,
+                    const double* freqs, uint64_t nf, double* v, double* i);
+
 /* ---- adjoint: the gradient of a flux objective over a box of design voxels ----
  * No counterpart in the reference (sims_field::fdtd has no adjoint). The objective is
  * J = |F|^2, F = sum over the (i, j) window of the z-plane plane_k of

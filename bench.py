@@ -452,7 +452,7 @@ def main():
     K, W = args.steps, max(args.warmup, 3)
     kt_steps = 10
     t = time.time()
-    sc = workload(args.cells, W + K + kt_steps, fused=not args.separate, pml=args.pml)
+    sc = workload(args.cells, W + K + kt_steps + (48 if K >= 48 else 0), fused=not args.separate, pml=args.pml)
     t_mat = time.time() - t
     t = time.time()
     sim = fdtd.Sim.try_new(*sc.args())
@@ -467,6 +467,11 @@ def main():
         f"materials {t_mat:.1f}s setup {t_setup:.1f}s upload {t_session:.2f}s, {s.variant}")
     stream = torch.cuda.ExternalStream(s.stream)
     s.step(W)
+    if K >= 48:
+        # the two-step mode captures its 48-step graph for a step phase (t mod 6) on first use:
+        # 48 more warm-up steps capture it for the phase the timed steps start at
+        s.step(48)
+        W += 48
     s.sync()
     torch.cuda.synchronize()
     if world > 1:
@@ -497,8 +502,11 @@ def main():
     debye_edges = sim.count("debye_edges")
     s.close()
     # the field update of a step: the march over the clean box plus the CPML shell kernels (or the
-    # separate H and E kernels); its time is what the 48 B/node roofline is measured against
-    field_parts = [k for k in ("fused_step", "shell_h", "shell_e", "update_h", "update_e") if k in kt]
+    # separate H and E kernels; in the two-step mode half a two-step march plus the one-step march
+    # of the remaining tiles and the shell, per step); its time is what the 48 B/node roofline is
+    # measured against
+    field_parts = [k for k in ("two_step", "edge_step", "fused_step", "shell_h", "shell_e", "update_h", "update_e")
+                   if k in kt]
     dom_name, dom_ms = "field_update", sum(kt[k] for k in field_parts)
     peak, peak_src = measured_peaks()
     achieved = BYTES_PER_NODE * nn / (dom_ms / 1e3) / 1e9

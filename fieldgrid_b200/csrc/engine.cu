@@ -20,6 +20,7 @@
 #include "stencil_separate.cuh"
 #include "stencil_shell.cuh"
 #include "stencil_tma.cuh"
+#include "stencil_tb2.cuh"
 #include "adjoint_kernels.cuh"
 
 #include <cudaTypedefs.h>
@@ -150,6 +151,38 @@ struct Session {
     // from FIELDGRID_TEST_WAIT_NS / FIELDGRID_TEST_STALL_PLANE, which only the failure-path test sets
     unsigned long long wait_ns = tma::WAIT_LIMIT_NS;
     int stall_plane = -1;
+    int2* tma_own = nullptr;        // per block of the one-step march: the rows it writes
+    // ---- the two-step mode (stencil_tb2.cuh). Step t reads field set, z-slab psi slot and Debye
+    // state slot t mod 3 and writes (t + 1) mod 3; the x/y slabs keep the one-step scheme (E in
+    // place, H by the parity of t). A double step is the two-step march over the interior tiles
+    // beside one step of the remaining tiles and the shell (second stream), then one more step of
+    // those.
+    bool slots = false;
+    float *e3 = nullptr, *h3 = nullptr;              // the third field set
+    float* zslot[3] = {nullptr, nullptr, nullptr};   // z-slab psi by time slot (psi_off offsets)
+    float* dslot[3] = {nullptr, nullptr, nullptr};   // Debye state by time slot: [edge * np + pole]
+    unsigned* dbase = nullptr;                       // per device node: its first Debye edge
+    long long* dd_f = nullptr;                       // Debye edges in node order, those of the one-step
+    unsigned* dd_s = nullptr;                        // tiles and shell first (dd_c of them), then the
+    float* dd_w = nullptr;                           // two-step tiles' (dd_all in all): field index,
+    float* dd_cb = nullptr;                          // state index, weight, cb
+    int dd_c = 0, dd_all = 0;
+    int4* c_blocks = nullptr;                        // the one-step tiles of a double step
+    int2* c_own = nullptr;
+    float* c_tables = nullptr;
+    int n_cblocks = 0;
+    int4* tb_blocks = nullptr;                       // the two-step tiles
+    int* tb_idbase = nullptr;
+    uint8_t* tb_ids = nullptr;
+    float* tb_tables = nullptr;
+    int n_tb = 0, tb_zblocks = 0, tb_rim = 0, tb_smem = 0;
+    size_t tb_planes = 0;                            // planes of the block-major class-id array
+    CUtensorMap tbm_e[3], tbm_h[3], tbm_c, tbm_zh[3], tbm_ze[3];   // the two-step march's maps
+    CUtensorMap d1_e[3], d1_h[3], d1_pze[3], d1_pzh[3];            // the one-step march's, per set/slot
+    cudaStream_t side = nullptr;
+    cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
+    std::map<int, cudaGraphExec_t> slot_graphs;      // captured steps by (kind, phase t mod 6)
+    std::vector<void*> extra_allocs;
 };
 
 static constexpr int ENERGY_BLOCKS = 1024;
@@ -252,6 +285,7 @@ inline int tma_ktiles(int za, int zb, int n2) {
 // the shell kernels. Blocks are (k0, j0, i0, i1): a TJ x TK tile over one x-segment.
 struct CleanPlan {
     std::vector<int4> blocks;    // k0 | TMA_ZL_TILE for the zblocks tiles that reach the k layer
+    std::vector<int2> own;       // per block: the rows [x, y) it writes (its tile's rows inside the box)
     int zblocks = 0;
     int seg = 0;                 // planes per block (at most)
     int lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
@@ -276,7 +310,11 @@ bool clean_range(const Axis& ax, int n, int& a, int& b) {
 
 // With z_layer (the z-slab psi fits the march's staged boxes) the box spans every column of its
 // rows and planes, and tiles that reach the k layer run the ZL instantiation.
-CleanPlan plan_clean(const HostSim& sim, const Geom& g, bool z_layer, int seg_fixed) {
+// With `anchor` >= 0 the tiles' rows are laid out so that a tile starts at row `anchor` (the
+// first tile may start below the box and own fewer rows), and `segs` (when not empty) gives the
+// x-segments explicitly: the two-step march pairs these tiles and reuses these segments.
+CleanPlan plan_clean(const HostSim& sim, const Geom& g, bool z_layer, int seg_fixed, int anchor = -1,
+                     const std::vector<int2>& segs = {}) {
     CleanPlan out;
     const int n[3] = {g.n0, g.n1, g.n2};
     for (int a = 0; a < 3; ++a)
@@ -290,24 +328,34 @@ CleanPlan plan_clean(const HostSim& sim, const Geom& g, bool z_layer, int seg_fi
     if (out.lo[2] >= out.hi[2]) return out;
     out.kbase = out.lo[2] & ~7;
     const int kt = tma_ktiles(out.kbase, out.hi[2], g.n2);
-    const int jt = (out.hi[1] - out.lo[1] + TMA_TJ - 1) / TMA_TJ;
+    // tile rows: from the box's first row, or laid out around `anchor`
+    const int jfirst = anchor < 0 ? out.lo[1] : anchor - TMA_TJ * ((anchor - out.lo[1] + TMA_TJ - 1) / TMA_TJ);
+    const int jt = (out.hi[1] - jfirst + TMA_TJ - 1) / TMA_TJ;
     const int xw = out.hi[0] - out.lo[0];
     // x-planes per block: enough blocks for several waves of 3 blocks per SM, at most TMA_SEGMAX
     int seg = TMA_SEGMAX;
     while (seg > 8 && (long long)kt * jt * ((xw + seg - 1) / seg) < 148 * 3 * 6) seg /= 2;
     if (seg_fixed > 0) seg = std::min(seg_fixed, TMA_SEGMAX);
-    out.seg = seg;
-    const int ns = (xw + seg - 1) / seg;
+    std::vector<int2> sg = segs;
+    if (sg.empty()) {
+        const int ns = (xw + seg - 1) / seg;
+        for (int q = 0; q < ns; ++q)
+            sg.push_back(make_int2(out.lo[0] + int((long long)xw * q / ns), out.lo[0] + int((long long)xw * (q + 1) / ns)));
+    }
+    out.seg = 0;
+    for (const int2& v : sg) out.seg = std::max(out.seg, v.y - v.x);
     auto hot_k = [&](int k) { return sim.ax[2].node[size_t(k)].slot_e >= 0 || sim.ax[2].node[size_t(k)].slot_h >= 0; };
-    for (int q = 0; q < ns; ++q) {
-        const int i0 = out.lo[0] + int((long long)xw * q / ns), i1 = out.lo[0] + int((long long)xw * (q + 1) / ns);
+    for (const int2& v : sg) {
+        const int i0 = v.x, i1 = v.y;
         for (int by = 0; by < jt; ++by)
             for (int bx = 0; bx < kt; ++bx) {
                 const int k0 = out.kbase + bx * TMA_TK;
+                const int j0 = jfirst + by * TMA_TJ;
                 bool edge = false;   // a column of the tile, its halo column or right-edge column is in the layer
                 for (int k = std::max(k0 - 1, 0); k <= std::min(k0 + TMA_TK, g.n2 - 1); ++k) edge = edge || hot_k(k);
                 out.zblocks += edge;
-                out.blocks.push_back(make_int4(edge ? (k0 | TMA_ZL_TILE) : k0, out.lo[1] + by * TMA_TJ, i0, i1));
+                out.blocks.push_back(make_int4(edge ? (k0 | TMA_ZL_TILE) : k0, j0, i0, i1));
+                out.own.push_back(make_int2(std::max(j0, out.lo[1]), std::min(j0 + TMA_TJ, out.hi[1])));
             }
     }
     // the shell rows around the clean box
@@ -347,14 +395,15 @@ LocalClasses build_local(const HostSim& sim, const Geom& g, const CleanPlan& cp)
         const int kbeg = std::max(k0, cp.lo[2]);
         int kend = std::min(k0 + TMA_TK, cp.hi[2]);
         if (cp.hi[2] == g.n2 && k0 + TMA_TK == g.n2 - 1) kend = g.n2;  // the owned right-edge column
-        const int jend = std::min(j0 + TMA_TJ, cp.hi[1]);
+        const int jbeg = cp.own[size_t(r)].x, jend = cp.own[size_t(r)].y;
         uint32_t keys[512];
         uint16_t vals[512];
         std::fill(keys, keys + 512, 0xffffffffu);
         int count = 0;
         float* tab = out.tables.data() + size_t(r) * LOCAL_CLASSES * 6;
+        (void)j0;
         for (int i = i0; i < i1 && !over; ++i)
-            for (int j = j0; j < jend && !over; ++j)
+            for (int j = jbeg; j < jend && !over; ++j)
                 for (int k = kbeg; k < kend; ++k) {
                     const uint32_t gid = sim.node_class[(size_t(i) * n1 + j) * n2 + k];
                     uint32_t h = (gid * 2654435761u) & 511u;
@@ -439,7 +488,7 @@ void plan_tma(Session& s) {
 int launch_tma(Session& s, int parity, float* e_out, float* h_out, float* psi_h_out) {
     const TmaPlan& t = s.tma;
     TmaArgs a{s.geom, s.classes, e_out, h_out, s.sc.k_mu, s.clean_lo[2], s.clean_hi[1], s.clean_hi[2], s.tma_blocks,
-              0, 1, s.psi, psi_h_out, s.tables, s.counter, s.error, s.wait_ns, s.stall_plane};
+              s.tma_own, 0, 1, s.psi, psi_h_out, s.tables, s.counter, s.error, s.wait_ns, s.stall_plane};
     // without k-layer tiles the last two maps are never read
     const CUtensorMap& pze = t.pz ? t.pze : t.c;
     const CUtensorMap& pzh = t.pz ? t.pzh[parity] : t.c;
@@ -502,12 +551,13 @@ int enqueue_step(Session& s, int parity, std::string& err) {
             const unsigned gb = (shell_rows + SHELL_THREADS / 32 - 1) / (SHELL_THREADS / 32);
             mark("shell_h");
             k_shell_h<<<gb, SHELL_THREADS, 0, st>>>(g, s.shell, s.kax, e_in, h_in, h_out, parity ? s.psi_h2 : s.psi,
+                                                    parity ? s.psi : s.psi_h2, parity ? s.psi_h2 : s.psi,
                                                     parity ? s.psi : s.psi_h2, s.sc.k_mu);
             mark("shell_e");
             switch (s.cid_bytes) {
-                case 1: k_shell_e<uint8_t><<<gb, SHELL_THREADS, 0, st>>>(g, s.shell, s.kax, (const uint8_t*)s.node_class, s.classes, h_out, e_in, e_out, s.psi); break;
-                case 2: k_shell_e<uint16_t><<<gb, SHELL_THREADS, 0, st>>>(g, s.shell, s.kax, (const uint16_t*)s.node_class, s.classes, h_out, e_in, e_out, s.psi); break;
-                default: k_shell_e<uint32_t><<<gb, SHELL_THREADS, 0, st>>>(g, s.shell, s.kax, (const uint32_t*)s.node_class, s.classes, h_out, e_in, e_out, s.psi); break;
+                case 1: k_shell_e<uint8_t><<<gb, SHELL_THREADS, 0, st>>>(g, s.shell, s.kax, (const uint8_t*)s.node_class, s.classes, h_out, e_in, e_out, s.psi, s.psi, s.psi); break;
+                case 2: k_shell_e<uint16_t><<<gb, SHELL_THREADS, 0, st>>>(g, s.shell, s.kax, (const uint16_t*)s.node_class, s.classes, h_out, e_in, e_out, s.psi, s.psi, s.psi); break;
+                default: k_shell_e<uint32_t><<<gb, SHELL_THREADS, 0, st>>>(g, s.shell, s.kax, (const uint32_t*)s.node_class, s.classes, h_out, e_in, e_out, s.psi, s.psi, s.psi); break;
             }
         }
         if (s.n_sheets) {
@@ -554,6 +604,13 @@ int enqueue_step(Session& s, int parity, std::string& err) {
 }
 
 uint64_t count_launches(const Session& s) {
+    if (s.slots) {
+        // a double step: the two-step march and twice (march, shell H and E, Debye, sources+probes)
+        const uint64_t one = 1 + ((s.shell.ra + s.shell.rb + s.shell.rc) ? 2 : 0) + (s.dd_c > 0 ? 1 : 0) +
+                             ((s.n_sources || s.n_inductors) && s.n_ports == 1 ? 1
+                              : uint64_t(s.n_sources || s.n_inductors) + uint64_t(s.n_ports > 0));
+        return (1 + 2 * one + 1) / 2;
+    }
     uint64_t n = 1;  // the field update (fused) or H update (separate)
     if (s.tma.ok && !s.direct && s.shell.ra + s.shell.rb + s.shell.rc > 0) n += 2;  // the CPML shell around the TMA march
     if (!s.fused) n += 1 + (s.n_debye ? 1 : 0);
@@ -580,6 +637,513 @@ int capture(Session& s, int steps, int parity0, cudaGraphExec_t* out, std::strin
     ce = cudaGraphInstantiate(out, graph, 0);
     cudaGraphDestroy(graph);
     if (ce != cudaSuccess) { err = std::string("cudaGraphInstantiate: ") + cudaGetErrorString(ce); return FG_ERR_CUDA; }
+    return FG_OK;
+}
+
+// ---- the two-step mode: plan --------------------------------------------------------------
+
+// The layout of a double step over the clean box: the two-step tiles (14 x 64 columns over
+// x-segments, each tile the pair of one-step tiles it replaces) and the one-step tiles left beside
+// them. Tiles whose halo (two nodes and two planes around them) would reach a node with its own
+// per-step terms (a port edge, a probe loop, a source or an inductor) or would need more than
+// LOCAL_CLASSES coefficient classes stay one-step. Two-step tiles next to a one-step tile (or the
+// shell) write their step-(n+1) fields as well ("rim").
+struct SlotPlan {
+    bool ok = false;
+    std::string why;
+    CleanPlan cp;                       // the one-step plan, rows and segments aligned with the tiles
+    std::vector<int4> tb;               // two-step tiles: k0 | TMA_ZL_TILE | TB_RIM, j0, i0, i1
+    std::vector<int> idbase;            // per two-step tile: its first plane in `ids`
+    std::vector<uint8_t> ids;           // block-major class ids: [plane][16 rows][TB_CW columns]
+    std::vector<float> tables;          // per two-step tile: LOCAL_CLASSES x (ca[3], cb[3], dd[3])
+    std::vector<int> cidx;              // one-step tiles of a double step (indices into cp.blocks)
+    std::vector<unsigned> dbase;        // per device node: its first Debye edge
+    std::vector<long long> dd_f;        // Debye edges in node order: one-step ones first
+    std::vector<unsigned> dd_s;
+    std::vector<float> dd_w, dd_cb;
+    int dd_c = 0;
+    int zblocks = 0, rim = 0;
+};
+
+SlotPlan plan_slots(const HostSim& sim, const Geom& g, bool z_layer, const std::vector<uint64_t>& special) {
+    SlotPlan P;
+    const int n[3] = {g.n0, g.n1, g.n2};
+    int lo[3], hi[3];
+    for (int a = 0; a < 3; ++a)
+        if (!clean_range(sim.ax[a], n[a], lo[a], hi[a]) && !(a == 2 && z_layer)) { P.why = "no clean box"; return P; }
+    // rows: the tile's halo rows j0 - 2 .. j0 + 15 stay in the clean rows [ya - 1, yb) and off the
+    // grid's first and last rows (j0 >= 2, j0 + 16 <= n1); planes likewise
+    const int ja = std::max(lo[1] + 1, 2);
+    const int jlim = std::min(hi[1], g.n1) - 2;
+    const int J = jlim > ja ? (jlim - ja) / TB_TJ : 0;
+    const int ia = std::max(lo[0] + 1, 2), ib = std::min(hi[0] - 2, g.n0 - 2);
+    if (J < 1 || ib - ia < 4) { P.why = "the interior is too small for two-step tiles"; return P; }
+    std::vector<int2> rsegs, segs;
+    {
+        const int w = ib - ia, ns = (w + TB_SEGMAX - 1) / TB_SEGMAX;
+        for (int q = 0; q < ns; ++q) rsegs.push_back(make_int2(ia + int((long long)w * q / ns), ia + int((long long)w * (q + 1) / ns)));
+    }
+    if (lo[0] < ia) segs.push_back(make_int2(lo[0], ia));
+    segs.insert(segs.end(), rsegs.begin(), rsegs.end());
+    if (ib < hi[0]) segs.push_back(make_int2(ib, hi[0]));
+    P.cp = plan_clean(sim, g, z_layer, 0, ja, segs);
+    if (!P.cp.ok) { P.why = "no clean box"; return P; }
+    const CleanPlan& cp = P.cp;
+    const int kt = tma_ktiles(cp.kbase, cp.hi[2], g.n2);
+    const int NS = int(rsegs.size());
+    auto flat = [&](int sg, int q, int bx) { return (size_t(sg) * J + q) * kt + bx; };
+    std::vector<uint8_t> on(size_t(NS) * J * kt, 1);
+    // halo of a tile: planes [i0 - 2, i1 + 2), rows [j0 - 2, j0 + 16), columns [k0 - 2, k0 + 66)
+    for (uint64_t id : special) {
+        const int i = int(id / (uint64_t(g.n1) * g.n2)), j = int((id / g.n2) % g.n1), k = int(id % g.n2);
+        for (int sg = 0; sg < NS; ++sg) {
+            if (i < rsegs[sg].x - 2 || i >= rsegs[sg].y + 2) continue;
+            for (int q = 0; q < J; ++q) {
+                const int j0 = ja + TB_TJ * q;
+                if (j < j0 - 2 || j >= j0 + 16) continue;
+                for (int bx = 0; bx < kt; ++bx) {
+                    const int k0 = cp.kbase + TB_TK * bx;
+                    if (k >= k0 - 2 && k < k0 + 66) on[flat(sg, q, bx)] = 0;
+                }
+            }
+        }
+    }
+    // Debye edges in node order; per node its first edge (or none)
+    const size_t nn = sim.nn, n1 = g.n1, n2 = g.n2;
+    std::vector<std::pair<uint64_t, uint32_t>> order;   // (id, comp)
+    order.reserve(sim.debye_edges.size());
+    for (const auto& q : sim.debye_edges) order.push_back({q.id, q.comp});
+    std::vector<size_t> perm(order.size());
+    for (size_t q = 0; q < perm.size(); ++q) perm[q] = q;
+    std::sort(perm.begin(), perm.end(), [&](size_t x, size_t y) { return order[x] < order[y]; });
+    std::vector<uint32_t> dfirst(sim.debye_edges.empty() ? 0 : nn, 0xffffffffu);
+    for (size_t e = 0; e < perm.size(); ++e) {
+        const uint64_t id = sim.debye_edges[perm[e]].id;
+        if (dfirst[id] == 0xffffffffu) dfirst[id] = uint32_t(e);
+    }
+    auto dd_of = [&](uint64_t id, float (&dd)[3]) {
+        dd[0] = dd[1] = dd[2] = 0.f;
+        if (dfirst.empty() || dfirst[id] == 0xffffffffu) return;
+        for (size_t e = dfirst[id]; e < perm.size() && sim.debye_edges[perm[e]].id == id; ++e)
+            dd[sim.debye_edges[perm[e]].comp] = float(sim.debye_edges[perm[e]].dd);
+    };
+    // per candidate tile: its coefficient classes over the region whose E it forms
+    // (planes i0 - 1 .. i1, rows j0 - 1 .. j0 + 14, columns k0 - 1 .. k0 + 64)
+    const long long cand = (long long)NS * J * kt;
+    std::vector<float> ctab(size_t(cand) * LOCAL_CLASSES * 9, 0.f);
+    std::vector<size_t> cand_idbase(static_cast<size_t>(cand));
+    {
+        size_t acc = 0;
+        for (long long c = 0; c < cand; ++c) {
+            cand_idbase[size_t(c)] = acc;
+            const int sg = int(c / ((long long)J * kt));
+            acc += size_t(rsegs[sg].y - rsegs[sg].x + 2);
+        }
+        P.ids.assign(acc * 16 * TB_CW, 0);
+    }
+#pragma omp parallel for schedule(dynamic, 4)
+    for (long long c = 0; c < cand; ++c) {
+        if (!on[size_t(c)]) continue;
+        const int sg = int(c / ((long long)J * kt)), q = int((c / kt) % J), bx = int(c % kt);
+        const int i0 = rsegs[sg].x, i1 = rsegs[sg].y, j0 = ja + TB_TJ * q, k0 = cp.kbase + TB_TK * bx;
+        struct Key { uint32_t gid; float dd[3]; };
+        Key keys[512];
+        bool used[512] = {};
+        uint8_t vals[512];
+        int count = 0;
+        bool over = false;
+        float* tab = ctab.data() + size_t(c) * LOCAL_CLASSES * 9;
+        uint8_t* idp = P.ids.data() + cand_idbase[size_t(c)] * 16 * TB_CW;
+        for (int i = i0 - 1; i <= i1 && !over; ++i)
+            for (int r = -1; r < 15 && !over; ++r)
+                for (int cc = -1; cc < 65; ++cc) {
+                    const int j = j0 + r, k = k0 + cc;
+                    if (k < 0 || k >= g.n2) continue;
+                    const uint64_t id = (uint64_t(i) * n1 + uint64_t(j)) * n2 + uint64_t(k);
+                    Key key;
+                    key.gid = sim.node_class[id];
+                    dd_of(id, key.dd);
+                    uint32_t hsh = key.gid * 2654435761u;
+                    for (int t = 0; t < 3; ++t) {
+                        uint32_t b;
+                        std::memcpy(&b, &key.dd[t], 4);
+                        hsh ^= b * (0x9e3779b9u + 2u * uint32_t(t));
+                        hsh *= 0x85ebca6bu;
+                    }
+                    uint32_t h = hsh & 511u;
+                    while (used[h] && !(keys[h].gid == key.gid && std::memcmp(keys[h].dd, key.dd, 12) == 0)) h = (h + 1) & 511u;
+                    if (!used[h]) {
+                        if (count == LOCAL_CLASSES) { over = true; break; }
+                        used[h] = true;
+                        keys[h] = key;
+                        vals[h] = uint8_t(count);
+                        const Coef& cf = sim.classes[key.gid];
+                        for (int t = 0; t < 3; ++t) {
+                            tab[count * 9 + t] = cf.ca[t];
+                            tab[count * 9 + 3 + t] = cf.cb[t];
+                            tab[count * 9 + 6 + t] = key.dd[t];
+                        }
+                        ++count;
+                    }
+                    idp[(size_t(i - (i0 - 1)) * 16 + size_t(r + 1)) * TB_CW + size_t(cc + 1)] = vals[h];
+                }
+        if (over) on[size_t(c)] = 0;
+    }
+    // the rim: a tile with a one-step node (or the shell) within two nodes
+    auto is_on = [&](int sg, int q, int bx) {
+        if (sg < 0 || sg >= NS || q < 0 || q >= J) return false;
+        if (bx < 0 || bx >= kt) return true;   // past the grid's k ends: no node there
+        return on[flat(sg, q, bx)] != 0;
+    };
+    std::vector<size_t> cand_of_tb;
+    for (int sg = 0; sg < NS; ++sg)
+        for (int q = 0; q < J; ++q)
+            for (int bx = 0; bx < kt; ++bx) {
+                if (!on[flat(sg, q, bx)]) continue;
+                bool rim = false;
+                for (int ds = -1; ds <= 1 && !rim; ++ds)
+                    for (int dq = -1; dq <= 1 && !rim; ++dq)
+                        for (int db = -1; db <= 1 && !rim; ++db)
+                            if (!is_on(sg + ds, q + dq, bx + db)) rim = true;
+                const int k0 = cp.kbase + TB_TK * bx;
+                bool zl = false;
+                for (int k = std::max(k0 - 2, 0); k <= std::min(k0 + 65, g.n2 - 1); ++k)
+                    zl = zl || sim.ax[2].node[size_t(k)].slot_e >= 0 || sim.ax[2].node[size_t(k)].slot_h >= 0;
+                P.zblocks += zl;
+                P.rim += rim;
+                P.tb.push_back(make_int4(k0 | (zl ? TMA_ZL_TILE : 0) | (rim ? TB_RIM : 0), ja + TB_TJ * q, rsegs[sg].x,
+                                         rsegs[sg].y));
+                cand_of_tb.push_back(flat(sg, q, bx));
+            }
+    if (P.tb.empty()) { P.why = "no two-step tile"; return P; }
+    // keep the ids and tables of the tiles kept
+    {
+        std::vector<uint8_t> ids;
+        std::vector<float> tabs(P.tb.size() * LOCAL_CLASSES * 9);
+        size_t acc = 0;
+        for (size_t b = 0; b < P.tb.size(); ++b) {
+            const size_t c = cand_of_tb[b];
+            const size_t planes = size_t(P.tb[b].w - P.tb[b].z + 2);
+            P.idbase.push_back(int(acc));
+            ids.insert(ids.end(), P.ids.begin() + cand_idbase[c] * 16 * TB_CW,
+                       P.ids.begin() + (cand_idbase[c] + planes) * 16 * TB_CW);
+            std::memcpy(tabs.data() + b * LOCAL_CLASSES * 9, ctab.data() + c * LOCAL_CLASSES * 9, LOCAL_CLASSES * 9 * 4);
+            acc += planes;
+        }
+        P.ids.swap(ids);
+        P.tables.swap(tabs);
+    }
+    // one-step tiles of a double step: those of the one-step plan no two-step tile replaces
+    std::vector<int> seg_of(size_t(g.n0), -1);
+    for (int sg = 0; sg < NS; ++sg)
+        for (int i = rsegs[sg].x; i < rsegs[sg].y; ++i) seg_of[size_t(i)] = sg;
+    auto two_step = [&](int i, int j, int k) {   // node (i, j, k) belongs to a two-step tile
+        const int sg = seg_of[size_t(i)];
+        if (sg < 0 || j < ja || j >= ja + TB_TJ * J) return false;
+        int bx = (k - cp.kbase) / TB_TK;
+        if (bx >= kt) bx = kt - 1;   // the last tile's extra column
+        return bx >= 0 && on[flat(sg, (j - ja) / TB_TJ, bx)] != 0;
+    };
+    for (size_t b = 0; b < cp.blocks.size(); ++b) {
+        const int4 bk = cp.blocks[b];
+        const int k0 = bk.x & ~TMA_ZL_TILE;
+        if (cp.own[b].x >= cp.own[b].y || !two_step(bk.z, cp.own[b].x, std::max(k0, cp.kbase)))
+            P.cidx.push_back(int(b));
+    }
+    // Debye edges: one-step ones first; per device node its first edge
+    const size_t nnp = size_t(g.n0) * n1 * size_t(g.p2);
+    if (!perm.empty()) P.dbase.assign(nnp, 0u);
+    std::vector<size_t> first_c, first_r;
+    for (size_t e = 0; e < perm.size(); ++e) {
+        const auto& q = sim.debye_edges[perm[e]];
+        const int i = int(q.id / (n1 * n2)), j = int((q.id / n2) % n1), k = int(q.id % n2);
+        (two_step(i, j, k) ? first_r : first_c).push_back(e);
+    }
+    auto devid = [&](uint64_t id) { return (long long)(id / n2) * g.p2 + (long long)(id % n2); };
+    for (size_t e = 0; e < perm.size(); ++e) {
+        const uint64_t id = sim.debye_edges[perm[e]].id;
+        if (dfirst[id] == uint32_t(e)) P.dbase[size_t(devid(id))] = uint32_t(e);
+    }
+    for (auto* list : {&first_c, &first_r})
+        for (size_t e : *list) {
+            const auto& q = sim.debye_edges[perm[e]];
+            P.dd_f.push_back((long long)q.comp * g.cs + devid(q.id));
+            P.dd_s.push_back(uint32_t(e));
+            P.dd_w.push_back(float(q.dd));
+            P.dd_cb.push_back(sim.cb(q.comp, q.id));
+        }
+    P.dd_c = int(first_c.size());
+    P.ok = true;
+    return P;
+}
+
+bool encode_tb2_maps(Session& s, std::string& why) {
+    const Geom& g = s.geom;
+    float* E[3] = {s.e, s.e2, s.e3};
+    float* H[3] = {s.h, s.h2, s.h3};
+    const cuuint64_t dims[4] = {cuuint64_t(g.n2), cuuint64_t(g.n1), cuuint64_t(g.n0), 3};
+    const cuuint64_t strides[3] = {cuuint64_t(g.p2) * 4, cuuint64_t(g.n1) * g.p2 * 4, cuuint64_t(g.cs) * 4};
+    using L = Tb2Layout<3>;
+    const cuuint32_t box_e[4] = {cuuint32_t(L::EW), cuuint32_t(L::ER), 1, 3};
+    const cuuint32_t box_h[4] = {cuuint32_t(L::HW), cuuint32_t(L::HR), 1, 3};
+    const cuuint32_t box_e1[4] = {cuuint32_t(TmaL<float>::EW), cuuint32_t(TmaL<float>::ER), 1, 3};
+    const cuuint32_t box_h1[4] = {cuuint32_t(TmaL<float>::HW), cuuint32_t(TmaL<float>::HR), 1, 3};
+    const long long zlen = g.psi_off[1 * 3 + 2] - g.psi_off[0 * 3 + 2];
+    const cuuint64_t zd[4] = {cuuint64_t(g.pw), cuuint64_t(g.n1), cuuint64_t(g.n0), 2};
+    const cuuint64_t zs[3] = {cuuint64_t(g.pw) * 4, cuuint64_t(g.n1) * g.pw * 4, cuuint64_t(zlen) * 4};
+    const cuuint32_t zbh[4] = {cuuint32_t(g.pw), cuuint32_t(L::ZHR), 1, 2};
+    const cuuint32_t zbe[4] = {cuuint32_t(g.pw), cuuint32_t(L::ZER), 1, 2};
+    const cuuint32_t zb1[4] = {cuuint32_t(g.pw), cuuint32_t(TMA_TJ + 1), 1, 2};
+    for (int q = 0; q < 3; ++q) {
+        if (!encode(&s.tbm_e[q], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, E[q], 4, dims, strides, box_e, why)) return false;
+        if (!encode(&s.tbm_h[q], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, H[q], 4, dims, strides, box_h, why)) return false;
+        if (!encode(&s.d1_e[q], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, E[q], 4, dims, strides, box_e1, why)) return false;
+        if (!encode(&s.d1_h[q], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, H[q], 4, dims, strides, box_h1, why)) return false;
+        if (g.pml > 0) {
+            float* ze = s.zslot[q] + g.psi_off[0 * 3 + 2];
+            float* zh = s.zslot[q] + g.psi_off[9 + 0 * 3 + 2];
+            if (!encode(&s.tbm_zh[q], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, zh, 4, zd, zs, zbh, why)) return false;
+            if (!encode(&s.tbm_ze[q], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, ze, 4, zd, zs, zbe, why)) return false;
+            if (!encode(&s.d1_pze[q], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, ze, 4, zd, zs, zb1, why)) return false;
+            if (!encode(&s.d1_pzh[q], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, zh, 4, zd, zs, zb1, why)) return false;
+        } else {
+            s.tbm_zh[q] = s.tbm_ze[q] = s.d1_pze[q] = s.d1_pzh[q] = s.tma.c;   // never read without a CPML
+        }
+    }
+    const cuuint64_t cd[3] = {cuuint64_t(TB_CW), 16, cuuint64_t(s.tb_planes)};
+    const cuuint64_t cs2[2] = {cuuint64_t(TB_CW), cuuint64_t(16 * TB_CW)};
+    const cuuint32_t cb[3] = {cuuint32_t(TB_CW), 16, 1};
+    return encode(&s.tbm_c, CU_TENSOR_MAP_DATA_TYPE_UINT8, s.tb_ids, 3, cd, cs2, cb, why);
+}
+
+// The one-step march's launch over a block list, from set a to set b.
+void launch_tma_slots(Session& s, bool all, int a, int b, cudaStream_t st) {
+    float* E[3] = {s.e, s.e2, s.e3};
+    float* H[3] = {s.h, s.h2, s.h3};
+    TmaArgs args{s.geom, s.classes, E[b], H[b], s.sc.k_mu, s.clean_lo[2], s.clean_hi[1], s.clean_hi[2],
+                 all ? s.tma_blocks : s.c_blocks, all ? s.tma_own : s.c_own, 0, 1, s.zslot[b], s.zslot[b],
+                 all ? s.tables : s.c_tables, s.counter, s.error, s.wait_ns, s.stall_plane};
+    const unsigned nb = unsigned(all ? s.tma.blocks : s.n_cblocks);
+    with_tma_kernel(s.cid_bytes, s.local, s.tma.shape, [&](auto kern, int smem) {
+        kern<<<nb, TMA_CONSUMERS + 32, smem, st>>>(s.d1_e[a], s.d1_h[a], s.tma.c, s.d1_pze[a], s.d1_pzh[a], args);
+        return true;
+    });
+}
+
+// The per-step terms after the field update (sources and inductors, then the port probes), as
+// enqueue_step forms them.
+void enqueue_lumped(Session& s, float* e_now, float* h_now, cudaStream_t st) {
+    const Geom& g = s.geom;
+    const bool lumped = s.n_sources || s.n_inductors, probes = s.n_ports && !s.quiet;
+    if (lumped && probes && s.n_ports == 1) {
+        k_lumped_probe<<<1, 256, 0, st>>>(s.sources, s.n_sources, s.inductors, s.n_inductors, s.sc, s.counter, e_now,
+                                          s.probes, s.port_edges, s.loops, g.cs, h_now, s.series);
+    } else {
+        if (lumped) k_lumped<<<1, 256, 0, st>>>(s.sources, s.n_sources, s.inductors, s.n_inductors, s.sc, s.counter, e_now);
+        if (probes) k_probe<<<s.n_ports, 256, 0, st>>>(s.probes, s.port_edges, s.loops, g.cs, e_now, h_now, s.counter, s.sc, s.series);
+    }
+}
+
+// One step t -> t + 1 of the one-step kernels in the slot scheme: the march over all one-step
+// tiles (all) or over those left beside the two-step tiles, the shell, Debye, sources, probes.
+void enqueue_slot_one(Session& s, uint64_t t, bool all, cudaStream_t st,
+                      std::vector<std::pair<const char*, cudaEvent_t>>* marks, bool last = true) {
+    auto mark = [&](const char* name) {
+        if (!marks) return;
+        cudaEvent_t ev;
+        cudaEventCreate(&ev);
+        cudaEventRecord(ev, st);
+        marks->push_back({name, ev});
+    };
+    const Geom& g = s.geom;
+    const int a = int(t % 3), b = int((t + 1) % 3), par = int(t & 1);
+    float* E[3] = {s.e, s.e2, s.e3};
+    float* H[3] = {s.h, s.h2, s.h3};
+    mark(all ? "fused_step" : "edge_step");
+    launch_tma_slots(s, all, a, b, st);
+    const unsigned shell_rows = s.shell.ra + s.shell.rb + s.shell.rc;
+    if (shell_rows > 0) {
+        const unsigned gb = (shell_rows + SHELL_THREADS / 32 - 1) / (SHELL_THREADS / 32);
+        mark("shell_h");
+        k_shell_h<<<gb, SHELL_THREADS, 0, st>>>(g, s.shell, s.kax, E[a], H[a], H[b], par ? s.psi_h2 : s.psi,
+                                                par ? s.psi : s.psi_h2, s.zslot[a], s.zslot[b], s.sc.k_mu);
+        mark("shell_e");
+        switch (s.cid_bytes) {
+            case 1: k_shell_e<uint8_t><<<gb, SHELL_THREADS, 0, st>>>(g, s.shell, s.kax, (const uint8_t*)s.node_class, s.classes, H[b], E[a], E[b], s.psi, s.zslot[a], s.zslot[b]); break;
+            case 2: k_shell_e<uint16_t><<<gb, SHELL_THREADS, 0, st>>>(g, s.shell, s.kax, (const uint16_t*)s.node_class, s.classes, H[b], E[a], E[b], s.psi, s.zslot[a], s.zslot[b]); break;
+            default: k_shell_e<uint32_t><<<gb, SHELL_THREADS, 0, st>>>(g, s.shell, s.kax, (const uint32_t*)s.node_class, s.classes, H[b], E[a], E[b], s.psi, s.zslot[a], s.zslot[b]); break;
+        }
+    }
+    const int nd = all ? s.dd_all : s.dd_c;
+    if (nd > 0) {
+        mark("debye_post");
+        k_debye_slots<<<(nd + 255) / 256, 256, 0, st>>>(s.dd_f, s.dd_s, s.dd_w, s.dd_cb, nd, E[a], s.debye_table,
+                                                        s.dslot[a], s.dslot[b], E[b]);
+    }
+    if (s.n_sources || s.n_inductors || (s.n_ports && !s.quiet)) mark("lumped_probe");
+    enqueue_lumped(s, E[b], H[b], st);
+    if (last) mark(nullptr);
+}
+
+// Steps t -> t + 2: the two-step march over the interior tiles, beside (on the side stream when
+// `fork`) the first one-step update of the other tiles and the shell; then the second.
+void enqueue_slot_double(Session& s, uint64_t t, cudaStream_t st, bool fork,
+                         std::vector<std::pair<const char*, cudaEvent_t>>* marks) {
+    const int a = int(t % 3), b = int((t + 1) % 3), c = int((t + 2) % 3);
+    float* E[3] = {s.e, s.e2, s.e3};
+    float* H[3] = {s.h, s.h2, s.h3};
+    Tb2Args ta{s.geom, s.sc.k_mu, s.tb_blocks, s.tb_idbase, s.tb_tables, E[b], H[b], E[c], H[c], s.zslot[b],
+               s.zslot[b], s.zslot[c], s.zslot[c], s.dbase, s.dslot[a], s.dslot[b], s.dslot[c], s.debye_table,
+               s.error, s.wait_ns};
+    if (fork) {
+        cudaEventRecord(s.fork_ev, st);
+        cudaStreamWaitEvent(s.side, s.fork_ev, 0);
+        enqueue_slot_one(s, t, false, s.side, nullptr);
+        cudaEventRecord(s.join_ev, s.side);
+    }
+    if (marks) {
+        cudaEvent_t ev;
+        cudaEventCreate(&ev);
+        cudaEventRecord(ev, st);
+        marks->push_back({"two_step", ev});
+    }
+    k_tb2_step<3><<<unsigned(s.n_tb), TB_THREADS, s.tb_smem, st>>>(s.tbm_e[a], s.tbm_h[a], s.tbm_c, s.tbm_zh[a],
+                                                                   s.tbm_ze[a], ta);
+    if (fork) cudaStreamWaitEvent(st, s.join_ev, 0);
+    else enqueue_slot_one(s, t, false, st, marks, false);
+    enqueue_slot_one(s, t + 1, false, st, marks);
+}
+
+// The captured graph of `kind` (0: one step, 1: a double step, 2: 24 double steps) starting at a
+// step of the given phase (t mod 6), captured on first use.
+int slot_graph(Session& s, int kind, int phase, cudaGraphExec_t* out, std::string& err) {
+    const int key = kind * 8 + phase;
+    auto it = s.slot_graphs.find(key);
+    if (it != s.slot_graphs.end()) { *out = it->second; return FG_OK; }
+    FG_CUDA(cudaStreamSynchronize(s.stream));
+    cudaGraph_t graph;
+    FG_CUDA(cudaStreamBeginCapture(s.stream, cudaStreamCaptureModeThreadLocal));
+    if (kind == 0) enqueue_slot_one(s, uint64_t(phase), true, s.stream, nullptr);
+    else
+        for (int q = 0; q < (kind == 1 ? 1 : 24); ++q) enqueue_slot_double(s, uint64_t(phase + 2 * q), s.stream, true, nullptr);
+    cudaError_t ce = cudaStreamEndCapture(s.stream, &graph);
+    if (ce != cudaSuccess) { err = std::string("cudaStreamEndCapture: ") + cudaGetErrorString(ce); return FG_ERR_CUDA; }
+    cudaGraphExec_t ex;
+    ce = cudaGraphInstantiate(&ex, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ce != cudaSuccess) { err = std::string("cudaGraphInstantiate: ") + cudaGetErrorString(ce); return FG_ERR_CUDA; }
+    s.slot_graphs[key] = ex;
+    *out = ex;
+    return FG_OK;
+}
+
+// Device buffers, tensor maps and launch settings of the two-step mode.
+int setup_slots(Session& s, const HostSim& sim, const SlotPlan& sp, long long psi_total, std::string& err) {
+    const Geom& g = s.geom;
+    auto alloc = [&](void** p, size_t bytes) -> int {
+        FG_CUDA(cudaMalloc(p, std::max<size_t>(bytes, 256)));
+        s.extra_allocs.push_back(*p);
+        return FG_OK;
+    };
+    auto upload = [&](void* dst, const void* src, size_t bytes) -> int {
+        if (bytes) FG_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s.stream));
+        s.h2d_bytes += bytes;
+        return FG_OK;
+    };
+    const size_t fb = size_t(3 * g.cs) * 4;
+    const size_t np = std::max<size_t>(sim.poles.size(), 1);
+    const size_t ne = sp.dd_f.size();
+    const size_t pz = size_t(std::max<long long>(psi_total, 1)) * 4;
+    int rc = FG_OK;
+    rc |= alloc((void**)&s.e3, fb);
+    rc |= alloc((void**)&s.h3, fb);
+    for (int q = 0; q < 3; ++q) {
+        rc |= alloc((void**)&s.zslot[q], pz);
+        rc |= alloc((void**)&s.dslot[q], std::max<size_t>(ne * np, 1) * 4);
+    }
+    if (rc) return rc;
+    const size_t nnp = size_t(g.n0) * g.n1 * size_t(g.p2);
+    if (ne) {
+        rc |= alloc((void**)&s.dbase, nnp * 4);
+        rc |= alloc((void**)&s.dd_f, ne * 8);
+        rc |= alloc((void**)&s.dd_s, ne * 4);
+        rc |= alloc((void**)&s.dd_w, ne * 4);
+        rc |= alloc((void**)&s.dd_cb, ne * 4);
+    }
+    std::vector<int4> cb;
+    std::vector<int2> co;
+    std::vector<float> ct;
+    for (int b : sp.cidx) {
+        cb.push_back(sp.cp.blocks[size_t(b)]);
+        co.push_back(sp.cp.own[size_t(b)]);
+    }
+    // the one-step tiles' coefficient tables, in the order of the double step's list
+    std::vector<float> all_tables(size_t(s.tma.blocks) * LOCAL_CLASSES * 6);
+    FG_CUDA(cudaMemcpy(all_tables.data(), s.tables, all_tables.size() * 4, cudaMemcpyDeviceToHost));
+    for (int b : sp.cidx)
+        ct.insert(ct.end(), all_tables.begin() + size_t(b) * LOCAL_CLASSES * 6,
+                  all_tables.begin() + size_t(b + 1) * LOCAL_CLASSES * 6);
+    rc |= alloc((void**)&s.c_blocks, cb.size() * sizeof(int4));
+    rc |= alloc((void**)&s.c_own, co.size() * sizeof(int2));
+    rc |= alloc((void**)&s.c_tables, ct.size() * 4);
+    rc |= alloc((void**)&s.tb_blocks, sp.tb.size() * sizeof(int4));
+    rc |= alloc((void**)&s.tb_idbase, sp.idbase.size() * 4);
+    rc |= alloc((void**)&s.tb_ids, sp.ids.size());
+    rc |= alloc((void**)&s.tb_tables, sp.tables.size() * 4);
+    if (rc) return rc;
+    for (float* p : {s.e3, s.h3}) FG_CUDA(cudaMemsetAsync(p, 0, fb, s.stream));
+    for (int q = 0; q < 3; ++q) {
+        FG_CUDA(cudaMemsetAsync(s.zslot[q], 0, pz, s.stream));
+        FG_CUDA(cudaMemsetAsync(s.dslot[q], 0, std::max<size_t>(ne * np, 1) * 4, s.stream));
+    }
+    if (ne) {
+        rc |= upload(s.dbase, sp.dbase.data(), nnp * 4);
+        rc |= upload(s.dd_f, sp.dd_f.data(), ne * 8);
+        rc |= upload(s.dd_s, sp.dd_s.data(), ne * 4);
+        rc |= upload(s.dd_w, sp.dd_w.data(), ne * 4);
+        rc |= upload(s.dd_cb, sp.dd_cb.data(), ne * 4);
+    }
+    rc |= upload(s.c_blocks, cb.data(), cb.size() * sizeof(int4));
+    rc |= upload(s.c_own, co.data(), co.size() * sizeof(int2));
+    rc |= upload(s.c_tables, ct.data(), ct.size() * 4);
+    rc |= upload(s.tb_blocks, sp.tb.data(), sp.tb.size() * sizeof(int4));
+    rc |= upload(s.tb_idbase, sp.idbase.data(), sp.idbase.size() * 4);
+    rc |= upload(s.tb_ids, sp.ids.data(), sp.ids.size());
+    rc |= upload(s.tb_tables, sp.tables.data(), sp.tables.size() * 4);
+    if (rc) return rc;
+    FG_CUDA(cudaStreamSynchronize(s.stream));
+    s.n_cblocks = int(cb.size());
+    s.n_tb = int(sp.tb.size());
+    s.tb_zblocks = sp.zblocks;
+    s.tb_rim = sp.rim;
+    s.dd_c = sp.dd_c;
+    s.dd_all = int(ne);
+    s.tb_planes = sp.ids.size() / (16 * TB_CW);
+    // every tile's boxes and halo stay inside the grid and its buffers: origins along k on 16 bytes
+    // (k0 - 4 floats, k0 a multiple of 8), planes i0 - 2 .. i1 + 1 and rows j0 - 2 .. j0 + 15 inside,
+    // its class planes inside the id array, the z-slab rows inside the staged pitch
+    if (g.pw > TB_PZW || sim.poles.size() > size_t(TB_NPMAX) || s.n_cblocks == 0) {
+        err = "internal: two-step limits";
+        return FG_ERR_INVALID;
+    }
+    for (size_t b = 0; b < sp.tb.size(); ++b) {
+        const int4 t = sp.tb[b];
+        const int k0 = t.x & ~(TMA_ZL_TILE | TB_RIM);
+        const bool okb = k0 % 8 == 0 && k0 >= 0 && k0 < g.n2 && t.z >= 2 && t.w + 2 <= g.n0 && t.w > t.z &&
+                         t.w - t.z <= TB_SEGMAX && t.y >= 2 && t.y + 16 <= g.n1 &&
+                         size_t(sp.idbase[b]) + size_t(t.w - t.z + 2) <= s.tb_planes;
+        if (!okb) { err = "internal: a two-step tile outside its limits"; return FG_ERR_INVALID; }
+    }
+    for (unsigned q : sp.dd_s)
+        if (size_t(q) >= ne) { err = "internal: a Debye state index outside the state"; return FG_ERR_INVALID; }
+    std::string why;
+    if (!encode_tb2_maps(s, why)) { err = "two-step march: " + why; return FG_ERR_CUDA; }
+    s.tb_smem = Tb2Layout<3>::TOTAL;
+    FG_CUDA(cudaFuncSetAttribute(k_tb2_step<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, s.tb_smem));
+    FG_CUDA(cudaStreamCreateWithFlags(&s.side, cudaStreamNonBlocking));
+    FG_CUDA(cudaEventCreateWithFlags(&s.fork_ev, cudaEventDisableTiming));
+    FG_CUDA(cudaEventCreateWithFlags(&s.join_ev, cudaEventDisableTiming));
+    s.slots = true;
     return FG_OK;
 }
 
@@ -677,6 +1241,13 @@ int session_new(Gpu* gpu, const HostSim& sim, const RunSpec& rs, Session** out, 
         debye_table.push_back(float((1.0 - 0.5 * x * sim.dt) / d));
         debye_table.push_back(float(EPS0 * a * x / d));
     }
+    // nodes with per-step terms of their own (a two-step tile's halo must not reach them)
+    std::vector<uint64_t> special;
+    for (auto& q : sim.port_src[rs.driven]) special.push_back(q.id);
+    for (auto& q : sim.inductors) special.push_back(q.id);
+    for (auto& p : sim.ports)
+        for (auto& col : p.columns)
+            for (auto& e : col) special.push_back(sim.idx(e.at[0], e.at[1], e.at[2]));
     std::vector<DevProbe> probes;
     std::vector<DevPortEdge> pedges;
     std::vector<DevLoop> loops;
@@ -714,6 +1285,7 @@ int session_new(Gpu* gpu, const HostSim& sim, const RunSpec& rs, Session** out, 
             for (auto& [kc, t] : turns) {
                 if (t == 0) continue;
                 const size_t id = kc.first;
+                special.push_back(uint64_t(id));
                 const int comp = kc.second;
                 const size_t pc = comp == 0 ? id / (n1 * n2) : (comp == 1 ? (id / n2) % n1 : id % n2);
                 const double w = double(t) * sim.ax[comp].dd[pc];
@@ -789,8 +1361,20 @@ int session_new(Gpu* gpu, const HostSim& sim, const RunSpec& rs, Session** out, 
     // per-region class tables for the TMA step (fused runs on sm_100)
     LocalClasses lc;
     CleanPlan cp;
+    SlotPlan sp;
+    const bool z_layer = g.pml > 0 && g.pw <= TmaL<float>::PZW;
     if (s->fused && rs.tma && !(std::getenv("FIELDGRID_NO_TMA") && std::getenv("FIELDGRID_NO_TMA")[0] == '1')) {
-        cp = plan_clean(sim, g, g.pml > 0 && g.pw <= TmaL<float>::PZW, rs.tma_seg);
+        // the two-step mode: graph-stepped fused runs with no wires, sheets, NTFF, plane DFT, design
+        // history, and at most TB_NPMAX Debye poles, on sm_100 (FIELDGRID_STEP_DEPTH=1 turns it off)
+        int dev = 0, major = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev);
+        const char* dv = std::getenv("FIELDGRID_STEP_DEPTH");
+        const bool want = rs.graphs && major >= 10 && !(dv && dv[0] == '1') && s->n_wires == 0 && s->n_sheets == 0 &&
+                          s->plane_len == 0 && s->ntff_len == 0 && !(rs.design && !rs.design->empty()) &&
+                          sim.poles.size() <= size_t(TB_NPMAX) && (g.pml == 0 || z_layer);
+        if (want) sp = plan_slots(sim, g, z_layer, special);
+        cp = sp.ok ? sp.cp : plan_clean(sim, g, z_layer, rs.tma_seg);
         if (cp.ok) {
             lc = build_local(sim, g, cp);
             s->local = lc.ok;
@@ -831,6 +1415,7 @@ int session_new(Gpu* gpu, const HostSim& sim, const RunSpec& rs, Session** out, 
     need += carve_size(64);
     if (s->local) need += carve_size(lc.ids.size()) + carve_size(lc.tables.size() * 4);
     need += carve_size(cp.blocks.size() * sizeof(int4));
+    need += carve_size(cp.own.size() * sizeof(int2));
     size_t free_b = 0, total_b = 0;
     FG_CUDA(cudaMemGetInfo(&free_b, &total_b));
     if (need + (size_t(256) << 20) > free_b) {
@@ -887,6 +1472,7 @@ int session_new(Gpu* gpu, const HostSim& sim, const RunSpec& rs, Session** out, 
         s->tables = carve<float>(cur, lc.tables.size());
     }
     if (!cp.blocks.empty()) s->tma_blocks = carve<int4>(cur, cp.blocks.size());
+    if (!cp.own.empty()) s->tma_own = carve<int2>(cur, cp.own.size());
     s->tma_plan_blocks = cp.blocks;
     s->tma.blocks = int(cp.blocks.size());
     s->tma.zblocks = cp.zblocks;
@@ -977,6 +1563,7 @@ int session_new(Gpu* gpu, const HostSim& sim, const RunSpec& rs, Session** out, 
         rc |= up(s->tables, lc.tables.data(), lc.tables.size() * 4);
     }
     if (!cp.blocks.empty()) rc |= up(s->tma_blocks, cp.blocks.data(), cp.blocks.size() * sizeof(int4));
+    if (!cp.own.empty()) rc |= up(s->tma_own, cp.own.data(), cp.own.size() * sizeof(int2));
     rc |= up(d_dft, t_dft.data(), t_dft.size() * 4);
     rc |= up(d_far, t_far.data(), t_far.size() * 4);
     if (rc) return FG_ERR_CUDA;
@@ -1001,7 +1588,17 @@ int session_new(Gpu* gpu, const HostSim& sim, const RunSpec& rs, Session** out, 
                                                                                tma::WAIT_LIMIT_MIN_NS), tma::WAIT_LIMIT_NS);
     if (const char* v = std::getenv("FIELDGRID_TEST_STALL_PLANE")) s->stall_plane = std::atoi(v);
     plan_tma(*s);
-    if (s->tma.ok)
+    if (sp.ok && s->tma.ok && s->local) {
+        rc = setup_slots(*s, sim, sp, psi_total, err);
+        if (rc) { session_free(s.release()); return rc; }
+    }
+    if (s->slots)
+        s->variant = "two-step march over " + std::to_string(s->n_tb) + " tiles of 14x64 (" + std::to_string(s->tb_zblocks) +
+                     " reaching the k layer, " + std::to_string(s->tb_rim) + " at the rim) beside the one-step TMA march on " +
+                     std::to_string(s->n_cblocks) + " tiles of 7x64 and a CPML shell of " +
+                     std::to_string(s->shell.ra + s->shell.rb + s->shell.rc) + " rows, " +
+                     std::to_string(s->dd_all) + " Debye edges in time slots";
+    else if (s->tma.ok)
         s->variant = "TMA fused march, tile " + std::to_string(s->tma.tj) + "x" + std::to_string(s->tma.tk) + ", " +
                      std::to_string(s->tma.seg) + " planes per block, " + std::to_string(s->tma.blocks) +
                      " blocks on the clean box (" + std::to_string(s->tma.zblocks) + " reaching the k layer), CPML shell of " +
@@ -1015,7 +1612,16 @@ int session_new(Gpu* gpu, const HostSim& sim, const RunSpec& rs, Session** out, 
     s->n_poles = int(sim.poles.size());
     s->currents_len = sheets.size() * nr_nc;
     s->ind_host = ind;
-    if (!rs.graphs) {
+    if (s->slots) {
+        // single and double steps of every phase now; the 48-step graphs on first use
+        for (int kind = 0; kind < 2 && !rc; ++kind)
+            for (int ph = 0; ph < 6 && !rc; ++ph) {
+                cudaGraphExec_t gx;
+                rc = slot_graph(*s, kind, ph, &gx, err);
+            }
+        if (rc) { session_free(s.release()); return rc; }
+    }
+    if (!rs.graphs || s->slots) {
         *out = s.release();
         return FG_OK;
     }
@@ -1038,6 +1644,11 @@ void session_free(Session* s) {
     if (s->graph_two) cudaGraphExecDestroy(s->graph_two);
     for (auto& gx : s->graph_one)
         if (gx) cudaGraphExecDestroy(gx);
+    for (auto& kv : s->slot_graphs) cudaGraphExecDestroy(kv.second);
+    for (void* p : s->extra_allocs) cudaFree(p);
+    if (s->side) cudaStreamDestroy(s->side);
+    if (s->fork_ev) cudaEventDestroy(s->fork_ev);
+    if (s->join_ev) cudaEventDestroy(s->join_ev);
     if (s->arena) cudaFree(s->arena);
     cudaFree(s->design);
     cudaFree(s->hist_e);
@@ -1053,8 +1664,13 @@ int session_reset(Session* s, std::string& err) {
     FG_CUDA(cudaSetDevice(s->gpu->device));
     cudaStream_t st = s->stream;
     const size_t fb = size_t(3 * s->geom.cs) * 4;
-    for (float* p : {s->e, s->h, s->e2, s->h2})
+    for (float* p : {s->e, s->h, s->e2, s->h2, s->e3, s->h3})
         if (p) FG_CUDA(cudaMemsetAsync(p, 0, fb, st));
+    if (s->slots)
+        for (int q = 0; q < 3; ++q) {
+            FG_CUDA(cudaMemsetAsync(s->zslot[q], 0, size_t(std::max<long long>(s->psi_total, 1)) * 4, st));
+            FG_CUDA(cudaMemsetAsync(s->dslot[q], 0, std::max<size_t>(size_t(s->dd_all) * size_t(std::max(s->n_poles, 1)), 1) * 4, st));
+        }
     FG_CUDA(cudaMemsetAsync(s->psi, 0, size_t(std::max<long long>(s->psi_total, 1)) * 4, st));
     if (s->fused && s->psi_total > s->psi_hbase)
         FG_CUDA(cudaMemsetAsync(s->psi_h2 + s->psi_hbase, 0, size_t(s->psi_total - s->psi_hbase) * 4, st));
@@ -1079,6 +1695,22 @@ int session_step(Session* s, uint64_t k, std::string& err) {
     if (!s->graph_many && !s->graph_one[0]) { err = "this session steps only as part of a batch"; return FG_ERR_INVALID; }
     FG_CUDA(cudaSetDevice(s->gpu->device));
     uint64_t done = 0;
+    if (s->slots) {
+        // 48 steps (24 double steps) keep the phase t mod 6 of the sets, slots and parity
+        while (done < k) {
+            const uint64_t left = k - done;
+            const int kind = left >= 48 ? 2 : (left >= 2 ? 1 : 0);
+            cudaGraphExec_t gx;
+            int rc = slot_graph(*s, kind, int(s->steps % 6), &gx, err);
+            if (rc) return rc;
+            FG_CUDA(cudaGraphLaunch(gx, s->stream));
+            const uint64_t n = kind == 2 ? 48 : (kind == 1 ? 2 : 1);
+            done += n;
+            s->steps += n;
+        }
+        FG_CUDA(cudaGetLastError());
+        return FG_OK;
+    }
     // the fused step alternates buffers: a whole graph block needs an even start
     while (done < k) {
         const uint64_t left = k - done;
@@ -1109,6 +1741,13 @@ int session_sync(Session* s, std::string& err) {
 
 // The buffers that hold the latest fields: after an odd number of fused steps, the second set.
 static void latest(const Session* s, float** e, float** h) {
+    if (s->slots) {
+        float* E[3] = {s->e, s->e2, s->e3};
+        float* H[3] = {s->h, s->h2, s->h3};
+        *e = E[s->steps % 3];
+        *h = H[s->steps % 3];
+        return;
+    }
     if (s->fused && (s->steps & 1)) { *e = s->e2; *h = s->h2; }
     else { *e = s->e; *h = s->h; }
 }
@@ -1205,13 +1844,19 @@ int session_kernel_times(Session* s, uint64_t steps, std::vector<std::pair<std::
     std::vector<std::pair<const char*, cudaEvent_t>> marks;
     std::vector<std::pair<std::string, double>> sums;
     std::vector<int> counts;
-    for (uint64_t q = 0; q < steps; ++q) {
+    // the two-step mode times double steps (one stream) and reports each kernel's time per step
+    const uint64_t per = s->slots ? 2 : 1;
+    for (uint64_t q = 0; q < steps; q += per) {
         marks.clear();
-        s->marks = &marks;
-        int rc = enqueue_step(*s, s->fused ? int(s->steps & 1) : 0, err);
-        s->marks = nullptr;
-        if (rc) return rc;
-        s->steps += 1;
+        if (s->slots) {
+            enqueue_slot_double(*s, s->steps, s->stream, false, &marks);
+        } else {
+            s->marks = &marks;
+            int rc = enqueue_step(*s, s->fused ? int(s->steps & 1) : 0, err);
+            s->marks = nullptr;
+            if (rc) return rc;
+        }
+        s->steps += per;
         FG_CUDA(cudaStreamSynchronize(s->stream));
         for (size_t m = 0; m + 1 < marks.size(); ++m) {
             float ms = 0.f;
@@ -1223,7 +1868,13 @@ int session_kernel_times(Session* s, uint64_t steps, std::vector<std::pair<std::
         for (auto& mk : marks) cudaEventDestroy(mk.second);
     }
     out.clear();
-    for (size_t m = 0; m < sums.size(); ++m) out.push_back({sums[m].first, sums[m].second / std::max(counts[m], 1)});
+    for (size_t m = 0; m < sums.size(); ++m) {
+        const double ms = sums[m].second / std::max(counts[m], 1) / double(per);
+        bool merged = false;   // a kernel that runs twice in a double step: its two launches summed
+        for (auto& o : out)
+            if (o.first == sums[m].first) { o.second += ms; merged = true; }
+        if (!merged) out.push_back({sums[m].first, ms});
+    }
     FG_CUDA(cudaGetLastError());
     return FG_OK;
 }

@@ -206,6 +206,29 @@ __global__ void k_debye_post_cb(const long long* __restrict__ f, const float* __
 }
 
 
+// The Debye ADE of k_debye_post_cb for edges whose pole state lives in time slots: edge q's state
+// is s_in[sidx[q] * np + k] before the step and s_out[...] after it (the steps of the two-step mode
+// keep three slots, so no kernel reads a state another has already advanced).
+__global__ void k_debye_slots(const long long* __restrict__ f, const unsigned* __restrict__ sidx,
+                              const float* __restrict__ dd, const float* __restrict__ cbq, int count,
+                              const float* __restrict__ eold, const float* __restrict__ table,
+                              const float* __restrict__ s_in, float* __restrict__ s_out, float* __restrict__ e) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= count) return;
+    const long long fi = f[q];
+    const float cb = cbq[q];
+    const float old = eold[fi];
+    const int np = int(table[0]);
+    const size_t b = size_t(sidx[q]) * size_t(np);
+    float s0 = 0.0f;
+    for (int k = 0; k < np; ++k) s0 += 0.5f * (1.0f + table[1 + 2 * k]) * s_in[b + k];
+    const float next = e[fi] - cb * s0;
+    e[fi] = next;
+    const float de = next - old;
+    const float w = dd[q];
+    for (int k = 0; k < np; ++k) s_out[b + k] = table[1 + 2 * k] * s_in[b + k] + w * table[2 + 2 * k] * de;
+}
+
 // cpu.rs:262-265
 __device__ __forceinline__ float pulse_at(const StepConst& sc, float t) {
     float x = (t - sc.t0) / sc.tau;

@@ -5,7 +5,10 @@
 // cpu.rs:48-167), as in the other pipelines:
 //   k_shell_h: H_out from E_in, H_in and the input set of H psi slabs (written to the output set);
 //   k_shell_e: E_out from E_in and the new H (the clean box's H written by the march, the shell's
-//              by k_shell_h), with the E psi slabs updated in place.
+//              by k_shell_h), with the E psi slabs along x and y updated in place.
+// The z slabs (derivative along k) are read from pz_in and written to pz_out, which are the psi
+// arrays themselves (in place for E, the two H sets) or, when the step keeps its z-slab psi in
+// time slots, the slot of the step's input and the slot of its output.
 // Run order within a step: the march and k_shell_h (independent), then k_shell_e.
 #pragma once
 
@@ -88,6 +91,7 @@ constexpr int SHELL_THREADS = 256;   // 8 rows per block
 __global__ void __launch_bounds__(SHELL_THREADS, 4) k_shell_h(Geom g, ShellRows b, KAxis kx, const float* __restrict__ e_in,
                                                            const float* __restrict__ h_in, float* __restrict__ h_out,
                                                            const float* __restrict__ psi_in, float* __restrict__ psi_out,
+                                                           const float* __restrict__ pz_in, float* __restrict__ pz_out,
                                                            float k_mu) {
     const unsigned r = blockIdx.x * (SHELL_THREADS / 32) + (threadIdx.x >> 5);
     if (r >= b.ra + b.rb + b.rc) return;
@@ -120,20 +124,20 @@ __global__ void __launch_bounds__(SHELL_THREADS, 4) k_shell_h(Geom g, ShellRows 
         const long long o1k = g.psi_off[9 + 1 * 3 + 2] + pz + ak.slot, o1i = g.psi_off[9 + 1 * 3 + 0] + px + k;
         const long long o2i = g.psi_off[9 + 2 * 3 + 0] + px + k, o2j = g.psi_off[9 + 2 * 3 + 1] + py + k;
         const bool lj = aj.slot_h >= 0, lk = ak.slot >= 0, li = ai.slot_h >= 0;
-        const float s0j = run0 && lj ? psi_in[o0j] : 0.f, s0k = run0 && lk ? psi_in[o0k] : 0.f;
-        const float s1k = run1 && lk ? psi_in[o1k] : 0.f, s1i = run1 && li ? psi_in[o1i] : 0.f;
+        const float s0j = run0 && lj ? psi_in[o0j] : 0.f, s0k = run0 && lk ? pz_in[o0k] : 0.f;
+        const float s1k = run1 && lk ? pz_in[o1k] : 0.f, s1i = run1 && li ? psi_in[o1i] : 0.f;
         const float s2i = run2 && li ? psi_in[o2i] : 0.f, s2j = run2 && lj ? psi_in[o2j] : 0.f;
         if (run0) {   // Hx: U = j, V = k
             const float ev = ez_j - ez, eu = ey_k - ey;
             float t1 = ev * aj.inv_d, t2 = eu * ak.inv;
             if (lj) { const float rr = cpml_term(aj.bh, s0j, aj.ch, ev, aj.raw_inv_d); psi_out[o0j] = rr; t1 += rr; }
-            if (lk) { const float rr = cpml_term(ak.b, s0k, ak.c, eu, ak.raw); psi_out[o0k] = rr; t2 += rr; }
+            if (lk) { const float rr = cpml_term(ak.b, s0k, ak.c, eu, ak.raw); pz_out[o0k] = rr; t2 += rr; }
             hx = hx - k_mu * (t1 - t2);
         }
         if (run1) {   // Hy: U = k, V = i
             const float ev = ex_k - ex, eu = ez_i - ez;
             float t1 = ev * ak.inv, t2 = eu * ai.inv_d;
-            if (lk) { const float rr = cpml_term(ak.b, s1k, ak.c, ev, ak.raw); psi_out[o1k] = rr; t1 += rr; }
+            if (lk) { const float rr = cpml_term(ak.b, s1k, ak.c, ev, ak.raw); pz_out[o1k] = rr; t1 += rr; }
             if (li) { const float rr = cpml_term(ai.bh, s1i, ai.ch, eu, ai.raw_inv_d); psi_out[o1i] = rr; t2 += rr; }
             hy = hy - k_mu * (t1 - t2);
         }
@@ -157,7 +161,8 @@ template <typename CID>
 __global__ void __launch_bounds__(SHELL_THREADS) k_shell_e(Geom g, ShellRows b, KAxis kx, const CID* __restrict__ node_class,
                                                            const DevCoef* __restrict__ classes,
                                                            const float* __restrict__ h, const float* __restrict__ e_in,
-                                                           float* __restrict__ e_out, float* __restrict__ psi) {
+                                                           float* __restrict__ e_out, float* __restrict__ psi,
+                                                           const float* pz_in, float* pz_out) {
     const unsigned r = blockIdx.x * (SHELL_THREADS / 32) + (threadIdx.x >> 5);
     if (r >= b.ra + b.rb + b.rc) return;
     int i, j;
@@ -188,20 +193,20 @@ __global__ void __launch_bounds__(SHELL_THREADS) k_shell_e(Geom g, ShellRows b, 
         const long long o1k = g.psi_off[1 * 3 + 2] + pz + ak.slot, o1i = g.psi_off[1 * 3 + 0] + px + k;
         const long long o2i = g.psi_off[2 * 3 + 0] + px + k, o2j = g.psi_off[2 * 3 + 1] + py + k;
         const bool lj = aj.slot_e >= 0, lk = ak.slot >= 0, li = ai.slot_e >= 0;
-        const float s0j = run0 && lj ? psi[o0j] : 0.f, s0k = run0 && lk ? psi[o0k] : 0.f;
-        const float s1k = run1 && lk ? psi[o1k] : 0.f, s1i = run1 && li ? psi[o1i] : 0.f;
+        const float s0j = run0 && lj ? psi[o0j] : 0.f, s0k = run0 && lk ? pz_in[o0k] : 0.f;
+        const float s1k = run1 && lk ? pz_in[o1k] : 0.f, s1i = run1 && li ? psi[o1i] : 0.f;
         const float s2i = run2 && li ? psi[o2i] : 0.f, s2j = run2 && lj ? psi[o2j] : 0.f;
         if (run0) {   // Ex: U = j, V = k
             const float hv = hz - hz_j, hu = hy - hy_k;
             float t1 = hv * aj.inv_dd, t2 = hu * ak.inv;
             if (lj) { const float rr = cpml_term(aj.be, s0j, aj.ce, hv, aj.raw_inv_dd); psi[o0j] = rr; t1 += rr; }
-            if (lk) { const float rr = cpml_term(ak.b, s0k, ak.c, hu, ak.raw); psi[o0k] = rr; t2 += rr; }
+            if (lk) { const float rr = cpml_term(ak.b, s0k, ak.c, hu, ak.raw); pz_out[o0k] = rr; t2 += rr; }
             ex = cf.ca[0] * ex + cf.cb[0] * (t1 - t2);
         }
         if (run1) {   // Ey: U = k, V = i
             const float hv = hx - hx_k, hu = hz - hz_i;
             float t1 = hv * ak.inv, t2 = hu * ai.inv_dd;
-            if (lk) { const float rr = cpml_term(ak.b, s1k, ak.c, hv, ak.raw); psi[o1k] = rr; t1 += rr; }
+            if (lk) { const float rr = cpml_term(ak.b, s1k, ak.c, hv, ak.raw); pz_out[o1k] = rr; t1 += rr; }
             if (li) { const float rr = cpml_term(ai.be, s1i, ai.ce, hu, ai.raw_inv_dd); psi[o1i] = rr; t2 += rr; }
             ey = cf.ca[1] * ey + cf.cb[1] * (t1 - t2);
         }

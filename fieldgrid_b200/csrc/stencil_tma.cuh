@@ -142,6 +142,7 @@ struct TmaArgs {
     float k_mu;
     int kbeg, jend, kend;                // the clean box: rows < jend, columns kbeg .. kend-1 are owned
     const int4* blocks;                  // per block: (k0, j0, i0, i1) of its tile and x-segment
+    const int2* own_rows;                // per block: the rows [x, y) it writes; null: [j0, jend)
     int block0;                          // this launch's first entry of `blocks`
     int bump;                            // this launch opens the step (raises the step counter)
     float* psi_e;                        // ZL: the E psi slabs (z slabs updated in place)
@@ -356,7 +357,8 @@ __device__ __forceinline__ void tma_march(const CUtensorMap& map_e, const CUtens
     const int jj = j0 + r, kk = k0 + c;
     const bool row_live = jj >= 0 && jj < g.n1;
     const bool live0 = row_live && kk < g.n2, live1 = row_live && kk + 1 < g.n2;
-    const bool own_row = r >= 0 && jj < a.jend && kk >= a.kbeg && kk < a.kend;   // the pair is written
+    const int2 orow = a.own_rows ? a.own_rows[bid] : make_int2(j0, a.jend);
+    const bool own_row = r >= 0 && jj >= orow.x && jj < orow.y && kk >= a.kbeg && kk < a.kend;   // the pair is written
     const AxisNode* rj = axj + (r + 1);
     const PtAxes q0{rj, axk + (c + 1), jj + 1 < g.n1, kk + 1 < g.n2};
     const PtAxes q1{rj, axk + (c + 2), jj + 1 < g.n1, kk + 2 < g.n2};
@@ -368,7 +370,7 @@ __device__ __forceinline__ void tma_march(const CUtensorMap& map_e, const CUtens
     const int xc = lane < TJ ? -1 : TK;                                   // column of the extra point
     const bool xtra = w == 0 && ((lane < TJ && k0 > 0) || (lane >= TJ && lane <= 2 * TJ && redge)) &&
                       j0 + xr >= 0 && j0 + xr < g.n1;
-    const bool xown = xtra && lane >= TJ && lane < 2 * TJ && j0 + xr < a.jend;  // right-edge points are owned
+    const bool xown = xtra && lane >= TJ && lane < 2 * TJ && j0 + xr >= orow.x && j0 + xr < orow.y;  // right-edge points are owned
     const int xj = j0 + xr, xk = k0 + xc;
     const PtAxes qx{axj + (xr + 1), axk + (xc + 1), xj + 1 < g.n1, xk + 1 < g.n2};
     const int xeo = (xr + 1) * L::EW + xc + 4, xho = (xr + 1) * L::HW + xc + 4, xno = (xr + 1) * L::NW + xc + 2;

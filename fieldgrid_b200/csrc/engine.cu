@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -1149,7 +1150,27 @@ int setup_slots(Session& s, const HostSim& sim, const SlotPlan& sp, long long ps
 
 }  // namespace
 
+// Wall-clock phases of session_new, printed to stderr when FIELDGRID_SETUP_TIMES=1.
+struct PhaseClock {
+    bool on = false;
+    std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now(), last = t0;
+    std::string text;
+    PhaseClock() { const char* v = std::getenv("FIELDGRID_SETUP_TIMES"); on = v && v[0] == '1'; }
+    void mark(const char* what) {
+        if (!on) return;
+        const auto now = std::chrono::steady_clock::now();
+        text += std::string(" ") + what + " " +
+                std::to_string(std::chrono::duration<double, std::milli>(now - last).count()).substr(0, 6) + " ms;";
+        last = now;
+    }
+    ~PhaseClock() {
+        if (on) std::fprintf(stderr, "session_new:%s total %.1f ms\n", text.c_str(),
+                             std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count());
+    }
+};
+
 int session_new(Gpu* gpu, const HostSim& sim, const RunSpec& rs, Session** out, std::string& err) {
+    PhaseClock clk;
     *out = nullptr;
     if (!gpu) { err = "no GPU: this engine has no CPU path"; return FG_ERR_NO_DEVICE; }
     FG_CUDA(cudaSetDevice(gpu->device));
@@ -1303,6 +1324,7 @@ int session_new(Gpu* gpu, const HostSim& sim, const RunSpec& rs, Session** out, 
                     return FG_ERR_PORT_INDEX;
                 }
 
+    clk.mark("lists");
     pulse_shape(rs.fc, s->t0, s->tau);
     StepConst& sc = s->sc;
     sc.k_mu = float(sim.dt / MU0);
@@ -1358,6 +1380,7 @@ int session_new(Gpu* gpu, const HostSim& sim, const RunSpec& rs, Session** out, 
     const size_t nr_nc = sim.sheet_table.size() >= 2 ? size_t(sim.sheet_table[0]) + 2 * size_t(sim.sheet_table[1]) : 0;
     (void)states;
 
+    clk.mark("tables");
     // per-region class tables for the TMA step (fused runs on sm_100)
     LocalClasses lc;
     CleanPlan cp;
@@ -1380,6 +1403,7 @@ int session_new(Gpu* gpu, const HostSim& sim, const RunSpec& rs, Session** out, 
             s->local = lc.ok;
         }
     }
+    clk.mark("plans");
     // size the arena
     const size_t fields = size_t(3 * cs);
     size_t need = 0;
@@ -1482,6 +1506,7 @@ int session_new(Gpu* gpu, const HostSim& sim, const RunSpec& rs, Session** out, 
     if (size_t(cur - s->arena) > need) { err = "internal: arena overflow"; return FG_ERR_INVALID; }
 
     cudaStream_t st = s->stream;
+    clk.mark("alloc");
     FG_CUDA(cudaMemsetAsync(s->arena, 0, need, st));
     // node classes, narrowed and laid out with the row pitch on the host in parallel
     {
@@ -1569,6 +1594,7 @@ int session_new(Gpu* gpu, const HostSim& sim, const RunSpec& rs, Session** out, 
     if (rc) return FG_ERR_CUDA;
     FG_CUDA(cudaStreamSynchronize(st));
 
+    clk.mark("upload");
     if (rs.design && !rs.design->empty()) {
         if (!s->fused) { err = "design recording needs the fused step"; return FG_ERR_INVALID; }
         s->n_design = int(rs.design->size());
@@ -1588,6 +1614,7 @@ int session_new(Gpu* gpu, const HostSim& sim, const RunSpec& rs, Session** out, 
                                                                                tma::WAIT_LIMIT_MIN_NS), tma::WAIT_LIMIT_NS);
     if (const char* v = std::getenv("FIELDGRID_TEST_STALL_PLANE")) s->stall_plane = std::atoi(v);
     plan_tma(*s);
+    clk.mark("tma_maps");
     if (sp.ok && s->tma.ok && s->local) {
         rc = setup_slots(*s, sim, sp, psi_total, err);
         if (rc) { session_free(s.release()); return rc; }
@@ -1612,6 +1639,7 @@ int session_new(Gpu* gpu, const HostSim& sim, const RunSpec& rs, Session** out, 
     s->n_poles = int(sim.poles.size());
     s->currents_len = sheets.size() * nr_nc;
     s->ind_host = ind;
+    clk.mark("slots");
     if (s->slots) {
         // single and double steps of every phase now; the 48-step graphs on first use
         for (int kind = 0; kind < 2 && !rc; ++kind)
@@ -1621,6 +1649,7 @@ int session_new(Gpu* gpu, const HostSim& sim, const RunSpec& rs, Session** out, 
             }
         if (rc) { session_free(s.release()); return rc; }
     }
+    clk.mark("graphs_slots");
     if (!rs.graphs || s->slots) {
         *out = s.release();
         return FG_OK;
@@ -1692,7 +1721,7 @@ int session_reset(Session* s, std::string& err) {
 }
 
 int session_step(Session* s, uint64_t k, std::string& err) {
-    if (!s->graph_many && !s->graph_one[0]) { err = "this session steps only as part of a batch"; return FG_ERR_INVALID; }
+    if (!s->slots && !s->graph_many && !s->graph_one[0]) { err = "this session steps only as part of a batch"; return FG_ERR_INVALID; }
     FG_CUDA(cudaSetDevice(s->gpu->device));
     uint64_t done = 0;
     if (s->slots) {

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <parallel/algorithm>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -187,6 +188,9 @@ struct Session {
 };
 
 static constexpr int ENERGY_BLOCKS = 1024;
+// Steps per sweep when FIELDGRID_STEP_DEPTH (1 or 2) does not say: 2 runs the two-step march where
+// a Sim qualifies for it.
+static constexpr int STEP_DEPTH_DEFAULT = 1;
 
 namespace {
 
@@ -656,7 +660,7 @@ struct SlotPlan {
     std::vector<int4> tb;               // two-step tiles: k0 | TMA_ZL_TILE | TB_RIM, j0, i0, i1
     std::vector<int> idbase;            // per two-step tile: its first plane in `ids`
     std::vector<uint8_t> ids;           // block-major class ids: [plane][16 rows][TB_CW columns]
-    std::vector<float> tables;          // per two-step tile: LOCAL_CLASSES x (ca[3], cb[3], dd[3])
+    std::vector<float> tables;          // per two-step tile: LOCAL_CLASSES records of TB_REC floats
     std::vector<int> cidx;              // one-step tiles of a double step (indices into cp.blocks)
     std::vector<unsigned> dbase;        // per device node: its first Debye edge
     std::vector<long long> dd_f;        // Debye edges in node order: one-step ones first
@@ -716,8 +720,13 @@ SlotPlan plan_slots(const HostSim& sim, const Geom& g, bool z_layer, const std::
     for (const auto& q : sim.debye_edges) order.push_back({q.id, q.comp});
     std::vector<size_t> perm(order.size());
     for (size_t q = 0; q < perm.size(); ++q) perm[q] = q;
-    std::sort(perm.begin(), perm.end(), [&](size_t x, size_t y) { return order[x] < order[y]; });
-    std::vector<uint32_t> dfirst(sim.debye_edges.empty() ? 0 : nn, 0xffffffffu);
+    __gnu_parallel::sort(perm.begin(), perm.end(), [&](size_t x, size_t y) { return order[x] < order[y]; });
+    std::vector<uint32_t> dfirst;
+    if (!sim.debye_edges.empty()) {
+        dfirst.resize(nn);
+#pragma omp parallel for schedule(static)
+        for (long long q = 0; q < (long long)nn; ++q) dfirst[size_t(q)] = 0xffffffffu;
+    }
     for (size_t e = 0; e < perm.size(); ++e) {
         const uint64_t id = sim.debye_edges[perm[e]].id;
         if (dfirst[id] == 0xffffffffu) dfirst[id] = uint32_t(e);
@@ -731,7 +740,7 @@ SlotPlan plan_slots(const HostSim& sim, const Geom& g, bool z_layer, const std::
     // per candidate tile: its coefficient classes over the region whose E it forms
     // (planes i0 - 1 .. i1, rows j0 - 1 .. j0 + 14, columns k0 - 1 .. k0 + 64)
     const long long cand = (long long)NS * J * kt;
-    std::vector<float> ctab(size_t(cand) * LOCAL_CLASSES * 9, 0.f);
+    std::vector<float> ctab(size_t(cand) * LOCAL_CLASSES * TB_REC, 0.f);
     std::vector<size_t> cand_idbase(static_cast<size_t>(cand));
     {
         size_t acc = 0;
@@ -753,7 +762,7 @@ SlotPlan plan_slots(const HostSim& sim, const Geom& g, bool z_layer, const std::
         uint8_t vals[512];
         int count = 0;
         bool over = false;
-        float* tab = ctab.data() + size_t(c) * LOCAL_CLASSES * 9;
+        float* tab = ctab.data() + size_t(c) * LOCAL_CLASSES * TB_REC;
         uint8_t* idp = P.ids.data() + cand_idbase[size_t(c)] * 16 * TB_CW;
         for (int i = i0 - 1; i <= i1 && !over; ++i)
             for (int r = -1; r < 15 && !over; ++r)
@@ -780,9 +789,9 @@ SlotPlan plan_slots(const HostSim& sim, const Geom& g, bool z_layer, const std::
                         vals[h] = uint8_t(count);
                         const Coef& cf = sim.classes[key.gid];
                         for (int t = 0; t < 3; ++t) {
-                            tab[count * 9 + t] = cf.ca[t];
-                            tab[count * 9 + 3 + t] = cf.cb[t];
-                            tab[count * 9 + 6 + t] = key.dd[t];
+                            tab[count * TB_REC + t] = cf.ca[t];
+                            tab[count * TB_REC + 3 + t] = cf.cb[t];
+                            tab[count * TB_REC + 6 + t] = key.dd[t];
                         }
                         ++count;
                     }
@@ -820,7 +829,7 @@ SlotPlan plan_slots(const HostSim& sim, const Geom& g, bool z_layer, const std::
     // keep the ids and tables of the tiles kept
     {
         std::vector<uint8_t> ids;
-        std::vector<float> tabs(P.tb.size() * LOCAL_CLASSES * 9);
+        std::vector<float> tabs(P.tb.size() * LOCAL_CLASSES * TB_REC);
         size_t acc = 0;
         for (size_t b = 0; b < P.tb.size(); ++b) {
             const size_t c = cand_of_tb[b];
@@ -828,7 +837,8 @@ SlotPlan plan_slots(const HostSim& sim, const Geom& g, bool z_layer, const std::
             P.idbase.push_back(int(acc));
             ids.insert(ids.end(), P.ids.begin() + cand_idbase[c] * 16 * TB_CW,
                        P.ids.begin() + (cand_idbase[c] + planes) * 16 * TB_CW);
-            std::memcpy(tabs.data() + b * LOCAL_CLASSES * 9, ctab.data() + c * LOCAL_CLASSES * 9, LOCAL_CLASSES * 9 * 4);
+            std::memcpy(tabs.data() + b * LOCAL_CLASSES * TB_REC, ctab.data() + c * LOCAL_CLASSES * TB_REC,
+                        LOCAL_CLASSES * TB_REC * 4);
             acc += planes;
         }
         P.ids.swap(ids);
@@ -853,7 +863,11 @@ SlotPlan plan_slots(const HostSim& sim, const Geom& g, bool z_layer, const std::
     }
     // Debye edges: one-step ones first; per device node its first edge
     const size_t nnp = size_t(g.n0) * n1 * size_t(g.p2);
-    if (!perm.empty()) P.dbase.assign(nnp, 0u);
+    if (!perm.empty()) {
+        P.dbase.resize(nnp);
+#pragma omp parallel for schedule(static)
+        for (long long q = 0; q < (long long)nnp; ++q) P.dbase[size_t(q)] = 0u;
+    }
     std::vector<size_t> first_c, first_r;
     for (size_t e = 0; e < perm.size(); ++e) {
         const auto& q = sim.debye_edges[perm[e]];
@@ -1388,12 +1402,13 @@ int session_new(Gpu* gpu, const HostSim& sim, const RunSpec& rs, Session** out, 
     const bool z_layer = g.pml > 0 && g.pw <= TmaL<float>::PZW;
     if (s->fused && rs.tma && !(std::getenv("FIELDGRID_NO_TMA") && std::getenv("FIELDGRID_NO_TMA")[0] == '1')) {
         // the two-step mode: graph-stepped fused runs with no wires, sheets, NTFF, plane DFT, design
-        // history, and at most TB_NPMAX Debye poles, on sm_100 (FIELDGRID_STEP_DEPTH=1 turns it off)
+        // history, and at most TB_NPMAX Debye poles, on sm_100 (FIELDGRID_STEP_DEPTH=1 or 2 chooses)
         int dev = 0, major = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev);
         const char* dv = std::getenv("FIELDGRID_STEP_DEPTH");
-        const bool want = rs.graphs && major >= 10 && !(dv && dv[0] == '1') && s->n_wires == 0 && s->n_sheets == 0 &&
+        const int depth = dv && (dv[0] == '1' || dv[0] == '2') ? dv[0] - '0' : STEP_DEPTH_DEFAULT;
+        const bool want = depth == 2 && rs.graphs && major >= 10 && s->n_wires == 0 && s->n_sheets == 0 &&
                           s->plane_len == 0 && s->ntff_len == 0 && !(rs.design && !rs.design->empty()) &&
                           sim.poles.size() <= size_t(TB_NPMAX) && (g.pml == 0 || z_layer);
         if (want) sp = plan_slots(sim, g, z_layer, special);

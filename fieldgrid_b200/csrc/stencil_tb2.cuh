@@ -16,10 +16,10 @@
 //
 // One producer warp streams, per x-plane, E^n (rows -2 .. 15), H^{n-1/2} (rows -2 .. 14), the
 // block's class ids and, in tiles that reach the k layer, the z-slab psi of E and H into a ring of
-// shared-memory stages with cp.async.bulk.tensor. 17 main warps own one row each (row w - 2) with
-// a column pair per lane; 2 edge warps take the 51 points of the extra columns -2, -1 and 64. A
-// point is always computed by the same thread, so each point's values of the previous x-plane stay
-// in registers; neighbours go through shared memory.
+// shared-memory stages with cp.async.bulk.tensor. 17 main warps own one row each (row w - 2), a
+// lane the columns lane and lane + 32; 2 edge warps take the 51 points of the extra columns -2, -1
+// and 64. A point is always computed by the same thread, so each point's values of the previous
+// x-plane stay in registers; neighbours go through shared memory.
 //
 // Tiles whose halo (two nodes around the tile and two planes around the segment) would reach an
 // x- or y-layer of the CPML, a port, probe loop, source or inductor are not run here; the one-step
@@ -44,6 +44,7 @@ constexpr int TB_PZW = 32;                       // z-slab psi row pitch in shar
 constexpr int TB_CW = 80;                        // class-id row pitch (columns -1 .. 78)
 constexpr int TB_SEGMAX = 64;
 constexpr int TB_NPMAX = 2;                      // Debye poles the two-step mode takes
+constexpr int TB_REC = 12;                       // floats per class record: ca[3], cb[3], dd[3], 3 pad
 
 template <int STAGES>
 struct Tb2Layout {
@@ -70,7 +71,7 @@ struct Tb2Layout {
     static constexpr int ZE1 = al(2 * 16 * TB_PZW * 4);      // psi E^{n+1} of the z slabs (x2)
     static constexpr int NAX = 18 + 68 + (TB_SEGMAX + 4);    // j rows -2 .. 15, k columns -2 .. 65, planes
     static constexpr int AX = al(NAX * int(sizeof(AxisNode)));
-    static constexpr int LT = al(LOCAL_CLASSES * 9 * 4);     // (ca[3], cb[3], dd[3]) per local class
+    static constexpr int LT = al(LOCAL_CLASSES * TB_REC * 4);   // the block's class records
     static constexpr int BARS = al(2 * STAGES * 8);
     static constexpr int OFF_WORK = STAGES * STAGE;
     static constexpr int OFF_E1 = OFF_WORK + H1;
@@ -88,7 +89,7 @@ struct Tb2Args {
     float k_mu;
     const int4* blocks;          // per block: (k0 | TMA_ZL_TILE | TB_RIM, j0, i0, i1)
     const int* id_base;          // per block: its first plane in the block-major class-id array
-    const float* tables;         // per block: LOCAL_CLASSES x (ca[3], cb[3], dd[3])
+    const float* tables;         // per block: LOCAL_CLASSES records of TB_REC floats (ca, cb, dd)
     float* e_out1;               // set B (step n + 1): written by rim tiles only
     float* h_out1;
     float* e_out2;               // set C (step n + 2)
@@ -116,14 +117,12 @@ struct Coef9 {
 };
 
 __device__ __forceinline__ Coef9 coef9(const float* lt, unsigned id) {
+    const float4* t = reinterpret_cast<const float4*>(lt + id * TB_REC);
+    const float4 v0 = t[0], v1 = t[1], v2 = t[2];
     Coef9 c;
-    const float* t = lt + id * 9;
-#pragma unroll
-    for (int q = 0; q < 3; ++q) {
-        c.ca[q] = t[q];
-        c.cb[q] = t[3 + q];
-        c.dd[q] = t[6 + q];
-    }
+    c.ca[0] = v0.x; c.ca[1] = v0.y; c.ca[2] = v0.z;
+    c.cb[0] = v0.w; c.cb[1] = v1.x; c.cb[2] = v1.y;
+    c.dd[0] = v1.z; c.dd[1] = v1.w; c.dd[2] = v2.x;
     return c;
 }
 
@@ -267,8 +266,9 @@ __device__ __forceinline__ void tb2_march(const CUtensorMap& map_e, const CUtens
         axj[q] = v;
     }
     {
-        const float* src = a.tables + (long long)blockIdx.x * (LOCAL_CLASSES * 9);
-        for (int q = tid; q < LOCAL_CLASSES * 9; q += blockDim.x) lt[q] = src[q];
+        const float4* src = reinterpret_cast<const float4*>(a.tables + (long long)blockIdx.x * (LOCAL_CLASSES * TB_REC));
+        float4* dst = reinterpret_cast<float4*>(lt);
+        for (int q = tid; q < LOCAL_CLASSES * TB_REC / 4; q += blockDim.x) dst[q] = src[q];
     }
     __syncthreads();
 
@@ -307,18 +307,21 @@ __device__ __forceinline__ void tb2_march(const CUtensorMap& map_e, const CUtens
     const bool main_w = w < TB_MAIN;
     constexpr int EC = L::ER * L::EW, HC = L::HR * L::HW, BW = L::BW;
     constexpr int H1C = 17 * BW, E1C = 16 * BW, H2C = 15 * BW;
-    // the points of this thread: main warps a column pair of row w - 2, edge warps one point
-    int npt, r, c0;
+    // The points of this thread. Main warps: row w - 2, columns lane and lane + 32 (a warp's lanes
+    // touch 32 consecutive words of every buffer: no bank conflicts). Edge warps: one point each.
+    int npt, r, cpt[2];
     if (main_w) {
         npt = 2;
         r = w - 2;
-        c0 = 2 * lane;
+        cpt[0] = lane;
+        cpt[1] = lane + 32;
     } else {
         const int q = (w - TB_MAIN) * 32 + lane;
         npt = q < TB_EDGE_POINTS ? 1 : 0;
         const int sel = q / 17;
         r = q % 17 - 2;
-        c0 = sel == 0 ? -2 : (sel == 1 ? -1 : 64);
+        cpt[0] = sel == 0 ? -2 : (sel == 1 ? -1 : 64);
+        cpt[1] = cpt[0];
     }
     const int jj = j0 + r;
     // the half steps each point takes part in (the two points of a main thread share them)
@@ -328,26 +331,37 @@ __device__ __forceinline__ void tb2_march(const CUtensorMap& map_e, const CUtens
         do_h2 = r >= -1 && r <= 13;
         do_e2 = r >= 0 && r <= 13;
     } else {
-        do_e1 = npt > 0 && c0 != -2 && r >= -1;
-        do_h2 = npt > 0 && r >= -1 && r <= 13 && (c0 == -1 || (c0 == 64 && redge));
-        do_e2 = npt > 0 && r >= 0 && r <= 13 && c0 == 64 && redge;
+        const int c = cpt[0];
+        do_e1 = npt > 0 && c != -2 && r >= -1;
+        do_h2 = npt > 0 && r >= -1 && r <= 13 && (c == -1 || (c == 64 && redge));
+        do_e2 = npt > 0 && r >= 0 && r <= 13 && c == 64 && redge;
     }
     const bool own_row = r >= 0 && r < TB_TJ;
-    // per point: grid column, liveness, guards, axis factors
-    int kk[2];
+    // per point: liveness, guards, k-axis factors; the second point of a main thread sits 32
+    // columns right of the first, so its offsets are the first's + 32
+    const int c0 = cpt[0];
     bool live[2], kn[2], kp[2], own[2];
-    const AxisNode* akp[2];
+    float dk[2], ek[2];
     const AxisNode& aj = axj[r + 2];
+    const float dj = aj.inv_d, ej = aj.inv_dd;
+#pragma unroll
     for (int q = 0; q < 2; ++q) {
-        const int c = c0 + q;
-        kk[q] = k0 + c;
-        live[q] = q < npt && kk[q] >= 0 && kk[q] < g.n2;
-        kn[q] = kk[q] + 1 < g.n2;
-        kp[q] = kk[q] > 0;
+        const int c = c0 + 32 * q;
+        const int k = k0 + c;
+        live[q] = q < npt && k >= 0 && k < g.n2;
+        kn[q] = k + 1 < g.n2;
+        kp[q] = k > 0;
         own[q] = live[q] && own_row && (c < TB_TK || (c == TB_TK && redge)) && c >= 0;
-        akp[q] = axk + min(max(c + 2, 0), 67);
+        const AxisNode* an = axk + min(max(c + 2, 0), 67);
+        dk[q] = an->inv_d;
+        ek[q] = an->inv_dd;
     }
-    const long long rowg = (long long)jj * g.p2;
+    const int eo0 = (r + 2) * L::EW + (c0 + 4);    // E^n / H^{n-1/2} boxes (same pitch)
+    const int b20 = (r + 2) * BW + (c0 + 2);       // H1 buffer (rows -2 ..)
+    const int b10 = (r + 1) * BW + (c0 + 1);       // E1 and H2 buffers (rows -1 ..)
+    const int cl0 = (r + 1) * TB_CW + (c0 + 1);    // class ids
+    const long long rowg = (long long)jj * g.p2 + (k0 + c0);
+    const long long psi_row = (long long)jj * pw;   // + plane * n1 * pw
 
     float h1p[2][3] = {{0, 0, 0}, {0, 0, 0}};   // H1 of the previous plane at the point
     float h2p[2][3] = {{0, 0, 0}, {0, 0, 0}};   // H2 of the previous plane at the point
@@ -365,54 +379,54 @@ __device__ __forceinline__ void tb2_march(const CUtensorMap& map_e, const CUtens
         const unsigned char* CL = base + s * L::STAGE + L::OFF_C;
         const float* ZH0 = reinterpret_cast<const float*>(base + s * L::STAGE + L::OFF_ZH);
         const float* ZE0 = reinterpret_cast<const float*>(base + s * L::STAGE + L::OFF_ZE);
-        const AxisNode& ai = axi[u];
-        const AxisNode& aim = axi[u > 0 ? u - 1 : 0];
+        const float di = axi[u].inv_d, ei = axi[u].inv_dd;
+        const float dim = axi[u > 0 ? u - 1 : 0].inv_d, eim = axi[u > 0 ? u - 1 : 0].inv_dd;
         float* e1cur = e1s + (t & 1) * (L::E1 / 4);
         const float* e1prv = e1s + ((t - 1) & 1) * (L::E1 / 4);
         float* zh1cur = zh1s + (t & 1) * (L::ZH1 / 4);
         const float* zh1prv = zh1s + ((t - 1) & 1) * (L::ZH1 / 4);
         float* ze1cur = ze1s + (t & 1) * (L::ZE1 / 4);
         const float* ze1prv = ze1s + ((t - 1) & 1) * (L::ZE1 / 4);
-        const long long plane = (long long)t * g.n1 * g.p2;
-        const long long planem = (long long)(t - 1) * g.n1 * g.p2;
+        const long long plane = (long long)t * g.n1 * g.p2 + rowg;
+        const long long planem = (long long)(t - 1) * g.n1 * g.p2 + rowg;
+        const long long zp = (long long)t * g.n1 * pw + psi_row, zpm = (long long)(t - 1) * g.n1 * pw + psi_row;
         const bool owned_t = t >= i0 && t < i1;       // plane t is owned (H1, E1 rim writes)
         const bool owned_tm = t - 1 >= i0 && t - 1 < i1;
 
         // 1. H1(t)
         float h1c[2][3] = {{0, 0, 0}, {0, 0, 0}};
         if (do_h1) {
-            for (int q = 0; q < npt; ++q) {
+#pragma unroll
+            for (int q = 0; q < 2; ++q) {
                 if (!live[q]) continue;
-                const int c = c0 + q;
-                const int eo = (r + 2) * L::EW + (c + 4), ho = (r + 2) * L::HW + (c + 4);
-                const float e0[3] = {E0[eo], E0[EC + eo], E0[2 * EC + eo]};
-                float h[3] = {H0[ho], H0[HC + ho], H0[2 * HC + ho]};
-                const tb::Fac f{ai.inv_d, aj.inv_d, akp[q]->inv_d, 0.f, 0.f, 0.f};
+                const int o = eo0 + 32 * q;
+                const float e0[3] = {E0[o], E0[EC + o], E0[2 * EC + o]};
+                float h[3] = {H0[o], H0[HC + o], H0[2 * HC + o]};
+                const tb::Fac f{di, dj, dk[q], 0.f, 0.f, 0.f};
                 const float* zin0 = ZH0 + (r + 2) * pw;
                 float z0 = 0.f, z1 = 0.f;
-                tb::h_point<ZL>(a.k_mu, f, e0, E0[2 * EC + eo + L::EW], E0[eo + L::EW], E0[EC + eo + 1], E0[eo + 1],
-                                E0n[2 * EC + eo], E0n[EC + eo], h, kn[q], akp[q], zin0, zin0 + L::ZHR * pw, z0, z1);
-                const int bo = (r + 2) * BW + (c + 2);
+                tb::h_point<ZL>(a.k_mu, f, e0, E0[2 * EC + o + L::EW], E0[o + L::EW], E0[EC + o + 1], E0[o + 1],
+                                E0n[2 * EC + o], E0n[EC + o], h, kn[q], (axk + min(max(c0 + 32 * q + 2, 0), 67)), zin0, zin0 + L::ZHR * pw, z0, z1);
+                const int bo = b20 + 32 * q;
                 h1s[bo] = h[0];
                 h1s[H1C + bo] = h[1];
                 h1s[2 * H1C + bo] = h[2];
                 h1c[q][0] = h[0];
                 h1c[q][1] = h[1];
                 h1c[q][2] = h[2];
-                const int sl = ZL ? akp[q]->slot_h : -1;
+                const int sl = ZL ? (axk + min(max(c0 + 32 * q + 2, 0), 67))->slot_h : -1;
                 if (ZL && sl >= 0 && kn[q]) {
                     zh1cur[(r + 2) * TB_PZW + sl] = z0;
                     zh1cur[17 * TB_PZW + (r + 2) * TB_PZW + sl] = z1;
                 }
                 if (rim && own[q] && owned_t) {
-                    const long long id = plane + rowg + kk[q];
-                    a.h_out1[id] = h[0];
-                    a.h_out1[g.cs + id] = h[1];
-                    a.h_out1[2 * g.cs + id] = h[2];
+                    float* out = a.h_out1 + plane + 32 * q;
+                    out[0] = h[0];
+                    out[g.cs] = h[1];
+                    out[2 * g.cs] = h[2];
                     if (ZL && sl >= 0 && kn[q]) {
-                        const long long o = ((long long)t * g.n1 + jj) * pw + sl;
-                        a.pz_h1[g.psi_off[9 + 0 * 3 + 2] + o] = z0;
-                        a.pz_h1[g.psi_off[9 + 1 * 3 + 2] + o] = z1;
+                        a.pz_h1[g.psi_off[9 + 0 * 3 + 2] + zp + sl] = z0;
+                        a.pz_h1[g.psi_off[9 + 1 * 3 + 2] + zp + sl] = z1;
                     }
                 }
             }
@@ -427,47 +441,45 @@ __device__ __forceinline__ void tb2_march(const CUtensorMap& map_e, const CUtens
         float e1c[2][3] = {{0, 0, 0}, {0, 0, 0}};
         unsigned cidc[2] = {0u, 0u};
         if (do_e1 && e1_plane) {
-            for (int q = 0; q < npt; ++q) {
+#pragma unroll
+            for (int q = 0; q < 2; ++q) {
                 if (!live[q]) continue;
-                const int c = c0 + q;
-                const int eo = (r + 2) * L::EW + (c + 4);
-                const int bo = (r + 2) * BW + (c + 2);
-                const float e_old[3] = {E0[eo], E0[EC + eo], E0[2 * EC + eo]};
+                const int o = eo0 + 32 * q, bo = b20 + 32 * q;
+                const float e_old[3] = {E0[o], E0[EC + o], E0[2 * EC + o]};
                 float e[3] = {e_old[0], e_old[1], e_old[2]};
-                cidc[q] = CL[(r + 1) * TB_CW + (c + 1)];
+                cidc[q] = CL[cl0 + 32 * q];
                 const tb::Coef9 cf = tb::coef9(lt, cidc[q]);
-                const tb::Fac f{0.f, 0.f, 0.f, ai.inv_dd, aj.inv_dd, akp[q]->inv_dd};
+                const tb::Fac f{0.f, 0.f, 0.f, ei, ej, ek[q]};
                 const float* zin0 = ZE0 + (r + 1) * pw;
                 float z0 = 0.f, z1 = 0.f;
                 tb::e_point<ZL>(f, cf, e, h1c[q], h1s[2 * H1C + bo - BW], h1s[bo - BW], h1s[H1C + bo - 1], h1s[bo - 1],
-                                h1p[q][1], h1p[q][2], kp[q], akp[q], zin0, zin0 + L::ZER * pw, z0, z1);
+                                h1p[q][1], h1p[q][2], kp[q], (axk + min(max(c0 + 32 * q + 2, 0), 67)), zin0, zin0 + L::ZER * pw, z0, z1);
                 const bool keep = own[q] && owned_t;
                 if (tb::has_debye(cf)) {
-                    const long long id = plane + rowg + kk[q];
                     // owned points keep s^{n+1} for their E2 (slot of step n + 1)
-                    tb::debye_point(cf, e, e_old, a.dbase[id], a.dtable, a.dstate_in, keep ? a.dstate_1 : nullptr);
+                    tb::debye_point(cf, e, e_old, a.dbase[plane + 32 * q], a.dtable, a.dstate_in,
+                                    keep ? a.dstate_1 : nullptr);
                 }
-                const int bo1 = (r + 1) * BW + (c + 1);
+                const int bo1 = b10 + 32 * q;
                 e1cur[bo1] = e[0];
                 e1cur[E1C + bo1] = e[1];
                 e1cur[2 * E1C + bo1] = e[2];
                 e1c[q][0] = e[0];
                 e1c[q][1] = e[1];
                 e1c[q][2] = e[2];
-                const int sl = ZL ? akp[q]->slot_e : -1;
+                const int sl = ZL ? (axk + min(max(c0 + 32 * q + 2, 0), 67))->slot_e : -1;
                 if (ZL && sl >= 0) {
                     ze1cur[(r + 1) * TB_PZW + sl] = z0;
                     ze1cur[16 * TB_PZW + (r + 1) * TB_PZW + sl] = z1;
                 }
                 if (rim && keep) {
-                    const long long id = plane + rowg + kk[q];
-                    a.e_out1[id] = e[0];
-                    a.e_out1[g.cs + id] = e[1];
-                    a.e_out1[2 * g.cs + id] = e[2];
+                    float* out = a.e_out1 + plane + 32 * q;
+                    out[0] = e[0];
+                    out[g.cs] = e[1];
+                    out[2 * g.cs] = e[2];
                     if (ZL && sl >= 0) {
-                        const long long o = ((long long)t * g.n1 + jj) * pw + sl;
-                        a.pz_e1[g.psi_off[0 * 3 + 2] + o] = z0;
-                        a.pz_e1[g.psi_off[1 * 3 + 2] + o] = z1;
+                        a.pz_e1[g.psi_off[0 * 3 + 2] + zp + sl] = z0;
+                        a.pz_e1[g.psi_off[1 * 3 + 2] + zp + sl] = z1;
                     }
                 }
             }
@@ -479,17 +491,17 @@ __device__ __forceinline__ void tb2_march(const CUtensorMap& map_e, const CUtens
         const bool h2_plane = t - 1 >= i0 - 1;
         float h2c[2][3] = {{0, 0, 0}, {0, 0, 0}};
         if (do_h2 && h2_plane) {
-            for (int q = 0; q < npt; ++q) {
+#pragma unroll
+            for (int q = 0; q < 2; ++q) {
                 if (!live[q]) continue;
-                const int c = c0 + q;
-                const int bo1 = (r + 1) * BW + (c + 1);
+                const int bo1 = b10 + 32 * q;
                 const float e0[3] = {e1prv[bo1], e1prv[E1C + bo1], e1prv[2 * E1C + bo1]};
                 float h[3] = {h1p[q][0], h1p[q][1], h1p[q][2]};
-                const tb::Fac f{aim.inv_d, aj.inv_d, akp[q]->inv_d, 0.f, 0.f, 0.f};
+                const tb::Fac f{dim, dj, dk[q], 0.f, 0.f, 0.f};
                 const float* zin0 = zh1prv + (r + 2) * TB_PZW;
                 float z0 = 0.f, z1 = 0.f;
                 tb::h_point<ZL>(a.k_mu, f, e0, e1prv[2 * E1C + bo1 + BW], e1prv[bo1 + BW], e1prv[E1C + bo1 + 1],
-                                e1prv[bo1 + 1], e1c[q][2], e1c[q][1], h, kn[q], akp[q], zin0, zin0 + 17 * TB_PZW, z0,
+                                e1prv[bo1 + 1], e1c[q][2], e1c[q][1], h, kn[q], (axk + min(max(c0 + 32 * q + 2, 0), 67)), zin0, zin0 + 17 * TB_PZW, z0,
                                 z1);
                 h2s[bo1] = h[0];
                 h2s[H2C + bo1] = h[1];
@@ -498,15 +510,14 @@ __device__ __forceinline__ void tb2_march(const CUtensorMap& map_e, const CUtens
                 h2c[q][1] = h[1];
                 h2c[q][2] = h[2];
                 if (own[q] && owned_tm) {
-                    const long long id = planem + rowg + kk[q];
-                    a.h_out2[id] = h[0];
-                    a.h_out2[g.cs + id] = h[1];
-                    a.h_out2[2 * g.cs + id] = h[2];
-                    const int sl = ZL ? akp[q]->slot_h : -1;
+                    float* out = a.h_out2 + planem + 32 * q;
+                    out[0] = h[0];
+                    out[g.cs] = h[1];
+                    out[2 * g.cs] = h[2];
+                    const int sl = ZL ? (axk + min(max(c0 + 32 * q + 2, 0), 67))->slot_h : -1;
                     if (ZL && sl >= 0 && kn[q]) {
-                        const long long o = ((long long)(t - 1) * g.n1 + jj) * pw + sl;
-                        a.pz_h2[g.psi_off[9 + 0 * 3 + 2] + o] = z0;
-                        a.pz_h2[g.psi_off[9 + 1 * 3 + 2] + o] = z1;
+                        a.pz_h2[g.psi_off[9 + 0 * 3 + 2] + zpm + sl] = z0;
+                        a.pz_h2[g.psi_off[9 + 1 * 3 + 2] + zpm + sl] = z1;
                     }
                 }
             }
@@ -518,32 +529,33 @@ __device__ __forceinline__ void tb2_march(const CUtensorMap& map_e, const CUtens
 
         // 4. E2(t - 1) (owned planes i0 .. i1 - 1)
         if (do_e2 && owned_tm) {
-            for (int q = 0; q < npt; ++q) {
+#pragma unroll
+            for (int q = 0; q < 2; ++q) {
                 if (!own[q]) continue;
-                const int c = c0 + q;
-                const int bo1 = (r + 1) * BW + (c + 1);
+                const int bo1 = b10 + 32 * q;
                 const float e_old[3] = {e1prv[bo1], e1prv[E1C + bo1], e1prv[2 * E1C + bo1]};
                 float e[3] = {e_old[0], e_old[1], e_old[2]};
                 const tb::Coef9 cf = tb::coef9(lt, cidp[q]);
-                const tb::Fac f{0.f, 0.f, 0.f, aim.inv_dd, aj.inv_dd, akp[q]->inv_dd};
+                const tb::Fac f{0.f, 0.f, 0.f, eim, ej, ek[q]};
                 const float* zin0 = ze1prv + (r + 1) * TB_PZW;
                 float z0 = 0.f, z1 = 0.f;
                 tb::e_point<ZL>(f, cf, e, h2c[q], h2s[2 * H2C + bo1 - BW], h2s[bo1 - BW], h2s[H2C + bo1 - 1],
-                                h2s[bo1 - 1], h2p[q][1], h2p[q][2], kp[q], akp[q], zin0, zin0 + 16 * TB_PZW, z0, z1);
-                const long long id = planem + rowg + kk[q];
-                if (tb::has_debye(cf)) tb::debye_point(cf, e, e_old, a.dbase[id], a.dtable, a.dstate_1, a.dstate_2);
-                a.e_out2[id] = e[0];
-                a.e_out2[g.cs + id] = e[1];
-                a.e_out2[2 * g.cs + id] = e[2];
-                const int sl = ZL ? akp[q]->slot_e : -1;
+                                h2s[bo1 - 1], h2p[q][1], h2p[q][2], kp[q], (axk + min(max(c0 + 32 * q + 2, 0), 67)), zin0, zin0 + 16 * TB_PZW, z0, z1);
+                if (tb::has_debye(cf))
+                    tb::debye_point(cf, e, e_old, a.dbase[planem + 32 * q], a.dtable, a.dstate_1, a.dstate_2);
+                float* out = a.e_out2 + planem + 32 * q;
+                out[0] = e[0];
+                out[g.cs] = e[1];
+                out[2 * g.cs] = e[2];
+                const int sl = ZL ? (axk + min(max(c0 + 32 * q + 2, 0), 67))->slot_e : -1;
                 if (ZL && sl >= 0) {
-                    const long long o = ((long long)(t - 1) * g.n1 + jj) * pw + sl;
-                    a.pz_e2[g.psi_off[0 * 3 + 2] + o] = z0;
-                    a.pz_e2[g.psi_off[1 * 3 + 2] + o] = z1;
+                    a.pz_e2[g.psi_off[0 * 3 + 2] + zpm + sl] = z0;
+                    a.pz_e2[g.psi_off[1 * 3 + 2] + zpm + sl] = z1;
                 }
             }
         }
         // this plane's values become the previous plane's
+#pragma unroll
         for (int q = 0; q < 2; ++q) {
             cidp[q] = cidc[q];
             for (int cc = 0; cc < 3; ++cc) {

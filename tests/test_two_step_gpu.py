@@ -2,9 +2,9 @@
 the one-step kernels on the tiles near ports, probes and the CPML's x/y layers, with the z-slab psi
 and the Debye state in three time slots. Each node's update is the one-step kernels' arithmetic in
 the same order, so a run in this mode must give the one-step run's fields, port series and energy
-bit for bit (FIELDGRID_STEP_DEPTH=1 turns the mode off), at odd and even step counts, with and
-without a CPML, with Debye media, and on a grid whose last tile owns the extra column of a
-64 t + 1 row. One case is also checked against the oracle."""
+bit for bit (FIELDGRID_STEP_DEPTH=2 asks for the mode, 1 for the one-step kernels alone), at odd
+and even step counts, with and without a CPML, with Debye media, and on a grid whose last tile
+owns the extra column of a 64 t + 1 row. One case is also checked against the oracle."""
 import numpy as np
 import pytest
 
@@ -17,10 +17,7 @@ pytestmark = pytest.mark.gpu
 
 
 def _run(gpu, sc, steps, one_step, monkeypatch):
-    if one_step:
-        monkeypatch.setenv("FIELDGRID_STEP_DEPTH", "1")
-    else:
-        monkeypatch.delenv("FIELDGRID_STEP_DEPTH", raising=False)
+    monkeypatch.setenv("FIELDGRID_STEP_DEPTH", "1" if one_step else "2")
     sim = fdtd.Sim.try_new(*sc.args())
     s = fdtd.Session(gpu, sim, 0, sc.pulse, sc.extras)
     variant = s.variant
@@ -60,7 +57,7 @@ def test_two_step_mode_equals_one_step_bit_for_bit(gpu, monkeypatch, name, make,
 
 def test_two_step_mode_matches_the_oracle(gpu, monkeypatch):
     sc = W.spheres(96, pml=6, count=30, rmin=4, rmax=14, steps=150)
-    monkeypatch.delenv("FIELDGRID_STEP_DEPTH", raising=False)
+    monkeypatch.setenv("FIELDGRID_STEP_DEPTH", "2")
     sim = fdtd.Sim.try_new(*sc.args())
     rec = fdtd.run(gpu, sim, 0, sc.pulse, sc.extras, keep_fields=True)
     ref = O.run_cpu(O.OracleSim(*sc.args(), bits=32), 0, sc.pulse, sc.extras, keep_fields=True)

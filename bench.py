@@ -61,6 +61,7 @@ def parse():
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
     p.add_argument("--cells", type=int, default=512, help="cells per axis (512 is the benchmark workload)")
+    p.add_argument("--spheres", type=int, default=None, help="spheres in the grid (default: 200 at 256 cells and up)")
     p.add_argument("--separate", action="store_true", help="time the unfused H and E kernels instead")
     p.add_argument("--pml", type=int, default=None, help="CPML depth in cells (default: 10 at 512^3)")
     p.add_argument("--cpu-steps", type=int, default=8, help="full time steps the CPU baseline times")
@@ -90,11 +91,11 @@ def measured_peaks():
         return 6650.0, "profiling recipe fallback 6.65 TB/s (of fallback)"
 
 
-def workload(cells: int, steps: int, fused: bool = True, pml=None):
+def workload(cells: int, steps: int, fused: bool = True, pml=None, spheres=None):
     from fieldgrid_b200 import workloads as W
     if pml is None:
         pml = 10 if cells >= 256 else max(4, cells // 16)
-    count = 200 if cells >= 256 else max(8, cells // 3)
+    count = spheres if spheres is not None else (200 if cells >= 256 else max(8, cells // 3))
     rmin, rmax = (5, 40) if cells >= 256 else (2, max(3, cells // 12))
     return W.spheres(cells=cells, pml=pml, steps=steps, count=count, rmin=rmin, rmax=rmax, fused=fused)
 
@@ -452,7 +453,8 @@ def main():
     K, W = args.steps, max(args.warmup, 3)
     kt_steps = 10
     t = time.time()
-    sc = workload(args.cells, W + K + kt_steps + (48 if K >= 48 else 0), fused=not args.separate, pml=args.pml)
+    sc = workload(args.cells, W + K + kt_steps + (48 if K >= 48 else 0), fused=not args.separate, pml=args.pml,
+                  spheres=args.spheres)
     t_mat = time.time() - t
     t = time.time()
     sim = fdtd.Sim.try_new(*sc.args())

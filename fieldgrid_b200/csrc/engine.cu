@@ -61,7 +61,57 @@ int gpu_open(int device, Gpu** out, std::string& err) {
     return FG_OK;
 }
 
-void gpu_close(Gpu* g) { delete g; }
+void gpu_close(Gpu* g) {
+    if (!g) return;
+    cudaSetDevice(g->device);
+    for (int b = 0; b < 2; ++b) {
+        if (g->stage_ev[b]) {
+            cudaEventSynchronize(static_cast<cudaEvent_t>(g->stage_ev[b]));
+            cudaEventDestroy(static_cast<cudaEvent_t>(g->stage_ev[b]));
+        }
+        if (g->stage[b]) cudaFreeHost(g->stage[b]);
+    }
+    delete g;
+}
+
+static constexpr size_t STAGE_BYTES = size_t(32) << 20;
+
+int staged_upload(Gpu* g, void* dst, const void* src, size_t bytes, void* stream) {
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (bytes < (size_t(4) << 20)) return int(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st));
+    for (int b = 0; b < 2; ++b) {
+        if (!g->stage[b]) {
+            cudaError_t e = cudaHostAlloc(&g->stage[b], STAGE_BYTES, cudaHostAllocDefault);
+            if (e != cudaSuccess) return int(e);
+            cudaEvent_t ev;
+            e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+            if (e != cudaSuccess) return int(e);
+            g->stage_ev[b] = ev;
+        }
+    }
+    const char* s8 = static_cast<const char*>(src);
+    char* d8 = static_cast<char*>(dst);
+    int b = 0;
+    for (size_t off = 0; off < bytes; off += STAGE_BYTES, b ^= 1) {
+        const size_t n = std::min(STAGE_BYTES, bytes - off);
+        cudaEvent_t ev = static_cast<cudaEvent_t>(g->stage_ev[b]);
+        cudaError_t e = cudaEventSynchronize(ev);   // the buffer's previous transfer has finished
+        if (e != cudaSuccess) return int(e);
+        char* buf = static_cast<char*>(g->stage[b]);
+        const long long parts = (long long)((n + (size_t(1) << 20) - 1) >> 20);
+#pragma omp parallel for schedule(static)
+        for (long long q = 0; q < parts; ++q) {
+            const size_t a = size_t(q) << 20, m = std::min(size_t(1) << 20, n - a);
+            std::memcpy(buf + a, s8 + off + a, m);
+        }
+        e = cudaMemcpyAsync(d8 + off, buf, n, cudaMemcpyHostToDevice, st);
+        if (e != cudaSuccess) return int(e);
+        e = cudaEventRecord(ev, st);
+        if (e != cudaSuccess) return int(e);
+    }
+    // the source may be reused as soon as it has been copied into the staging buffers
+    return int(cudaSuccess);
+}
 
 struct Session {
     Gpu* gpu = nullptr;
@@ -662,7 +712,6 @@ struct SlotPlan {
     std::vector<uint8_t> ids;           // block-major class ids: [plane][16 rows][TB_CW columns]
     std::vector<float> tables;          // per two-step tile: LOCAL_CLASSES records of TB_REC floats
     std::vector<int> cidx;              // one-step tiles of a double step (indices into cp.blocks)
-    std::vector<unsigned> dbase;        // per device node: its first Debye edge
     std::vector<long long> dd_f;        // Debye edges in node order: one-step ones first
     std::vector<unsigned> dd_s;
     std::vector<float> dd_w, dd_cb;
@@ -749,7 +798,7 @@ SlotPlan plan_slots(const HostSim& sim, const Geom& g, bool z_layer, const std::
             const int sg = int(c / ((long long)J * kt));
             acc += size_t(rsegs[sg].y - rsegs[sg].x + 2);
         }
-        P.ids.assign(acc * 16 * TB_CW, 0);
+        P.ids.resize(acc * 16 * TB_CW);   // each candidate clears and fills its own planes below
     }
 #pragma omp parallel for schedule(dynamic, 4)
     for (long long c = 0; c < cand; ++c) {
@@ -764,6 +813,9 @@ SlotPlan plan_slots(const HostSim& sim, const Geom& g, bool z_layer, const std::
         bool over = false;
         float* tab = ctab.data() + size_t(c) * LOCAL_CLASSES * TB_REC;
         uint8_t* idp = P.ids.data() + cand_idbase[size_t(c)] * 16 * TB_CW;
+        std::memset(idp, 0, size_t(i1 - i0 + 2) * 16 * TB_CW);
+        Key last{0xffffffffu, {0.f, 0.f, 0.f}};   // runs of equal keys along a row skip the hash
+        uint8_t last_val = 0;
         for (int i = i0 - 1; i <= i1 && !over; ++i)
             for (int r = -1; r < 15 && !over; ++r)
                 for (int cc = -1; cc < 65; ++cc) {
@@ -773,6 +825,10 @@ SlotPlan plan_slots(const HostSim& sim, const Geom& g, bool z_layer, const std::
                     Key key;
                     key.gid = sim.node_class[id];
                     dd_of(id, key.dd);
+                    if (key.gid == last.gid && std::memcmp(key.dd, last.dd, 12) == 0) {
+                        idp[(size_t(i - (i0 - 1)) * 16 + size_t(r + 1)) * TB_CW + size_t(cc + 1)] = last_val;
+                        continue;
+                    }
                     uint32_t hsh = key.gid * 2654435761u;
                     for (int t = 0; t < 3; ++t) {
                         uint32_t b;
@@ -796,6 +852,8 @@ SlotPlan plan_slots(const HostSim& sim, const Geom& g, bool z_layer, const std::
                         ++count;
                     }
                     idp[(size_t(i - (i0 - 1)) * 16 + size_t(r + 1)) * TB_CW + size_t(cc + 1)] = vals[h];
+                    last = key;
+                    last_val = vals[h];
                 }
         if (over) on[size_t(c)] = 0;
     }
@@ -826,22 +884,16 @@ SlotPlan plan_slots(const HostSim& sim, const Geom& g, bool z_layer, const std::
                 cand_of_tb.push_back(flat(sg, q, bx));
             }
     if (P.tb.empty()) { P.why = "no two-step tile"; return P; }
-    // keep the ids and tables of the tiles kept
+    // the tiles kept point into the candidates' id planes (a dropped candidate leaves its planes
+    // unused); their tables are gathered in tile order
     {
-        std::vector<uint8_t> ids;
         std::vector<float> tabs(P.tb.size() * LOCAL_CLASSES * TB_REC);
-        size_t acc = 0;
         for (size_t b = 0; b < P.tb.size(); ++b) {
             const size_t c = cand_of_tb[b];
-            const size_t planes = size_t(P.tb[b].w - P.tb[b].z + 2);
-            P.idbase.push_back(int(acc));
-            ids.insert(ids.end(), P.ids.begin() + cand_idbase[c] * 16 * TB_CW,
-                       P.ids.begin() + (cand_idbase[c] + planes) * 16 * TB_CW);
+            P.idbase.push_back(int(cand_idbase[c]));
             std::memcpy(tabs.data() + b * LOCAL_CLASSES * TB_REC, ctab.data() + c * LOCAL_CLASSES * TB_REC,
                         LOCAL_CLASSES * TB_REC * 4);
-            acc += planes;
         }
-        P.ids.swap(ids);
         P.tables.swap(tabs);
     }
     // one-step tiles of a double step: those of the one-step plan no two-step tile replaces
@@ -861,13 +913,7 @@ SlotPlan plan_slots(const HostSim& sim, const Geom& g, bool z_layer, const std::
         if (cp.own[b].x >= cp.own[b].y || !two_step(bk.z, cp.own[b].x, std::max(k0, cp.kbase)))
             P.cidx.push_back(int(b));
     }
-    // Debye edges: one-step ones first; per device node its first edge
-    const size_t nnp = size_t(g.n0) * n1 * size_t(g.p2);
-    if (!perm.empty()) {
-        P.dbase.resize(nnp);
-#pragma omp parallel for schedule(static)
-        for (long long q = 0; q < (long long)nnp; ++q) P.dbase[size_t(q)] = 0u;
-    }
+    // Debye edges: one-step ones first (each node's first edge is found on the device)
     std::vector<size_t> first_c, first_r;
     for (size_t e = 0; e < perm.size(); ++e) {
         const auto& q = sim.debye_edges[perm[e]];
@@ -875,10 +921,6 @@ SlotPlan plan_slots(const HostSim& sim, const Geom& g, bool z_layer, const std::
         (two_step(i, j, k) ? first_r : first_c).push_back(e);
     }
     auto devid = [&](uint64_t id) { return (long long)(id / n2) * g.p2 + (long long)(id % n2); };
-    for (size_t e = 0; e < perm.size(); ++e) {
-        const uint64_t id = sim.debye_edges[perm[e]].id;
-        if (dfirst[id] == uint32_t(e)) P.dbase[size_t(devid(id))] = uint32_t(e);
-    }
     for (auto* list : {&first_c, &first_r})
         for (size_t e : *list) {
             const auto& q = sim.debye_edges[perm[e]];
@@ -1061,7 +1103,7 @@ int setup_slots(Session& s, const HostSim& sim, const SlotPlan& sp, long long ps
         return FG_OK;
     };
     auto upload = [&](void* dst, const void* src, size_t bytes) -> int {
-        if (bytes) FG_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s.stream));
+        if (bytes) FG_CUDA(cudaError_t(staged_upload(s.gpu, dst, src, bytes, s.stream)));
         s.h2d_bytes += bytes;
         return FG_OK;
     };
@@ -1112,7 +1154,6 @@ int setup_slots(Session& s, const HostSim& sim, const SlotPlan& sp, long long ps
         FG_CUDA(cudaMemsetAsync(s.dslot[q], 0, std::max<size_t>(ne * np, 1) * 4, s.stream));
     }
     if (ne) {
-        rc |= upload(s.dbase, sp.dbase.data(), nnp * 4);
         rc |= upload(s.dd_f, sp.dd_f.data(), ne * 8);
         rc |= upload(s.dd_s, sp.dd_s.data(), ne * 4);
         rc |= upload(s.dd_w, sp.dd_w.data(), ne * 4);
@@ -1126,6 +1167,12 @@ int setup_slots(Session& s, const HostSim& sim, const SlotPlan& sp, long long ps
     rc |= upload(s.tb_ids, sp.ids.data(), sp.ids.size());
     rc |= upload(s.tb_tables, sp.tables.data(), sp.tables.size() * 4);
     if (rc) return rc;
+    if (ne) {
+        // each Debye node's first edge: the smallest state index among its edges
+        FG_CUDA(cudaMemsetAsync(s.dbase, 0xff, nnp * 4, s.stream));
+        k_debye_base<<<unsigned((ne + 255) / 256), 256, 0, s.stream>>>(s.dd_f, s.dd_s, (long long)ne, g.cs, s.dbase);
+        FG_CUDA(cudaGetLastError());
+    }
     FG_CUDA(cudaStreamSynchronize(s.stream));
     s.n_cblocks = int(cb.size());
     s.n_tb = int(sp.tb.size());
@@ -1263,13 +1310,9 @@ int session_new(Gpu* gpu, const HostSim& sim, const RunSpec& rs, Session** out, 
         d.face_b = unsigned(q.faces[1]);
         sheets.push_back(d);
     }
+    // the Debye edge list of the one-step scheme (filled below unless the two-step mode keeps its own)
     std::vector<long long> debye_f;
     std::vector<float> debye_dd, debye_cb;
-    for (auto& q : sim.debye_edges) {
-        debye_f.push_back((long long)q.comp * cs + dev(q.id));
-        debye_dd.push_back(float(q.dd));
-        debye_cb.push_back(sim.cb(q.comp, q.id));
-    }
     std::vector<float> debye_table{float(sim.poles.size())};
     for (auto& [x, a] : sim.poles) {
         double d = 1.0 + 0.5 * x * sim.dt;
@@ -1355,7 +1398,6 @@ int session_new(Gpu* gpu, const HostSim& sim, const RunSpec& rs, Session** out, 
     s->n_ports = int(probes.size());
     s->n_wires = int(wires.size());
     s->n_sheets = int(sheets.size());
-    s->n_debye = int(debye_f.size());
     s->plane_k = int(rs.has_plane_k ? rs.plane_k : 0);
     s->plane_len = rs.has_plane_k ? uint64_t(n0) * n1 * sc.nf * 10 : 0;
     if (rs.has_plane_k && rs.plane_k >= n2) { err = "plane_k is outside the grid"; return FG_ERR_INVALID; }
@@ -1419,6 +1461,20 @@ int session_new(Gpu* gpu, const HostSim& sim, const RunSpec& rs, Session** out, 
         }
     }
     clk.mark("plans");
+    if (!sp.ok && !sim.debye_edges.empty()) {
+        const long long ne = (long long)sim.debye_edges.size();
+        debye_f.resize(size_t(ne));
+        debye_dd.resize(size_t(ne));
+        debye_cb.resize(size_t(ne));
+#pragma omp parallel for schedule(static)
+        for (long long q = 0; q < ne; ++q) {
+            const auto& d = sim.debye_edges[size_t(q)];
+            debye_f[size_t(q)] = (long long)d.comp * cs + dev(d.id);
+            debye_dd[size_t(q)] = float(d.dd);
+            debye_cb[size_t(q)] = sim.cb(d.comp, d.id);
+        }
+    }
+    s->n_debye = int(debye_f.size());
     // size the arena
     const size_t fields = size_t(3 * cs);
     size_t need = 0;
@@ -1543,7 +1599,7 @@ int session_new(Gpu* gpu, const HostSim& sim, const RunSpec& rs, Session** out, 
                 std::memcpy(d, in, n2 * 4);
             }
         }
-        FG_CUDA(cudaMemcpyAsync(s->node_class, narrow.data(), narrow.size(), cudaMemcpyHostToDevice, st));
+        FG_CUDA(cudaError_t(staged_upload(s->gpu, s->node_class, narrow.data(), narrow.size(), st)));
         s->h2d_bytes += narrow.size();
         FG_CUDA(cudaStreamSynchronize(st));
     }
@@ -1577,7 +1633,7 @@ int session_new(Gpu* gpu, const HostSim& sim, const RunSpec& rs, Session** out, 
     s->h2d_bytes += ncls * sizeof(DevCoef) + axes.size() * sizeof(AxisNode);
     auto up = [&](void* dst, const void* srcp, size_t bytes) -> int {
         s->h2d_bytes += bytes;
-        if (bytes) FG_CUDA(cudaMemcpyAsync(dst, srcp, bytes, cudaMemcpyHostToDevice, st));
+        if (bytes) FG_CUDA(cudaError_t(staged_upload(s->gpu, dst, srcp, bytes, st)));
         return FG_OK;
     };
     int rc = FG_OK;

@@ -40,7 +40,16 @@ struct Session;
 struct Gpu {
     int device = 0;
     std::string name;
+    // pinned staging for host-to-device uploads (allocated on the first large upload): a copy goes
+    // through the two buffers in turn, so filling one overlaps the transfer of the other
+    void* stage[2] = {nullptr, nullptr};
+    void* stage_ev[2] = {nullptr, nullptr};   // cudaEvent_t: the last transfer out of each buffer
 };
+
+// Copies `bytes` from pageable host memory to the device through the Gpu's pinned staging buffers
+// (OpenMP copies into them, the transfers overlap the next copy); on return the source may be
+// reused. Small copies go straight. Returns a cudaError_t as int.
+int staged_upload(Gpu* g, void* dst, const void* src, size_t bytes, void* stream);
 
 int gpu_open(int device, Gpu** out, std::string& err);
 void gpu_close(Gpu* g);

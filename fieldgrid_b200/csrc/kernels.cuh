@@ -229,6 +229,15 @@ __global__ void k_debye_slots(const long long* __restrict__ f, const unsigned* _
     for (int k = 0; k < np; ++k) s_out[b + k] = table[1 + 2 * k] * s_in[b + k] + w * table[2 + 2 * k] * de;
 }
 
+// Per Debye node (device index), the state index of its first edge: the smallest index among the
+// node's edges (f = comp * cs + node, sidx = the edge's state index); dbase starts at all ones.
+__global__ void k_debye_base(const long long* __restrict__ f, const unsigned* __restrict__ sidx, long long count,
+                             long long cs, unsigned* __restrict__ dbase) {
+    const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= count) return;
+    atomicMin(dbase + (f[q] % cs), sidx[q]);
+}
+
 // cpu.rs:262-265
 __device__ __forceinline__ float pulse_at(const StepConst& sc, float t) {
     float x = (t - sc.t0) / sc.tau;

@@ -257,6 +257,111 @@ __device__ __forceinline__ CoefRef coef_of(const TmaArgs& a, const float* lt, un
     return c;
 }
 
+// Pairs of f32 in one instruction (sm_100's packed FP32: add/sub/mul .rn .f32x2). Each lane of the
+// pair is rounded as the scalar operation would be (round to nearest, never fused), so a pair update
+// gives the scalar update's bits.
+namespace f2 {
+__device__ __forceinline__ float2 add(float2 a, float2 b) {
+    float2 d;
+    asm("{\n\t.reg .b64 ra, rb, rd;\n\tmov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t"
+        "add.rn.f32x2 rd, ra, rb;\n\tmov.b64 {%0, %1}, rd;\n\t}"
+        : "=f"(d.x), "=f"(d.y) : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+    return d;
+}
+__device__ __forceinline__ float2 sub(float2 a, float2 b) {
+    float2 d;
+    asm("{\n\t.reg .b64 ra, rb, rd;\n\tmov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t"
+        "sub.rn.f32x2 rd, ra, rb;\n\tmov.b64 {%0, %1}, rd;\n\t}"
+        : "=f"(d.x), "=f"(d.y) : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+    return d;
+}
+__device__ __forceinline__ float2 mul(float2 a, float2 b) {
+    float2 d;
+    asm("{\n\t.reg .b64 ra, rb, rd;\n\tmov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t"
+        "mul.rn.f32x2 rd, ra, rb;\n\tmov.b64 {%0, %1}, rd;\n\t}"
+        : "=f"(d.x), "=f"(d.y) : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+    return d;
+}
+__device__ __forceinline__ float2 bc(float v) { return make_float2(v, v); }
+__device__ __forceinline__ float2 pick(bool px, bool py, float2 n, float2 o) {
+    return make_float2(px ? n.x : o.x, py ? n.y : o.y);
+}
+}  // namespace f2
+
+// The pair's E around its H updates: own (x, y, z), +j (zj, xj), +k (yk, xk: the columns c + 1 and
+// c + 2), +i (zi, yi).
+struct EPair {
+    float2 x, y, z, zj, xj, yk, xk, zi, yi;
+};
+
+// The k-layer CPML terms of one column of a pair (z_terms on a single point, fed by the pair's t).
+template <int F>
+__device__ __forceinline__ void z_col(const TmaArgs& a, const AxisNode& ak, float d01, float d10, float& t01,
+                                      float& t10, bool run0, bool run1, const float* zrow, int zc, int i, int j,
+                                      bool own) {
+    float d[3][2] = {{0.f, d01}, {d10, 0.f}, {0.f, 0.f}};
+    float t[3][2] = {{0.f, t01}, {t10, 0.f}, {0.f, 0.f}};
+    z_terms<F>(a, ak, d, t, run0, run1, zrow, zc, i, j, own);
+    t01 = t[0][1];
+    t10 = t[1][0];
+}
+
+// New H of a column pair outside the CPML (h_node on both columns at once); dk, kn per column.
+template <bool ZL>
+__device__ __forceinline__ void h_pair(const TmaArgs& a, const EPair& n, float2& hx, float2& hy, float2& hz, float di,
+                                       float dj, float2 dk, bool jn, bool kn0, bool kn1, bool in, bool live1,
+                                       const AxisNode* ak0, const AxisNode* ak1, const float* zrow, int zc, int i,
+                                       int j, bool own) {
+    using namespace f2;
+    const float2 d00 = sub(n.zj, n.z), d01 = sub(n.yk, n.y);
+    const float2 d10 = sub(n.xk, n.x), d11 = sub(n.zi, n.z);
+    const float2 d20 = sub(n.yi, n.y), d21 = sub(n.xj, n.x);
+    float2 t00 = mul(d00, bc(dj)), t01 = mul(d01, dk);
+    float2 t10 = mul(d10, dk), t11 = mul(d11, bc(di));
+    const float2 t20 = mul(d20, bc(di)), t21 = mul(d21, bc(dj));
+    if constexpr (ZL) {
+        z_col<1>(a, *ak0, d01.x, d10.x, t01.x, t10.x, jn && kn0, kn0 && in, zrow, zc, i, j, own);
+        if (live1) z_col<1>(a, *ak1, d01.y, d10.y, t01.y, t10.y, jn && kn1, kn1 && in, zrow, zc, i, j, own);
+    }
+    const float2 km = bc(a.k_mu);
+    const float2 nx = sub(hx, mul(km, sub(t00, t01)));
+    const float2 ny = sub(hy, mul(km, sub(t10, t11)));
+    const float2 nz = sub(hz, mul(km, sub(t20, t21)));
+    hx = pick(jn && kn0, jn && kn1 && live1, nx, hx);
+    hy = pick(kn0 && in, kn1 && in && live1, ny, hy);
+    hz = pick(in && jn, in && jn && live1, nz, hz);
+}
+
+// New E of a column pair outside the CPML (e_node on both columns); hj: H at j - 1, hk: H at k - 1
+// (columns c - 1 and c), p: H of plane i - 1.
+template <bool ZL>
+__device__ __forceinline__ void e_pair(const TmaArgs& a, const CoefRef& c0, const CoefRef& c1, float2& ex, float2& ey,
+                                       float2& ez, float2 hx, float2 hy, float2 hz, float2 hzj, float2 hxj, float2 hyk,
+                                       float2 hxk, float2 py, float2 pz, float ei, float ej, float2 ek, int i, int j,
+                                       int k, bool live1, const AxisNode* ak0, const AxisNode* ak1, const float* zrow,
+                                       int zc) {
+    using namespace f2;
+    const float2 d00 = sub(hz, hzj), d01 = sub(hy, hyk);
+    const float2 d10 = sub(hx, hxk), d11 = sub(hz, pz);
+    const float2 d20 = sub(hy, py), d21 = sub(hx, hxj);
+    float2 t00 = mul(d00, bc(ej)), t01 = mul(d01, ek);
+    float2 t10 = mul(d10, ek), t11 = mul(d11, bc(ei));
+    const float2 t20 = mul(d20, bc(ei)), t21 = mul(d21, bc(ej));
+    const bool r00 = c0.cb[0] != 0.0f && j > 0 && k > 0, r01 = live1 && c1.cb[0] != 0.0f && j > 0;
+    const bool r10 = c0.cb[1] != 0.0f && k > 0 && i > 0, r11 = live1 && c1.cb[1] != 0.0f && i > 0;
+    const bool r20 = c0.cb[2] != 0.0f && i > 0 && j > 0, r21 = live1 && c1.cb[2] != 0.0f && i > 0 && j > 0;
+    if constexpr (ZL) {
+        z_col<0>(a, *ak0, d01.x, d10.x, t01.x, t10.x, r00, r10, zrow, zc, i, j, true);
+        if (live1) z_col<0>(a, *ak1, d01.y, d10.y, t01.y, t10.y, r01, r11, zrow, zc, i, j, true);
+    }
+    const float2 nx = add(mul(make_float2(c0.ca[0], c1.ca[0]), ex), mul(make_float2(c0.cb[0], c1.cb[0]), sub(t00, t01)));
+    const float2 ny = add(mul(make_float2(c0.ca[1], c1.ca[1]), ey), mul(make_float2(c0.cb[1], c1.cb[1]), sub(t10, t11)));
+    const float2 nz = add(mul(make_float2(c0.ca[2], c1.ca[2]), ez), mul(make_float2(c0.cb[2], c1.cb[2]), sub(t20, t21)));
+    ex = pick(r00, r01, nx, ex);
+    ey = pick(r10, r11, ny, ey);
+    ez = pick(r20, r21, nz, ez);
+}
+
 // The fused step on the clean box: every point a block computes (its tile, halo row j0-1, halo
 // column k0-1 and halo plane i0-1) lies outside the CPML, so no psi term appears; the absorbing
 // shell around the box is updated by the shell kernels (stencil_shell.cuh).
@@ -376,7 +481,11 @@ __device__ __forceinline__ void tma_march(const CUtensorMap& map_e, const CUtens
     const int xeo = (xr + 1) * L::EW + xc + 4, xho = (xr + 1) * L::HW + xc + 4, xno = (xr + 1) * L::NW + xc + 2;
     const unsigned xgoff = unsigned(min(xj, g.n1 - 1)) * unsigned(g.p2) + unsigned(max(xk, 0));
 
-    float py0 = 0.f, pz0 = 0.f, py1 = 0.f, pz1 = 0.f, pyx = 0.f, pzx = 0.f;  // H of plane i-1
+    // the pair's axis factors, kept in registers (the i factors are read per plane)
+    const float dj = rj->inv_d, ej = rj->inv_dd;
+    const float2 dk2 = make_float2(q0.ak->inv_d, q1.ak->inv_d), ek2 = make_float2(q0.ak->inv_dd, q1.ak->inv_dd);
+    float2 pyp = make_float2(0.f, 0.f), pzp = make_float2(0.f, 0.f);   // the pair's H of plane i-1
+    float pyx = 0.f, pzx = 0.f;                                         // warp 0's extra point's
     bool bad = false;
     for (int p = p_first; p < i1; ++p) {
         const int u = p - p_first;
@@ -399,37 +508,34 @@ __device__ __forceinline__ void tma_march(const CUtensorMap& map_e, const CUtens
         const long long plane = (long long)i * g.n1 * g.p2;
         const bool own = own_row && !pre;
 
-        // 1. new H: the pair (two columns), and warp 0's extra point
-        ENb nb0, nb1;
-        float hx0 = 0.f, hy0 = 0.f, hz0 = 0.f, hx1 = 0.f, hy1 = 0.f, hz1 = 0.f;
+        // 1. new H: the pair (two columns, one packed update), and warp 0's extra point
+        EPair nb{};
+        float2 hxp = make_float2(0.f, 0.f), hyp = hxp, hzp = hxp;
         if (live0) {
-            const float2 x = *reinterpret_cast<const float2*>(E + eo);
-            const float2 y = *reinterpret_cast<const float2*>(E + EC + eo);
-            const float2 z = *reinterpret_cast<const float2*>(E + 2 * EC + eo);
-            const float2 zj = *reinterpret_cast<const float2*>(E + 2 * EC + eo + L::EW);
-            const float2 xj = *reinterpret_cast<const float2*>(E + eo + L::EW);
-            const float2 zi = *reinterpret_cast<const float2*>(E1 + 2 * EC + eo);
-            const float2 yi = *reinterpret_cast<const float2*>(E1 + EC + eo);
-            const float y2 = E[EC + eo + 2], x2 = E[eo + 2];
-            nb0 = ENb{x.x, y.x, z.x, zj.x, xj.x, y.y, x.y, zi.x, yi.x};
-            nb1 = ENb{x.y, y.y, z.y, zj.y, xj.y, y2, x2, zi.y, yi.y};
-            const float2 hx = *reinterpret_cast<const float2*>(H + ho);
-            const float2 hy = *reinterpret_cast<const float2*>(H + HC + ho);
-            const float2 hz = *reinterpret_cast<const float2*>(H + 2 * HC + ho);
-            hx0 = hx.x; hy0 = hy.x; hz0 = hz.x;
-            hx1 = hx.y; hy1 = hy.y; hz1 = hz.y;
+            nb.x = *reinterpret_cast<const float2*>(E + eo);
+            nb.y = *reinterpret_cast<const float2*>(E + EC + eo);
+            nb.z = *reinterpret_cast<const float2*>(E + 2 * EC + eo);
+            nb.zj = *reinterpret_cast<const float2*>(E + 2 * EC + eo + L::EW);
+            nb.xj = *reinterpret_cast<const float2*>(E + eo + L::EW);
+            nb.zi = *reinterpret_cast<const float2*>(E1 + 2 * EC + eo);
+            nb.yi = *reinterpret_cast<const float2*>(E1 + EC + eo);
+            nb.yk = make_float2(nb.y.y, E[EC + eo + 2]);
+            nb.xk = make_float2(nb.x.y, E[eo + 2]);
+            hxp = *reinterpret_cast<const float2*>(H + ho);
+            hyp = *reinterpret_cast<const float2*>(H + HC + ho);
+            hzp = *reinterpret_cast<const float2*>(H + 2 * HC + ho);
             const float* zr = ZL ? ZH + (r + 1) * g.pw : nullptr;
-            h_node<ZL>(a, nb0, hx0, hy0, hz0, q0, ai, in, zr, zc, i, jj, own);
-            if (live1) h_node<ZL>(a, nb1, hx1, hy1, hz1, q1, ai, in, zr, zc, i, jj, own);
-            *reinterpret_cast<float2*>(hn + no) = make_float2(hx0, hx1);
-            *reinterpret_cast<float2*>(hn + NC + no) = make_float2(hy0, hy1);
-            *reinterpret_cast<float2*>(hn + 2 * NC + no) = make_float2(hz0, hz1);
+            h_pair<ZL>(a, nb, hxp, hyp, hzp, ai.inv_d, dj, dk2, q0.jn, q0.kn, q1.kn, in, live1, q0.ak, q1.ak, zr, zc, i,
+                       jj, own);
+            *reinterpret_cast<float2*>(hn + no) = hxp;
+            *reinterpret_cast<float2*>(hn + NC + no) = hyp;
+            *reinterpret_cast<float2*>(hn + 2 * NC + no) = hzp;
             if (own) {
                 // a dead second column is padding past n2 and stays zero
                 float* o = a.h_out + plane + goff;
-                *reinterpret_cast<float2*>(o) = make_float2(hx0, live1 ? hx1 : 0.f);
-                *reinterpret_cast<float2*>(o + g.cs) = make_float2(hy0, live1 ? hy1 : 0.f);
-                *reinterpret_cast<float2*>(o + 2 * g.cs) = make_float2(hz0, live1 ? hz1 : 0.f);
+                *reinterpret_cast<float2*>(o) = make_float2(hxp.x, live1 ? hxp.y : 0.f);
+                *reinterpret_cast<float2*>(o + g.cs) = make_float2(hyp.x, live1 ? hyp.y : 0.f);
+                *reinterpret_cast<float2*>(o + 2 * g.cs) = make_float2(hzp.x, live1 ? hzp.y : 0.f);
             }
         }
         ENb nx;
@@ -475,24 +581,20 @@ __device__ __forceinline__ void tma_march(const CUtensorMap& map_e, const CUtens
                     id1 = CL[r * L::CW + c + 1];
                 }
                 const CoefRef cf0 = coef_of<LOCAL>(a, lt, id0);
+                const CoefRef cf1 = coef_of<LOCAL>(a, lt, live1 ? id1 : id0);
                 const float2 hzj = *reinterpret_cast<const float2*>(hn + 2 * NC + no - L::NW);
                 const float2 hxj = *reinterpret_cast<const float2*>(hn + no - L::NW);
-                const float hyk = hn[NC + no - 1], hxk = hn[no - 1];
-                float ex0 = nb0.x, ey0 = nb0.y, ez0 = nb0.z;
+                const float2 hyk = make_float2(hn[NC + no - 1], hyp.x), hxk = make_float2(hn[no - 1], hxp.x);
+                // a dead second column keeps E = 0
+                float2 ex = make_float2(nb.x.x, live1 ? nb.x.y : 0.f), ey = make_float2(nb.y.x, live1 ? nb.y.y : 0.f);
+                float2 ez = make_float2(nb.z.x, live1 ? nb.z.y : 0.f);
                 const float* ze = ZL ? ZE + (r + 1) * g.pw : nullptr;
-                e_node<ZL>(a, cf0, ex0, ey0, ez0, hx0, hy0, hz0, hzj.x, hxj.x, hyk, hxk, py0, pz0, q0, ai, i, jj, kk, ze,
-                           zc);
-                float ex1 = 0.f, ey1 = 0.f, ez1 = 0.f;
-                if (live1) {
-                    const CoefRef cf1 = coef_of<LOCAL>(a, lt, id1);
-                    ex1 = nb1.x; ey1 = nb1.y; ez1 = nb1.z;
-                    e_node<ZL>(a, cf1, ex1, ey1, ez1, hx1, hy1, hz1, hzj.y, hxj.y, hy0, hx0, py1, pz1, q1, ai, i, jj,
-                               kk + 1, ze, zc);
-                }
+                e_pair<ZL>(a, cf0, cf1, ex, ey, ez, hxp, hyp, hzp, hzj, hxj, hyk, hxk, pyp, pzp, ai.inv_dd, ej, ek2, i,
+                           jj, kk, live1, q0.ak, q1.ak, ze, zc);
                 float* o = a.e_out + plane + goff;
-                *reinterpret_cast<float2*>(o) = make_float2(ex0, ex1);
-                *reinterpret_cast<float2*>(o + g.cs) = make_float2(ey0, ey1);
-                *reinterpret_cast<float2*>(o + 2 * g.cs) = make_float2(ez0, ez1);
+                *reinterpret_cast<float2*>(o) = ex;
+                *reinterpret_cast<float2*>(o + g.cs) = ey;
+                *reinterpret_cast<float2*>(o + 2 * g.cs) = ez;
             }
             if (xown) {
                 const CoefRef cf = coef_of<LOCAL>(a, lt, CL[xr * L::CW + xc]);
@@ -506,7 +608,7 @@ __device__ __forceinline__ void tma_march(const CUtensorMap& map_e, const CUtens
                 o[2 * g.cs] = ez;
             }
         }
-        py0 = hy0; pz0 = hz0; py1 = hy1; pz1 = hz1; pyx = hyx; pzx = hzx;
+        pyp = hyp; pzp = hzp; pyx = hyx; pzx = hzx;
         tma::mbar_arrive(&empty[s]);
     }
     // the last plane's stage (E(i1)) was waited on by the final iteration; nothing is in flight

@@ -543,7 +543,7 @@ void plan_tma(Session& s) {
 int launch_tma(Session& s, int parity, float* e_out, float* h_out, float* psi_h_out) {
     const TmaPlan& t = s.tma;
     TmaArgs a{s.geom, s.classes, e_out, h_out, s.sc.k_mu, s.clean_lo[2], s.clean_hi[1], s.clean_hi[2], s.tma_blocks,
-              s.tma_own, 0, 1, s.psi, psi_h_out, s.tables, s.counter, s.error, s.wait_ns, s.stall_plane};
+              s.tma_own, 0, 1, s.psi, psi_h_out, s.tables, s.counter, s.error, s.wait_ns, -0.0f, s.stall_plane};
     // without k-layer tiles the last two maps are never read
     const CUtensorMap& pze = t.pz ? t.pze : t.c;
     const CUtensorMap& pzh = t.pz ? t.pzh[parity] : t.c;
@@ -979,7 +979,7 @@ void launch_tma_slots(Session& s, bool all, int a, int b, cudaStream_t st) {
     float* H[3] = {s.h, s.h2, s.h3};
     TmaArgs args{s.geom, s.classes, E[b], H[b], s.sc.k_mu, s.clean_lo[2], s.clean_hi[1], s.clean_hi[2],
                  all ? s.tma_blocks : s.c_blocks, all ? s.tma_own : s.c_own, 0, 1, s.zslot[b], s.zslot[b],
-                 all ? s.tables : s.c_tables, s.counter, s.error, s.wait_ns, s.stall_plane};
+                 all ? s.tables : s.c_tables, s.counter, s.error, s.wait_ns, -0.0f, s.stall_plane};
     const unsigned nb = unsigned(all ? s.tma.blocks : s.n_cblocks);
     with_tma_kernel(s.cid_bytes, s.local, s.tma.shape, [&](auto kern, int smem) {
         kern<<<nb, TMA_CONSUMERS + 32, smem, st>>>(s.d1_e[a], s.d1_h[a], s.tma.c, s.d1_pze[a], s.d1_pzh[a], args);

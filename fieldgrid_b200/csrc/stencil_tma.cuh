@@ -151,6 +151,7 @@ struct TmaArgs {
     unsigned* counter;
     int* error;
     unsigned long long wait_ns;          // the limit of every mbarrier wait (2 s in normal runs)
+    float neg0;                          // -0.0f (the packed products' addend, see f2::mul)
     int stall_plane;                     // test knob, -1 in normal runs: the full barrier of this
                                          // plane expects 16 bytes more than its copies deliver, so
                                          // the waits on it run out (the failure path under test)
@@ -257,9 +258,9 @@ __device__ __forceinline__ CoefRef coef_of(const TmaArgs& a, const float* lt, un
     return c;
 }
 
-// Pairs of f32 in one instruction (sm_100's packed FP32: add/sub/mul .rn .f32x2). Each lane of the
-// pair is rounded as the scalar operation would be (round to nearest, never fused), so a pair update
-// gives the scalar update's bits.
+// Pairs of f32 in one instruction (sm_100's packed FP32: add/sub .rn .f32x2 and products as a fused
+// multiply-add of -0). Each lane of the pair is rounded as the scalar operation would be (round to
+// nearest, never fused with another operation), so a pair update gives the scalar update's bits.
 namespace f2 {
 __device__ __forceinline__ float2 add(float2 a, float2 b) {
     float2 d;
@@ -275,11 +276,16 @@ __device__ __forceinline__ float2 sub(float2 a, float2 b) {
         : "=f"(d.x), "=f"(d.y) : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
     return d;
 }
-__device__ __forceinline__ float2 mul(float2 a, float2 b) {
+// The product as fma(a, b, z) with z = (-0, -0): one rounding, the product's own (x + (-0) = x for
+// every x, signed zeros included). The assembler contracts a packed mul.rn with a following packed
+// add or sub into one fused operation (one rounding where the scalar path rounds twice), and it
+// would drop a literal -0 addend and contract again; z therefore comes from a kernel argument, whose
+// value it cannot see, and the product stays a fused operation of its own.
+__device__ __forceinline__ float2 mul(float2 a, float2 b, float2 z) {
     float2 d;
-    asm("{\n\t.reg .b64 ra, rb, rd;\n\tmov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t"
-        "mul.rn.f32x2 rd, ra, rb;\n\tmov.b64 {%0, %1}, rd;\n\t}"
-        : "=f"(d.x), "=f"(d.y) : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+    asm("{\n\t.reg .b64 ra, rb, rz, rd;\n\tmov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t"
+        "mov.b64 rz, {%6, %7};\n\tfma.rn.f32x2 rd, ra, rb, rz;\n\tmov.b64 {%0, %1}, rd;\n\t}"
+        : "=f"(d.x), "=f"(d.y) : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y), "f"(z.x), "f"(z.y));
     return d;
 }
 __device__ __forceinline__ float2 bc(float v) { return make_float2(v, v); }
@@ -308,7 +314,7 @@ __device__ __forceinline__ void z_col(const TmaArgs& a, const AxisNode& ak, floa
 
 // New H of a column pair outside the CPML (h_node on both columns at once); dk, kn per column.
 template <bool ZL>
-__device__ __forceinline__ void h_pair(const TmaArgs& a, const EPair& n, float2& hx, float2& hy, float2& hz, float di,
+__device__ __forceinline__ void h_pair(const TmaArgs& a, float2 mz, const EPair& n, float2& hx, float2& hy, float2& hz, float di,
                                        float dj, float2 dk, bool jn, bool kn0, bool kn1, bool in, bool live1,
                                        const AxisNode* ak0, const AxisNode* ak1, const float* zrow, int zc, int i,
                                        int j, bool own) {
@@ -316,17 +322,17 @@ __device__ __forceinline__ void h_pair(const TmaArgs& a, const EPair& n, float2&
     const float2 d00 = sub(n.zj, n.z), d01 = sub(n.yk, n.y);
     const float2 d10 = sub(n.xk, n.x), d11 = sub(n.zi, n.z);
     const float2 d20 = sub(n.yi, n.y), d21 = sub(n.xj, n.x);
-    float2 t00 = mul(d00, bc(dj)), t01 = mul(d01, dk);
-    float2 t10 = mul(d10, dk), t11 = mul(d11, bc(di));
-    const float2 t20 = mul(d20, bc(di)), t21 = mul(d21, bc(dj));
+    float2 t00 = mul(d00, bc(dj), mz), t01 = mul(d01, dk, mz);
+    float2 t10 = mul(d10, dk, mz), t11 = mul(d11, bc(di), mz);
+    const float2 t20 = mul(d20, bc(di), mz), t21 = mul(d21, bc(dj), mz);
     if constexpr (ZL) {
         z_col<1>(a, *ak0, d01.x, d10.x, t01.x, t10.x, jn && kn0, kn0 && in, zrow, zc, i, j, own);
         if (live1) z_col<1>(a, *ak1, d01.y, d10.y, t01.y, t10.y, jn && kn1, kn1 && in, zrow, zc, i, j, own);
     }
     const float2 km = bc(a.k_mu);
-    const float2 nx = sub(hx, mul(km, sub(t00, t01)));
-    const float2 ny = sub(hy, mul(km, sub(t10, t11)));
-    const float2 nz = sub(hz, mul(km, sub(t20, t21)));
+    const float2 nx = sub(hx, mul(km, sub(t00, t01), mz));
+    const float2 ny = sub(hy, mul(km, sub(t10, t11), mz));
+    const float2 nz = sub(hz, mul(km, sub(t20, t21), mz));
     hx = pick(jn && kn0, jn && kn1 && live1, nx, hx);
     hy = pick(kn0 && in, kn1 && in && live1, ny, hy);
     hz = pick(in && jn, in && jn && live1, nz, hz);
@@ -335,7 +341,7 @@ __device__ __forceinline__ void h_pair(const TmaArgs& a, const EPair& n, float2&
 // New E of a column pair outside the CPML (e_node on both columns); hj: H at j - 1, hk: H at k - 1
 // (columns c - 1 and c), p: H of plane i - 1.
 template <bool ZL>
-__device__ __forceinline__ void e_pair(const TmaArgs& a, const CoefRef& c0, const CoefRef& c1, float2& ex, float2& ey,
+__device__ __forceinline__ void e_pair(const TmaArgs& a, float2 mz, const CoefRef& c0, const CoefRef& c1, float2& ex, float2& ey,
                                        float2& ez, float2 hx, float2 hy, float2 hz, float2 hzj, float2 hxj, float2 hyk,
                                        float2 hxk, float2 py, float2 pz, float ei, float ej, float2 ek, int i, int j,
                                        int k, bool live1, const AxisNode* ak0, const AxisNode* ak1, const float* zrow,
@@ -344,9 +350,9 @@ __device__ __forceinline__ void e_pair(const TmaArgs& a, const CoefRef& c0, cons
     const float2 d00 = sub(hz, hzj), d01 = sub(hy, hyk);
     const float2 d10 = sub(hx, hxk), d11 = sub(hz, pz);
     const float2 d20 = sub(hy, py), d21 = sub(hx, hxj);
-    float2 t00 = mul(d00, bc(ej)), t01 = mul(d01, ek);
-    float2 t10 = mul(d10, ek), t11 = mul(d11, bc(ei));
-    const float2 t20 = mul(d20, bc(ei)), t21 = mul(d21, bc(ej));
+    float2 t00 = mul(d00, bc(ej), mz), t01 = mul(d01, ek, mz);
+    float2 t10 = mul(d10, ek, mz), t11 = mul(d11, bc(ei), mz);
+    const float2 t20 = mul(d20, bc(ei), mz), t21 = mul(d21, bc(ej), mz);
     const bool r00 = c0.cb[0] != 0.0f && j > 0 && k > 0, r01 = live1 && c1.cb[0] != 0.0f && j > 0;
     const bool r10 = c0.cb[1] != 0.0f && k > 0 && i > 0, r11 = live1 && c1.cb[1] != 0.0f && i > 0;
     const bool r20 = c0.cb[2] != 0.0f && i > 0 && j > 0, r21 = live1 && c1.cb[2] != 0.0f && i > 0 && j > 0;
@@ -354,9 +360,9 @@ __device__ __forceinline__ void e_pair(const TmaArgs& a, const CoefRef& c0, cons
         z_col<0>(a, *ak0, d01.x, d10.x, t01.x, t10.x, r00, r10, zrow, zc, i, j, true);
         if (live1) z_col<0>(a, *ak1, d01.y, d10.y, t01.y, t10.y, r01, r11, zrow, zc, i, j, true);
     }
-    const float2 nx = add(mul(make_float2(c0.ca[0], c1.ca[0]), ex), mul(make_float2(c0.cb[0], c1.cb[0]), sub(t00, t01)));
-    const float2 ny = add(mul(make_float2(c0.ca[1], c1.ca[1]), ey), mul(make_float2(c0.cb[1], c1.cb[1]), sub(t10, t11)));
-    const float2 nz = add(mul(make_float2(c0.ca[2], c1.ca[2]), ez), mul(make_float2(c0.cb[2], c1.cb[2]), sub(t20, t21)));
+    const float2 nx = add(mul(make_float2(c0.ca[0], c1.ca[0]), ex, mz), mul(make_float2(c0.cb[0], c1.cb[0]), sub(t00, t01), mz));
+    const float2 ny = add(mul(make_float2(c0.ca[1], c1.ca[1]), ey, mz), mul(make_float2(c0.cb[1], c1.cb[1]), sub(t10, t11), mz));
+    const float2 nz = add(mul(make_float2(c0.ca[2], c1.ca[2]), ez, mz), mul(make_float2(c0.cb[2], c1.cb[2]), sub(t20, t21), mz));
     ex = pick(r00, r01, nx, ex);
     ey = pick(r10, r11, ny, ey);
     ez = pick(r20, r21, nz, ez);
@@ -485,6 +491,7 @@ __device__ __forceinline__ void tma_march(const CUtensorMap& map_e, const CUtens
     const float dj = rj->inv_d, ej = rj->inv_dd;
     const float2 dk2 = make_float2(q0.ak->inv_d, q1.ak->inv_d), ek2 = make_float2(q0.ak->inv_dd, q1.ak->inv_dd);
     float2 pyp = make_float2(0.f, 0.f), pzp = make_float2(0.f, 0.f);   // the pair's H of plane i-1
+    const float2 mz = make_float2(a.neg0, a.neg0);
     float pyx = 0.f, pzx = 0.f;                                         // warp 0's extra point's
     bool bad = false;
     for (int p = p_first; p < i1; ++p) {
@@ -525,7 +532,7 @@ __device__ __forceinline__ void tma_march(const CUtensorMap& map_e, const CUtens
             hyp = *reinterpret_cast<const float2*>(H + HC + ho);
             hzp = *reinterpret_cast<const float2*>(H + 2 * HC + ho);
             const float* zr = ZL ? ZH + (r + 1) * g.pw : nullptr;
-            h_pair<ZL>(a, nb, hxp, hyp, hzp, ai.inv_d, dj, dk2, q0.jn, q0.kn, q1.kn, in, live1, q0.ak, q1.ak, zr, zc, i,
+            h_pair<ZL>(a, mz, nb, hxp, hyp, hzp, ai.inv_d, dj, dk2, q0.jn, q0.kn, q1.kn, in, live1, q0.ak, q1.ak, zr, zc, i,
                        jj, own);
             *reinterpret_cast<float2*>(hn + no) = hxp;
             *reinterpret_cast<float2*>(hn + NC + no) = hyp;
@@ -589,7 +596,7 @@ __device__ __forceinline__ void tma_march(const CUtensorMap& map_e, const CUtens
                 float2 ex = make_float2(nb.x.x, live1 ? nb.x.y : 0.f), ey = make_float2(nb.y.x, live1 ? nb.y.y : 0.f);
                 float2 ez = make_float2(nb.z.x, live1 ? nb.z.y : 0.f);
                 const float* ze = ZL ? ZE + (r + 1) * g.pw : nullptr;
-                e_pair<ZL>(a, cf0, cf1, ex, ey, ez, hxp, hyp, hzp, hzj, hxj, hyk, hxk, pyp, pzp, ai.inv_dd, ej, ek2, i,
+                e_pair<ZL>(a, mz, cf0, cf1, ex, ey, ez, hxp, hyp, hzp, hzj, hxj, hyk, hxk, pyp, pzp, ai.inv_dd, ej, ek2, i,
                            jj, kk, live1, q0.ak, q1.ak, ze, zc);
                 float* o = a.e_out + plane + goff;
                 *reinterpret_cast<float2*>(o) = ex;

@@ -1,8 +1,10 @@
 // The C ABI of include/fieldgrid.h. Thin: argument checks, error texts, and the run loop of
 // run.rs:681-757 (chunks of check_every steps, energy check, decay, progress, early stop) on top of
 // the device session.
+#include <chrono>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <string>
@@ -44,6 +46,26 @@ RunSpec run_spec(uint64_t driven, const fg_pulse* pulse, const fg_extras* x) {
 struct Far {
     std::vector<double> pos, area, jm;  // jm: 12 doubles per patch (J then M, re/im, x y z)
     double freq = 0;
+};
+
+// FIELDGRID_SETUP_TIMES=1: fg_run prints the wall time of its phases to stderr
+struct RunClock {
+    bool on = false;
+    std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now(), last = t0;
+    std::string text;
+    RunClock() { const char* v = std::getenv("FIELDGRID_SETUP_TIMES"); on = v && v[0] == '1'; }
+    void mark(const char* what) {
+        if (!on) return;
+        const auto now = std::chrono::steady_clock::now();
+        char buf[64];
+        std::snprintf(buf, sizeof buf, " %s %.2f ms;", what, std::chrono::duration<double, std::milli>(now - last).count());
+        text += buf;
+        last = now;
+    }
+    ~RunClock() {
+        if (on) std::fprintf(stderr, "fg_run:%s total %.1f ms\n", text.c_str(),
+                             std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count());
+    }
 };
 
 }  // namespace
@@ -235,12 +257,18 @@ int fg_run(fg_gpu* g, const fg_sim* sim, uint64_t driven, const fg_pulse* pulse,
     *out = nullptr;
     if (!g) return fail(FG_ERR_NO_DEVICE, "no GPU: this engine has no CPU path", err, errlen);
     if (!sim || !pulse || !extras) return fail(FG_ERR_INVALID, "null argument", err, errlen);
+    RunClock clk;
     Session* s = nullptr;
     std::string e;
     RunSpec rs = run_spec(driven, pulse, extras);
     int rc = session_new(g->g, *sim->s, rs, &s, e);
     if (rc) return fail(rc, e, err, errlen);
-    std::unique_ptr<Session, void (*)(Session*)> guard(s, session_free);
+    clk.mark("session_new");
+    struct Free {   // the session goes back before the clock reports
+        RunClock& c;
+        void operator()(Session* x) const { session_free(x); c.mark("free"); }
+    };
+    std::unique_ptr<Session, Free> guard(s, Free{clk});
     // run.rs:681-748
     const uint64_t chunk = extras->check_every == 0 ? 1000 : extras->check_every;
     const uint64_t pulse_end = uint64_t(2.0 * session_t0(s) / sim->s->dt);
@@ -260,6 +288,7 @@ int fg_run(fg_gpu* g, const fg_sim* sim, uint64_t driven, const fg_pulse* pulse,
         if (progress && !progress(user, steps, decay)) return fail(FG_ERR_CANCELLED, "cancelled", err, errlen);
         if (steps > std::max(pulse_end, extras->min_steps) && decay >= extras->decay_db) break;
     }
+    clk.mark("steps");
     auto rec = std::make_unique<fg_record>();
     rec->steps = steps;
     rec->ports = session_ports(s);
@@ -282,6 +311,7 @@ int fg_run(fg_gpu* g, const fg_sim* sim, uint64_t driven, const fg_pulse* pulse,
         rec->has_fields = true;
     }
     if (rc) return fail(rc, e, err, errlen);
+    clk.mark("read");
     rec->h2d = session_h2d_bytes(s);
     rec->d2h = session_d2h_bytes(s);
     // the kernel report steps the session further, so it comes after the record is read

@@ -23,6 +23,7 @@
 #include "stencil_shell.cuh"
 #include "stencil_tma.cuh"
 #include "stencil_tb2.cuh"
+#include "setup_kernels.cuh"
 #include "adjoint_kernels.cuh"
 
 #include <cudaTypedefs.h>
@@ -76,9 +77,11 @@ void gpu_close(Gpu* g) {
 
 static constexpr size_t STAGE_BYTES = size_t(32) << 20;
 
-int staged_upload(Gpu* g, void* dst, const void* src, size_t bytes, void* stream) {
-    cudaStream_t st = static_cast<cudaStream_t>(stream);
-    if (bytes < (size_t(4) << 20)) return int(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st));
+// Host -> device through the two pinned staging buffers: fill(buf, off, n) writes bytes [off,
+// off + n) of the destination's contents into buf; it runs on the host threads (OpenMP, 1 MB
+// parts) while the previous buffer's copy is in flight.
+template <class Fill>
+int staged_fill(Gpu* g, void* dst, size_t bytes, cudaStream_t st, Fill&& fill) {
     for (int b = 0; b < 2; ++b) {
         if (!g->stage[b]) {
             cudaError_t e = cudaHostAlloc(&g->stage[b], STAGE_BYTES, cudaHostAllocDefault);
@@ -89,7 +92,6 @@ int staged_upload(Gpu* g, void* dst, const void* src, size_t bytes, void* stream
             g->stage_ev[b] = ev;
         }
     }
-    const char* s8 = static_cast<const char*>(src);
     char* d8 = static_cast<char*>(dst);
     int b = 0;
     for (size_t off = 0; off < bytes; off += STAGE_BYTES, b ^= 1) {
@@ -102,7 +104,7 @@ int staged_upload(Gpu* g, void* dst, const void* src, size_t bytes, void* stream
 #pragma omp parallel for schedule(static)
         for (long long q = 0; q < parts; ++q) {
             const size_t a = size_t(q) << 20, m = std::min(size_t(1) << 20, n - a);
-            std::memcpy(buf + a, s8 + off + a, m);
+            fill(buf + a, off + a, m);
         }
         e = cudaMemcpyAsync(d8 + off, buf, n, cudaMemcpyHostToDevice, st);
         if (e != cudaSuccess) return int(e);
@@ -111,6 +113,13 @@ int staged_upload(Gpu* g, void* dst, const void* src, size_t bytes, void* stream
     }
     // the source may be reused as soon as it has been copied into the staging buffers
     return int(cudaSuccess);
+}
+
+int staged_upload(Gpu* g, void* dst, const void* src, size_t bytes, void* stream) {
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (bytes < (size_t(4) << 20)) return int(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st));
+    const char* s8 = static_cast<const char*>(src);
+    return staged_fill(g, dst, bytes, st, [s8](char* buf, size_t off, size_t n) { std::memcpy(buf, s8 + off, n); });
 }
 
 struct Session {
@@ -428,56 +437,6 @@ CleanPlan plan_clean(const HostSim& sim, const Geom& g, bool z_layer, int seg_fi
 // Per block of the TMA step (a TJ x TK tile over one x-segment): the distinct node classes
 // it holds, renumbered from 0, and each node's index into that short list. ok = false when a
 // region holds more than LOCAL_CLASSES classes.
-struct LocalClasses {
-    std::vector<uint8_t> ids;    // device node layout (pitch p2)
-    std::vector<float> tables;   // regions x LOCAL_CLASSES x 6
-    bool ok = true;
-};
-
-LocalClasses build_local(const HostSim& sim, const Geom& g, const CleanPlan& cp) {
-    const std::vector<int4>& blocks = cp.blocks;
-    LocalClasses out;
-    const long long regions = (long long)blocks.size();
-    out.ids.assign(size_t(g.n0) * g.n1 * g.p2, 0);
-    out.tables.assign(size_t(regions) * LOCAL_CLASSES * 6, 0.f);
-    bool over = false;
-    const size_t n1 = g.n1, n2 = g.n2;
-#pragma omp parallel for schedule(dynamic, 8) reduction(|| : over)
-    for (long long r = 0; r < regions; ++r) {
-        if (over) continue;
-        const int4 b = blocks[size_t(r)];
-        const int k0 = b.x & ~TMA_ZL_TILE, j0 = b.y, i0 = b.z, i1 = b.w;
-        const int kbeg = std::max(k0, cp.lo[2]);
-        int kend = std::min(k0 + TMA_TK, cp.hi[2]);
-        if (cp.hi[2] == g.n2 && k0 + TMA_TK == g.n2 - 1) kend = g.n2;  // the owned right-edge column
-        const int jbeg = cp.own[size_t(r)].x, jend = cp.own[size_t(r)].y;
-        uint32_t keys[512];
-        uint16_t vals[512];
-        std::fill(keys, keys + 512, 0xffffffffu);
-        int count = 0;
-        float* tab = out.tables.data() + size_t(r) * LOCAL_CLASSES * 6;
-        (void)j0;
-        for (int i = i0; i < i1 && !over; ++i)
-            for (int j = jbeg; j < jend && !over; ++j)
-                for (int k = kbeg; k < kend; ++k) {
-                    const uint32_t gid = sim.node_class[(size_t(i) * n1 + j) * n2 + k];
-                    uint32_t h = (gid * 2654435761u) & 511u;
-                    while (keys[h] != 0xffffffffu && keys[h] != gid) h = (h + 1) & 511u;
-                    if (keys[h] == 0xffffffffu) {
-                        if (count == LOCAL_CLASSES) { over = true; break; }
-                        keys[h] = gid;
-                        vals[h] = uint16_t(count);
-                        const Coef& cf = sim.classes[gid];
-                        for (int c = 0; c < 3; ++c) { tab[count * 6 + c] = cf.ca[c]; tab[count * 6 + 3 + c] = cf.cb[c]; }
-                        ++count;
-                    }
-                    out.ids[(size_t(i) * n1 + j) * g.p2 + k] = uint8_t(vals[h]);
-                }
-    }
-    out.ok = !over;
-    return out;
-}
-
 // Builds the tensor maps of the TMA step: E and H of both buffer sets, and the class ids.
 void plan_tma(Session& s) {
     TmaPlan& t = s.tma;
@@ -1310,9 +1269,7 @@ int session_new(Gpu* gpu, const HostSim& sim, const RunSpec& rs, Session** out, 
         d.face_b = unsigned(q.faces[1]);
         sheets.push_back(d);
     }
-    // the Debye edge list of the one-step scheme (filled below unless the two-step mode keeps its own)
-    std::vector<long long> debye_f;
-    std::vector<float> debye_dd, debye_cb;
+    // the Debye edge list of the one-step scheme is formed on the device (below)
     std::vector<float> debye_table{float(sim.poles.size())};
     for (auto& [x, a] : sim.poles) {
         double d = 1.0 + 0.5 * x * sim.dt;
@@ -1437,8 +1394,7 @@ int session_new(Gpu* gpu, const HostSim& sim, const RunSpec& rs, Session** out, 
     (void)states;
 
     clk.mark("tables");
-    // per-region class tables for the TMA step (fused runs on sm_100)
-    LocalClasses lc;
+    // per-region class tables for the TMA step (fused runs on sm_100), formed on the device below
     CleanPlan cp;
     SlotPlan sp;
     const bool z_layer = g.pml > 0 && g.pw <= TmaL<float>::PZW;
@@ -1455,26 +1411,13 @@ int session_new(Gpu* gpu, const HostSim& sim, const RunSpec& rs, Session** out, 
                           sim.poles.size() <= size_t(TB_NPMAX) && (g.pml == 0 || z_layer);
         if (want) sp = plan_slots(sim, g, z_layer, special);
         cp = sp.ok ? sp.cp : plan_clean(sim, g, z_layer, rs.tma_seg);
-        if (cp.ok) {
-            lc = build_local(sim, g, cp);
-            s->local = lc.ok;
-        }
+        s->local = cp.ok;
     }
     clk.mark("plans");
-    if (!sp.ok && !sim.debye_edges.empty()) {
-        const long long ne = (long long)sim.debye_edges.size();
-        debye_f.resize(size_t(ne));
-        debye_dd.resize(size_t(ne));
-        debye_cb.resize(size_t(ne));
-#pragma omp parallel for schedule(static)
-        for (long long q = 0; q < ne; ++q) {
-            const auto& d = sim.debye_edges[size_t(q)];
-            debye_f[size_t(q)] = (long long)d.comp * cs + dev(d.id);
-            debye_dd[size_t(q)] = float(d.dd);
-            debye_cb[size_t(q)] = sim.cb(d.comp, d.id);
-        }
-    }
-    s->n_debye = int(debye_f.size());
+    // the one-step Debye list exists in the two-step mode too: its fallback when the slot set-up
+    // does not apply (a region with more classes than a local table)
+    const size_t nd = sim.debye_edges.size();
+    s->n_debye = int(nd);
     // size the arena
     const size_t fields = size_t(3 * cs);
     size_t need = 0;
@@ -1500,15 +1443,18 @@ int session_new(Gpu* gpu, const HostSim& sim, const RunSpec& rs, Session** out, 
     need += carve_size(std::max<size_t>(sheets.size(), 1) * sizeof(DevSheet));
     need += carve_size(std::max<size_t>(sim.sheet_table.size(), 1) * 4);
     need += carve_size(std::max<size_t>(sheets.size() * nr_nc, 1) * 4);
-    need += carve_size(std::max<size_t>(debye_f.size(), 1) * 8);
-    need += carve_size(std::max<size_t>(debye_f.size(), 1) * 4) * 3;
-    need += carve_size(std::max<size_t>(debye_f.size() * sim.poles.size(), 1) * 4);
+    need += carve_size(std::max<size_t>(nd, 1) * 8);
+    need += carve_size(std::max<size_t>(nd, 1) * 4) * 3;
+    need += carve_size(std::max<size_t>(nd * sim.poles.size(), 1) * 4);
+    need += carve_size(std::max<size_t>(nd, 1) * sizeof(DebyeEdge));   // the host records, set-up only
     need += carve_size(debye_table.size() * 4);
     need += carve_size(std::max<size_t>(t_pulse.size(), 1) * 4);
     need += carve_size(std::max<size_t>(t_dft.size(), 1) * 4) * 2;
     need += carve_size(ENERGY_BLOCKS * 8);
     need += carve_size(64);
-    if (s->local) need += carve_size(lc.ids.size()) + carve_size(lc.tables.size() * 4);
+    const size_t local_tables = cp.blocks.size() * LOCAL_CLASSES * 6;
+    if (s->local) need += carve_size(nnp) + carve_size(local_tables * 4);
+    need += carve_size(64);
     need += carve_size(cp.blocks.size() * sizeof(int4));
     need += carve_size(cp.own.size() * sizeof(int2));
     size_t free_b = 0, total_b = 0;
@@ -1519,6 +1465,7 @@ int session_new(Gpu* gpu, const HostSim& sim, const RunSpec& rs, Session** out, 
     }
     FG_CUDA(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
     FG_CUDA(cudaMalloc(&s->arena, need));
+    clk.mark("malloc");
     s->arena_bytes = need;
     char* cur = s->arena;
     s->e = carve<float>(cur, fields);
@@ -1548,11 +1495,12 @@ int session_new(Gpu* gpu, const HostSim& sim, const RunSpec& rs, Session** out, 
     s->sheets = carve<DevSheet>(cur, std::max<size_t>(sheets.size(), 1));
     s->branch = carve<float>(cur, std::max<size_t>(sim.sheet_table.size(), 1));
     s->currents = carve<float>(cur, std::max<size_t>(sheets.size() * nr_nc, 1));
-    s->debye_f = carve<long long>(cur, std::max<size_t>(debye_f.size(), 1));
-    s->debye_dd = carve<float>(cur, std::max<size_t>(debye_f.size(), 1));
-    s->debye_cb = carve<float>(cur, std::max<size_t>(debye_f.size(), 1));
-    s->debye_old = carve<float>(cur, std::max<size_t>(debye_f.size(), 1));
-    s->debye_state = carve<float>(cur, std::max<size_t>(debye_f.size() * sim.poles.size(), 1));
+    s->debye_f = carve<long long>(cur, std::max<size_t>(nd, 1));
+    s->debye_dd = carve<float>(cur, std::max<size_t>(nd, 1));
+    s->debye_cb = carve<float>(cur, std::max<size_t>(nd, 1));
+    s->debye_old = carve<float>(cur, std::max<size_t>(nd, 1));
+    s->debye_state = carve<float>(cur, std::max<size_t>(nd * sim.poles.size(), 1));
+    DebyeEdge* debye_raw = carve<DebyeEdge>(cur, std::max<size_t>(nd, 1));
     s->debye_table = carve<float>(cur, debye_table.size());
     float* d_pulse = carve<float>(cur, std::max<size_t>(t_pulse.size(), 1));
     float* d_dft = carve<float>(cur, std::max<size_t>(t_dft.size(), 1));
@@ -1563,9 +1511,10 @@ int session_new(Gpu* gpu, const HostSim& sim, const RunSpec& rs, Session** out, 
     s->partial = carve<double>(cur, ENERGY_BLOCKS);
     s->error = carve<int>(cur, 16);
     if (s->local) {
-        s->local_ids = carve<uint8_t>(cur, lc.ids.size());
-        s->tables = carve<float>(cur, lc.tables.size());
+        s->local_ids = carve<uint8_t>(cur, nnp);
+        s->tables = carve<float>(cur, local_tables);
     }
+    int* setup_flag = carve<int>(cur, 16);
     if (!cp.blocks.empty()) s->tma_blocks = carve<int4>(cur, cp.blocks.size());
     if (!cp.own.empty()) s->tma_own = carve<int2>(cur, cp.own.size());
     s->tma_plan_blocks = cp.blocks;
@@ -1579,30 +1528,33 @@ int session_new(Gpu* gpu, const HostSim& sim, const RunSpec& rs, Session** out, 
     cudaStream_t st = s->stream;
     clk.mark("alloc");
     FG_CUDA(cudaMemsetAsync(s->arena, 0, need, st));
-    // node classes, narrowed and laid out with the row pitch on the host in parallel
+    // node classes, narrowed and laid out with the row pitch while they are staged for the upload
     {
-        std::vector<uint8_t> narrow(nnp * size_t(s->cid_bytes), 0);
         const uint32_t* src_c = sim.node_class.data();
-        const long long rows = (long long)(n0 * n1);
-        const int cb = s->cid_bytes, p2 = g.p2;
-#pragma omp parallel for schedule(static)
-        for (long long r = 0; r < rows; ++r) {
-            const uint32_t* in = src_c + r * (long long)n2;
-            if (cb == 1) {
-                uint8_t* d = narrow.data() + r * p2;
-                for (size_t k = 0; k < n2; ++k) d[k] = uint8_t(in[k]);
-            } else if (cb == 2) {
-                uint16_t* d = reinterpret_cast<uint16_t*>(narrow.data()) + r * p2;
-                for (size_t k = 0; k < n2; ++k) d[k] = uint16_t(in[k]);
-            } else {
-                uint32_t* d = reinterpret_cast<uint32_t*>(narrow.data()) + r * p2;
-                std::memcpy(d, in, n2 * 4);
+        const int cb = s->cid_bytes;
+        const size_t p2 = size_t(g.p2);
+        auto narrow = [&](char* buf, size_t off, size_t n) {
+            // bytes [off, off + n) of the pitched array: elements off / cb .. (off + n) / cb
+            const size_t e0 = off / size_t(cb), e1 = (off + n) / size_t(cb);
+            size_t e = e0;
+            while (e < e1) {
+                const size_t r = e / p2, k0 = e % p2, kn = std::min(p2, k0 + (e1 - e));
+                const uint32_t* in = src_c + r * n2;
+                char* o = buf + (e - e0) * size_t(cb);
+                for (size_t k = k0; k < kn; ++k) {
+                    const uint32_t v = k < n2 ? in[k] : 0u;
+                    if (cb == 1) o[k - k0] = char(uint8_t(v));
+                    else if (cb == 2) reinterpret_cast<uint16_t*>(o)[k - k0] = uint16_t(v);
+                    else reinterpret_cast<uint32_t*>(o)[k - k0] = v;
+                }
+                e += kn - k0;
             }
-        }
-        FG_CUDA(cudaError_t(staged_upload(s->gpu, s->node_class, narrow.data(), narrow.size(), st)));
-        s->h2d_bytes += narrow.size();
-        FG_CUDA(cudaStreamSynchronize(st));
+        };
+        const size_t bytes = nnp * size_t(cb);
+        FG_CUDA(cudaError_t(staged_fill(s->gpu, s->node_class, bytes, st, narrow)));
+        s->h2d_bytes += bytes;
     }
+    clk.mark("classes_up");
     std::vector<DevCoef> dcls(ncls);
     for (size_t q = 0; q < ncls; ++q) {
         for (int c = 0; c < 3; ++c) { dcls[q].ca[c] = sim.classes[q].ca[c]; dcls[q].cb[c] = sim.classes[q].cb[c]; }
@@ -1649,21 +1601,37 @@ int session_new(Gpu* gpu, const HostSim& sim, const RunSpec& rs, Session** out, 
     rc |= up(s->wires, wires.data(), wires.size() * sizeof(DevWire));
     rc |= up(s->sheets, sheets.data(), sheets.size() * sizeof(DevSheet));
     rc |= up(s->branch, sim.sheet_table.data(), sim.sheet_table.size() * 4);
-    rc |= up(s->debye_f, debye_f.data(), debye_f.size() * 8);
-    rc |= up(s->debye_dd, debye_dd.data(), debye_dd.size() * 4);
-    rc |= up(s->debye_cb, debye_cb.data(), debye_cb.size() * 4);
+    rc |= up(debye_raw, sim.debye_edges.data(), nd * sizeof(DebyeEdge));
     rc |= up(s->debye_table, debye_table.data(), debye_table.size() * 4);
     rc |= up(d_pulse, t_pulse.data(), t_pulse.size() * 4);
-    if (s->local) {
-        rc |= up(s->local_ids, lc.ids.data(), lc.ids.size());
-        rc |= up(s->tables, lc.tables.data(), lc.tables.size() * 4);
-    }
     if (!cp.blocks.empty()) rc |= up(s->tma_blocks, cp.blocks.data(), cp.blocks.size() * sizeof(int4));
     if (!cp.own.empty()) rc |= up(s->tma_own, cp.own.data(), cp.own.size() * sizeof(int2));
     rc |= up(d_dft, t_dft.data(), t_dft.size() * 4);
     rc |= up(d_far, t_far.data(), t_far.size() * 4);
     if (rc) return FG_ERR_CUDA;
+    // the Debye list and the per-block class tables from the uploaded node classes
+    auto with_cid = [&](auto fn) {
+        if (s->cid_bytes == 1) fn(static_cast<const uint8_t*>(s->node_class));
+        else if (s->cid_bytes == 2) fn(static_cast<const uint16_t*>(s->node_class));
+        else fn(static_cast<const uint32_t*>(s->node_class));
+    };
+    if (nd)
+        with_cid([&](auto nc) {
+            const unsigned grid = unsigned(std::min<size_t>((nd + 255) / 256, size_t(148) * 16));
+            k_debye_lists<<<grid, 256, 0, st>>>(debye_raw, (long long)nd, nc, s->classes, (long long)n2, (long long)g.p2,
+                                                (long long)cs, s->debye_f, s->debye_dd, s->debye_cb);
+        });
+    if (s->local && !cp.blocks.empty())
+        with_cid([&](auto nc) {
+            k_local_classes<<<unsigned(cp.blocks.size()), 256, 0, st>>>(nc, s->classes, s->tma_blocks, s->tma_own, g.n1,
+                                                                       g.n2, g.p2, TMA_TK, cp.lo[2], cp.hi[2],
+                                                                       s->local_ids, s->tables, setup_flag);
+        });
+    FG_CUDA(cudaGetLastError());
+    int over = 0;
+    FG_CUDA(cudaMemcpyAsync(&over, setup_flag, sizeof(int), cudaMemcpyDeviceToHost, st));
     FG_CUDA(cudaStreamSynchronize(st));
+    if (over) s->local = false;   // a region holds more classes than a local table: global ids
 
     clk.mark("upload");
     if (rs.design && !rs.design->empty()) {
@@ -1721,6 +1689,10 @@ int session_new(Gpu* gpu, const HostSim& sim, const RunSpec& rs, Session** out, 
         if (rc) { session_free(s.release()); return rc; }
     }
     clk.mark("graphs_slots");
+    struct Done {   // the graph captures below are the last phase
+        PhaseClock& c;
+        ~Done() { c.mark("graphs"); }
+    } done{clk};
     if (!rs.graphs || s->slots) {
         *out = s.release();
         return FG_OK;

@@ -207,6 +207,71 @@ int fgo_sim_wires(void* p, uint64_t* h, uint64_t* e, double* c) {
     return FG_OK;
 }
 
+// Sim.ax[axis] (sim.rs:12-27): per node inv_d, inv_dd, raw_inv_d, raw_inv_dd, be, ce, bh, ch,
+// slot_e, slot_h (10 values, the order of the packed axis table, run.rs:205-212).
+int fgo_sim_axis(void* p, uint32_t axis, double* out) {
+    auto* a = static_cast<AnySim*>(p);
+    if (axis > 2) return FG_ERR_INVALID;
+    auto fill = [&](auto& s) {
+        const auto& x = s.ax[axis];
+        for (size_t q = 0; q < x.inv_d.size(); ++q) {
+            const double v[10] = {double(x.inv_d[q]), double(x.inv_dd[q]), double(x.raw_inv_d[q]),
+                                  double(x.raw_inv_dd[q]), double(x.be[q]), double(x.ce[q]), double(x.bh[q]),
+                                  double(x.ch[q]), double(x.slot_e[q]), double(x.slot_h[q])};
+            for (int f = 0; f < 10; ++f) out[10 * q + f] = v[f];
+        }
+    };
+    if (a->bits == 64) fill(*a->d);
+    else fill(*a->f);
+    return FG_OK;
+}
+
+// The Sim's sparse lists: "debye" (comp, id; dd), "sources<p>" of port p (comp, id; src),
+// "inductors" (comp, id; ke, ki), "poles" (-; x, a). idx gets 2 entries, val 2 per item.
+int fgo_sim_list(void* p, const char* what, uint64_t* idx, double* val, uint64_t* count) {
+    auto* a = static_cast<AnySim*>(p);
+    const std::string w(what);
+    auto fill = [&](auto& s) -> int {
+        size_t n = 0;
+        if (w == "debye") {
+            for (auto& [c, id, dd] : s.debye_edges) { idx[2 * n] = c; idx[2 * n + 1] = id; val[2 * n] = dd; val[2 * n + 1] = 0; ++n; }
+        } else if (w.rfind("sources", 0) == 0) {
+            const size_t port = std::stoul(w.substr(7));
+            if (port >= s.port_src.size()) return FG_ERR_INVALID;
+            for (auto& [c, id, v] : s.port_src[port]) { idx[2 * n] = c; idx[2 * n + 1] = id; val[2 * n] = double(v); val[2 * n + 1] = 0; ++n; }
+        } else if (w == "inductors") {
+            for (auto& [c, id, ke, ki] : s.inductors) { idx[2 * n] = c; idx[2 * n + 1] = id; val[2 * n] = double(ke); val[2 * n + 1] = double(ki); ++n; }
+        } else if (w == "poles") {
+            for (auto& [x, am] : s.poles) { idx[2 * n] = 0; idx[2 * n + 1] = 0; val[2 * n] = x; val[2 * n + 1] = am; ++n; }
+        } else {
+            return FG_ERR_INVALID;
+        }
+        *count = n;
+        return FG_OK;
+    };
+    return a->bits == 64 ? fill(*a->d) : fill(*a->f);
+}
+
+// Sim.sheets (sim.rs:197-206): idx gets comp, id, faces[0], faces[1]; val gets r, adaptive, len,
+// c; table (NULL: count only) gets Sim.sheet_table.
+int fgo_sim_sheets(void* p, uint64_t* idx, double* val, uint64_t* count, float* table, uint64_t* table_len) {
+    auto* a = static_cast<AnySim*>(p);
+    auto fill = [&](auto& s) {
+        *count = s.sheets.size();
+        *table_len = s.sheet_table.size();
+        if (!idx) return;
+        for (size_t q = 0; q < s.sheets.size(); ++q) {
+            const auto& e = s.sheets[q];
+            idx[4 * q] = e.comp; idx[4 * q + 1] = e.id; idx[4 * q + 2] = e.faces[0]; idx[4 * q + 3] = e.faces[1];
+            val[4 * q] = e.r; val[4 * q + 1] = e.adaptive ? 1.0 : 0.0; val[4 * q + 2] = e.len; val[4 * q + 3] = e.c;
+        }
+        std::copy(s.sheet_table.begin(), s.sheet_table.end(), table);
+    };
+    if (a->bits == 64) fill(*a->d);
+    else fill(*a->f);
+    return FG_OK;
+}
+
 // port_loop (run.rs:102-127) for port `port`, around axis `axis` at height k.
 int fgo_port_loop(void* p, uint64_t port, uint64_t axis, uint64_t k, uint64_t* ids, uint32_t* comps, double* w,
                   uint64_t cap, uint64_t* count) {

@@ -62,6 +62,9 @@ def lib():
         "fgo_far_eval": (C.c_int, [P(dbl), P(dbl), u64, P(C.c_float), u64, u64, dbl, dbl, dbl, P(dbl), u64, P(dbl), P(dbl)]),
         "fgo_far_radiated": (C.c_int, [P(dbl), P(dbl), u64, P(C.c_float), u64, u64, dbl, dbl, dbl, u64, P(dbl), P(dbl)]),
         "fgo_time_steps": (C.c_int, [vp, u64, P(A.fg_pulse), P(A.fg_extras), u64, u64, P(dbl), cp, sz]),
+        "fgo_sim_axis": (C.c_int, [vp, u32, P(dbl)]),
+        "fgo_sim_list": (C.c_int, [vp, cp, P(u64), P(dbl), P(u64)]),
+        "fgo_sim_sheets": (C.c_int, [vp, P(u64), P(dbl), P(u64), P(C.c_float), P(u64)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -139,6 +142,44 @@ class OracleSim:
             raise OracleError("port_loop needs a 32-bit sim")
         n = count.value
         return [(int(ids[q]), int(comps[q]), float(w[q])) for q in range(n)]
+
+    def axis(self, a: int) -> np.ndarray:
+        """Sim.ax[a] as an (n, 10) f64 array: inv_d, inv_dd, raw_inv_d, raw_inv_dd, be, ce, bh, ch,
+        slot_e, slot_h."""
+        n = self.dims()[a]
+        out = np.zeros((n, 10))
+        lib().fgo_sim_axis(self._h, a, out.ctypes.data_as(C.POINTER(C.c_double)))
+        return out
+
+    def items(self, what: str):
+        """A sparse list of the Sim: "debye", "sources<p>", "inductors" or "poles", as (idx
+        (n, 2) uint64, val (n, 2) f64)."""
+        cap = max(self.count("debye_edges"), self.count("inductors"), 64,
+                  max((self.count(f"port_src{p}") for p in range(max(len(self.ports), 1))), default=0))
+        idx = np.zeros((cap, 2), np.uint64)
+        val = np.zeros((cap, 2))
+        count = C.c_uint64()
+        code = lib().fgo_sim_list(self._h, what.encode(), idx.ctypes.data_as(C.POINTER(C.c_uint64)),
+                                  val.ctypes.data_as(C.POINTER(C.c_double)), C.byref(count))
+        if code:
+            raise OracleError(f"no list {what!r}", code)
+        n = count.value
+        return idx[:n], val[:n]
+
+    def sheets(self):
+        """Sim.sheets as (idx (n, 4) uint64: comp, id, face a, face b; val (n, 4): r, adaptive, len,
+        c) and Sim.sheet_table (f32)."""
+        L = lib()
+        P = C.POINTER
+        n, t = C.c_uint64(), C.c_uint64()
+        L.fgo_sim_sheets(self._h, C.cast(None, P(C.c_uint64)), C.cast(None, P(C.c_double)), C.byref(n),
+                         C.cast(None, P(C.c_float)), C.byref(t))
+        idx = np.zeros((max(n.value, 1), 4), np.uint64)
+        val = np.zeros((max(n.value, 1), 4))
+        table = np.zeros(max(t.value, 1), np.float32)
+        L.fgo_sim_sheets(self._h, idx.ctypes.data_as(P(C.c_uint64)), val.ctypes.data_as(P(C.c_double)), C.byref(n),
+                         table.ctypes.data_as(P(C.c_float)), C.byref(t))
+        return idx[: n.value], val[: n.value], table[: t.value]
 
     def coef_sets(self, narrow: int):
         L = lib()

@@ -10,7 +10,7 @@ L2, so no flush is needed between timed steps.
 
 value: whole-job nodes x steps / device time of the K timed steps (CUDA events on the session's
 stream, max over ranks). Ranks run independent replicas (weak scaling): the reference solves one
-grid on one device, and the north star keeps a grid on one GPU.
+grid on one device, and this engine keeps a grid on one GPU.
 
 --impl reference: the CPU baseline arm (rank 0 only): the oracle (a C++ restatement of the
 reference's own CPU FDTD, cpu.rs) on all host cores, on a bounded sample of full time steps of the
@@ -67,6 +67,8 @@ def parse():
     p.add_argument("--cpu-steps", type=int, default=8, help="full time steps the CPU baseline times")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-extras", action="store_true",
+                   help="throughput: skip the batched and adjoint ratios that the line also carries")
     p.add_argument("--workload", choices=["throughput", "adjoint", "batched", "batched-adjoint"], default="throughput",
                    help="throughput: the 512^3 spheres step (the headline); adjoint: the flux-objective "
                         "gradient over a 32x32x8 design block on 160x160x96 cells, 4000 steps; batched: 192 "
@@ -271,7 +273,7 @@ def run_adjoint(args):
               "max_rel_err": float(max(errs)), "median_rel_err": float(np.median(errs)),
               "within_1e-3": int(sum(e <= 1e-3 for e in errs)), "seconds": time.perf_counter() - t0}
     if rank != 0:
-        return 0
+        return None
     dev_f = float(np.median([x[1] for x in fwd]))
     dev_g = float(np.median([x[1].forward_ms + x[1].backward_ms for x in grad]))
     wall_f = float(np.median([x[0] for x in fwd]))
@@ -293,8 +295,7 @@ def run_adjoint(args):
                        "the gradient"},
         "objective": r.objective, "clocks": clocks, "fd_check": fd,
     }
-    print(json.dumps(line))
-    return 0
+    return line
 
 
 def run_batched(args):
@@ -347,7 +348,7 @@ def run_batched(args):
     b.close()
     clocks = sampler.stop()
     if rank != 0:
-        return 0
+        return None
     line = {
         "metric": "batched speed-up over sequential per-grid runs", "value": seq_ms / bat_ms, "unit": "x",
         "n_gpus": world, "steps": K, "warmup": 2, "higher_is_better": True, "scaling": "weak",
@@ -363,8 +364,7 @@ def run_batched(args):
         "clocks": clocks,
         "series_finite": bool(all(np.all(np.isfinite(x)) for x in series)),
     }
-    print(json.dumps(line))
-    return 0
+    return line
 
 
 def run_batched_adjoint(args):
@@ -427,10 +427,11 @@ def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
-    if args.workload == "adjoint":
-        return run_adjoint(args)
-    if args.workload == "batched":
-        return run_batched(args)
+    if args.workload in ("adjoint", "batched"):
+        line = (run_adjoint if args.workload == "adjoint" else run_batched)(args)
+        if line is not None:
+            print(json.dumps(line), flush=True)
+        return 0
     if args.workload == "batched-adjoint":
         return run_batched_adjoint(args)
     rank = int(os.environ.get("RANK", "0"))
@@ -538,6 +539,22 @@ def main():
         del sim
         cpu = cpu_baseline(args, sc)
 
+    # the batched and adjoint ratios, each on its own workload with its own clock record (one GPU)
+    extras = {}
+    if world == 1 and not args.no_extras:
+        bat = run_batched(argparse.Namespace(steps=1500, count=192))
+        extras["batched_speedup"] = {
+            "value": bat["value"], "unit": "x", "workload": bat["config"]["workload"], "steps": bat["steps"],
+            "batched_ms": bat["batched_ms"], "sequential_ms": bat["sequential_ms"], "tuned": bat["tuned"],
+            "timing": bat["timing"], "clocks": bat["clocks"]}
+        adj = run_adjoint(argparse.Namespace(steps=4000, warmup=3, checkpoints=64, fd=0))
+        extras["adjoint_grad_over_forward"] = {
+            "value": adj["value"], "unit": "x", "higher_is_better": False, "workload": adj["config"]["workload"],
+            "steps": adj["steps"], "checkpoints": adj["config"]["checkpoints"], "forward_ms": adj["forward_ms"],
+            "gradient_ms": adj["gradient_ms"], "parts_ms": adj["gradient_parts_ms"],
+            "timing": "device time of the forward and of the gradient (forward with checkpoints + recomputation + "
+                      "backward sweep), medians of 3 after 3 warm-ups", "clocks": adj["clocks"]}
+
     if rank == 0:
         line = {
             "metric": "Mcell-updates/s", "value": value, "unit": "Mcell/s", "n_gpus": world, "steps": K,
@@ -560,6 +577,7 @@ def main():
             "e2e": e2e,
             "cpu_baseline": cpu,
             "energy_after": energy,
+            **extras,
         }
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -4,7 +4,7 @@ the reference's arithmetic, and in f64, the FP64 truth run of the same update, a
 series, every field component's L2 norm, the fields at 8192 seeded nodes, samples of the plane DFT
 or NTFF accumulators and, for the antenna, the far field on the 5-degree grid).
 
-The bar is the north star's: relative L2 at most 1e-4 against the oracle's f32 run on fields,
+The bar: relative L2 at most 1e-4 against the oracle's f32 run on fields,
 series, accumulators and far field, after the full step count. Each case also prints the error of
 the GPU run and of the oracle's f32 run against the f64 run (the per-configuration error
 statement)."""

@@ -94,6 +94,11 @@ def _declare(L):
                                        P(dbl), cp, sz]),
         "fg_energy_noalloc": (C.c_int, [vp, vp, u64, vp, vp]),
         "fg_port_spectra": (C.c_int, [P(C.c_float), u64, u64, u64, dbl, P(dbl), u64, P(dbl), P(dbl)]),
+        "fg_raster_fill": (C.c_int, [vp, P(dbl), u64, P(dbl), u64, P(dbl), u64, P(dbl), u64, C.c_int, P(C.c_uint8), P(C.c_uint8), cp, sz]),
+        "fg_raster_solid_edges": (C.c_int, [vp, P(dbl), u64, P(dbl), u64, P(dbl), u64, P(dbl), u64, P(C.c_uint8), cp, sz]),
+        "fg_raster_solid_cells": (C.c_int, [vp, P(dbl), u64, P(dbl), u64, P(dbl), u64, P(dbl), u64, P(C.c_uint8), cp, sz]),
+        "fg_raster_sheet_edges": (C.c_int, [vp, P(dbl), u64, P(dbl), u64, P(dbl), u64, P(dbl), u64, P(C.c_uint8), cp, sz]),
+        "fg_raster_closed": (C.c_int, [P(dbl), u64]),
         "fg_flux_gradient_batch": (C.c_int, [vp, vp, P(u64), P(A.fg_pulse), P(A.fg_flux_spec), u64, C.c_int,
                                              P(A.fg_flux_result), vp, vp, cp, sz]),
     }

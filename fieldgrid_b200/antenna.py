@@ -6,8 +6,9 @@ and the far-field box (gain pattern).
 
 Names, argument meanings and error texts follow the reference. `run_gpu` is the reference's
 `run_gpu`; there is no CPU path (the reference's `run` calls `run_cpu`, which this package does not
-have). Meshed triangle parts (`Part`, which need the reference's rasteriser, raster.rs) are refused.
-The V/I spectra of `finish` come from the C ABI's fg_port_spectra (f64, host); the far field from
+have). Meshed triangle parts (`Part`) go through the CUDA rasteriser (fieldgrid_b200.raster, the
+reference's raster.rs): dielectric parts fill the cells whose centres they hold, metal parts mark
+the edges they pass through and, when closed, the edges inside them. The V/I spectra of `finish` come from the C ABI's fg_port_spectra (f64, host); the far field from
 `fdtd.Far` (f64, device).
 """
 from __future__ import annotations
@@ -57,6 +58,74 @@ class Dielectric:
 
 
 @dataclass
+class Metal:
+    """Stuff::Metal (mod.rs:57-61)."""
+
+
+@dataclass
+class DielectricStuff:
+    """Stuff::Dielectric { eps_r, tan_d } (mod.rs:57-61)."""
+
+    eps_r: float
+    tan_d: float
+
+
+@dataclass
+class Part:
+    """mod.rs:63-115: a triangle mesh ((n, 3, 3) vertices) of one material."""
+
+    triangles: np.ndarray
+    stuff: object
+
+    def __post_init__(self):
+        self.triangles = np.asarray(self.triangles, np.float64).reshape(-1, 3, 3)
+
+    def bounds(self) -> Optional[Aabb]:
+        """mod.rs:69-76."""
+        if len(self.triangles) == 0:
+            return None
+        p = self.triangles.reshape(-1, 3)
+        return Aabb(tuple(float(v) for v in p.min(axis=0)), tuple(float(v) for v in p.max(axis=0)))
+
+    def planes(self, axis: int) -> list:
+        """mod.rs:78-88: the coordinates of the triangles flat in `axis`, sorted, deduplicated to 1e-9."""
+        t = self.triangles
+        flat = np.all(np.abs(t[:, :, axis] - t[:, :1, axis]) < 1e-12, axis=1)
+        vals = sorted(float(v) for v in t[flat, 0, axis])
+        out: list = []
+        for v in vals:               # Vec::dedup_by against the last kept value
+            if not out or abs(v - out[-1]) >= 1e-9:
+                out.append(v)
+        return out
+
+    def rims(self, axis: int) -> list:
+        """mod.rs:90-114: (coordinate, inward sign) of the boundary edges (used by one triangle)
+        that lie flat in `axis` with the triangle's third vertex off that plane."""
+        key = [[tuple(np.float64(v).tobytes() for v in p) for p in tri] for tri in self.triangles]
+        count: dict = {}
+        for tk in key:
+            for k in range(3):
+                a, b = tk[k], tk[(k + 1) % 3]
+                e = (a, b) if a < b else (b, a)
+                count[e] = count.get(e, 0) + 1
+        out = []
+        for tri, tk in zip(self.triangles, key):
+            for k in range(3):
+                a, b, c = tri[k], tri[(k + 1) % 3], tri[(k + 2) % 3]
+                ka, kb = tk[k], tk[(k + 1) % 3]
+                once = count.get((ka, kb) if ka < kb else (kb, ka)) == 1
+                if not once or abs(a[axis] - b[axis]) > 1e-12 or abs(c[axis] - a[axis]) < 1e-12:
+                    continue
+                out.append((float(a[axis]), math.copysign(1.0, c[axis] - a[axis])))
+        out.sort()
+        dedup: list = []
+        for v in out:                # dedup_by: equal to 1e-9 with the same sign
+            if not dedup or not (abs(v[0] - dedup[-1][0]) < 1e-9 and v[1] == dedup[-1][1]):
+                dedup.append(v)
+        return dedup
+
+
+@dataclass
 class Wire:
     """mod.rs:40-45."""
 
@@ -76,7 +145,7 @@ class Port:
 
 @dataclass
 class Model:
-    """mod.rs:120-131. `parts` (triangle meshes) must be empty here."""
+    """mod.rs:118-128."""
 
     parts: list = field(default_factory=list)
     metal: List[Aabb] = field(default_factory=list)
@@ -91,7 +160,8 @@ class Model:
     def bounds(self) -> Optional[Aabb]:
         """mod.rs:133-148: the box around metal, wires, dielectrics and the port."""
         boxes = list(self.metal) + [Aabb.new(w.a, w.b) for w in self.wires] + \
-            [d.bounds for d in self.dielectrics] + ([Aabb.new(self.port.a, self.port.b)] if self.port else [])
+            [d.bounds for d in self.dielectrics] + [b for b in (p.bounds() for p in self.parts) if b is not None] + \
+            ([Aabb.new(self.port.a, self.port.b)] if self.port else [])
         if not boxes:
             return None
         lo = tuple(min(b.lo[i] for b in boxes) for i in range(3))
@@ -146,9 +216,8 @@ def mesh(model: Model, pml: int) -> Optional[Grid]:
     two thirds outside a wide plate's edge, the edge itself for thin or shared faces), dielectric
     faces and the port's ends, graded from the feature sizes at ratio 1.3 up to lambda/20 in air
     (lambda/20/sqrt(eps_r) inside dielectrics), smoothed to a 1.5 neighbour ratio and padded with
-    the CPML cells; the box reaches a quarter wavelength at f0 past the model."""
-    if model.parts:
-        raise ValueError("meshed parts need the rasteriser of sims-field (raster.rs), which this package does not build")
+    the CPML cells; the box reaches a quarter wavelength at f0 past the model. Parts pin their flat
+    planes and (metal) their rims (mesh.rs:44-70)."""
     bounds = model.bounds()
     if bounds is None:
         return None
@@ -177,6 +246,30 @@ def mesh(model: Model, pml: int) -> Optional[Grid]:
                 else:
                     fixed.append(v)
                 features.append((v, fine))
+        for part in model.parts:
+            b = part.bounds()
+            if b is None:
+                continue
+            if isinstance(part.stuff, DielectricStuff):
+                local = lam / 20.0 / math.sqrt(part.stuff.eps_r)
+                thick = b.hi[a] - b.lo[a]
+                size = max(thick / 4.0, 1e-6) if thick < 4.0 * local else local
+            else:
+                size = fine
+            for v in part.planes(a):
+                fixed.append(v)
+                features.append((v, size))
+            if isinstance(part.stuff, Metal):
+                wide = b.hi[a] - b.lo[a] > 2.0 * fine
+                for v, inward in part.rims(a):
+                    if wide:
+                        fixed.append(v + inward * fine / 3.0)
+                        fixed.append(v - inward * 2.0 * fine / 3.0)
+                    else:
+                        fixed.append(v)
+                    features.append((v, fine))
+            features.append((b.lo[a], size))
+            features.append((b.hi[a], size))
         for d in model.dielectrics:
             lo, hi = d.bounds.lo[a], d.bounds.hi[a]
             fixed += [lo, hi]
@@ -199,6 +292,10 @@ def mesh(model: Model, pml: int) -> Optional[Grid]:
             if not dedup or abs(v - dedup[-1]) >= 1e-7:
                 dedup.append(v)
         slow = [(d.bounds.lo[a], d.bounds.hi[a], d.eps_r) for d in model.dielectrics]
+        for part in model.parts:
+            b = part.bounds()
+            if isinstance(part.stuff, DielectricStuff) and b is not None:
+                slow.append((b.lo[a], b.hi[a], part.stuff.eps_r))
 
         def coarse(x, slow=slow):
             s = coarse_air
@@ -217,9 +314,10 @@ def _span(line: np.ndarray, lo: float, hi: float):
     return int(np.searchsorted(line, lo - 1e-9, side="left")), int(np.searchsorted(line, hi + 1e-9, side="right"))
 
 
-def materials(grid: Grid, model: Model) -> fdtd.Materials:
-    """engine.rs:10-43: each dielectric box sets eps, eps_inf and sigma = w eps0 eps_r tan_d (at f0)
-    on the cells between its faces."""
+def materials(grid: Grid, model: Model, raster=None) -> fdtd.Materials:
+    """engine.rs:9-41: each dielectric box sets eps, eps_inf and sigma = w eps0 eps_r tan_d (at f0)
+    on the cells between its faces, then each dielectric part on the cells whose centres it holds
+    (raster.solid_cells)."""
     nx, ny, nz = grid.dims()
     mats = fdtd.Materials.new(grid)
     w = 2.0 * math.pi * model.f0
@@ -234,6 +332,14 @@ def materials(grid: Grid, model: Model) -> fdtd.Materials:
         eps[r[0], r[1], r[2]] = np.float32(d.eps_r)
         inf[r[0], r[1], r[2]] = np.float32(d.eps_r)
         sig[r[0], r[1], r[2]] = np.float32(w * EPS0 * d.eps_r * d.tan_d)
+    for part in model.parts:
+        if not isinstance(part.stuff, DielectricStuff):
+            continue
+        inside = raster.solid_cells(part.triangles, grid).reshape(nx - 1, ny - 1, nz - 1)
+        er, td = part.stuff.eps_r, part.stuff.tan_d
+        eps[inside] = np.float32(er)
+        inf[inside] = np.float32(er)
+        sig[inside] = np.float32(w * EPS0 * er * td)
     return mats
 
 
@@ -285,20 +391,31 @@ def wire_edges(grid: Grid, wires: List[Wire]):
     return out
 
 
-def sim_args(grid: Grid, model: Model, port: Port):
-    """The arguments of Sim::try_new that engine.rs:113-130 builds: materials, the PEC mask of the
-    metal boxes and wires, one port and the thin wires."""
-    mats = materials(grid, model)
+def sim_args(grid: Grid, model: Model, port: Port, raster=None):
+    """The arguments of Sim::try_new that engine.rs:105-131 builds: materials, the PEC mask of the
+    metal boxes, wires and metal parts (the edges a part passes through and, for a closed part,
+    the edges inside it), one port and the thin wires."""
+    mats = materials(grid, model, raster)
     wires = wire_edges(grid, model.wires)
     solid = list(model.metal) + [Aabb.new(w.a, w.b) for w in model.wires]
     mask = metal_edges(grid, solid)
+    n = tuple(grid.dims())
+    for part in model.parts:
+        if not isinstance(part.stuff, Metal):
+            continue
+        more = [raster.sheet_edges(part.triangles, grid)]
+        if raster.closed(part.triangles):
+            more.append(raster.solid_edges(part.triangles, grid))
+        for m in more:
+            for c in range(3):
+                mask[c] |= np.asarray(m[c], np.uint8).reshape(n)
     return (grid, mats, mask.reshape(-1), [], [port_def(grid, port)], [],
             fdtd.Media(fdtd.Sheets(), fdtd.Debye(), wires))
 
 
-def build(grid: Grid, model: Model, port: Port) -> fdtd.Sim:
-    """engine.rs:113-130."""
-    return fdtd.Sim.try_new(*sim_args(grid, model, port))
+def build(grid: Grid, model: Model, port: Port, raster=None) -> fdtd.Sim:
+    """engine.rs:105-131."""
+    return fdtd.Sim.try_new(*sim_args(grid, model, port, raster))
 
 
 @dataclass
@@ -320,21 +437,28 @@ def sweep_freqs(model: Model, points: int) -> np.ndarray:
     return np.array([f0 * (1.0 - model.span + 2.0 * model.span * i / max(points - 1, 1)) for i in range(points)])
 
 
-def setup(model: Model, opts: Options, sim_factory: Callable = None, patch_fn: Callable = None) -> Setup:
-    """mod.rs:201-223. `sim_factory(*args)` builds the Sim and `patch_fn(sim, inset)` its NTFF box
-    (defaults: this engine's Sim.try_new and fdtd.patches)."""
+def setup(model: Model, opts: Options, sim_factory: Callable = None, patch_fn: Callable = None,
+          raster=None) -> Setup:
+    """mod.rs:195-213. `sim_factory(*args)` builds the Sim, `patch_fn(sim, inset)` its NTFF box and
+    `raster` rasterises the parts (defaults: this engine's Sim.try_new, fdtd.patches and the CUDA
+    rasteriser on a Gpu opened here when the model has parts)."""
     port = model.port
     if port is None:
         raise fdtd.FdtdError("the model has no port")
-    if model.parts:
-        raise fdtd.FdtdError("meshed parts need the rasteriser of sims-field (raster.rs), which this package does not build")
-    solid = Model(metal=list(model.metal) + [Aabb.new(w.a, w.b) for w in model.wires], wires=list(model.wires),
-                  dielectrics=list(model.dielectrics), port=model.port, f0=model.f0, span=model.span,
-                  fine=model.fine, ground_plane_z=model.ground_plane_z)
+    if model.parts and raster is None:
+        from .gpu import Gpu
+        from .raster import GpuRaster
+        raster = GpuRaster(Gpu.open())
+    closed = raster.closed if raster is not None else (lambda _t: False)
+    if any(isinstance(p.stuff, DielectricStuff) and not closed(p.triangles) for p in model.parts):
+        raise fdtd.FdtdError("a dielectric part is not a closed mesh")
+    solid = Model(parts=list(model.parts), metal=list(model.metal) + [Aabb.new(w.a, w.b) for w in model.wires],
+                  wires=list(model.wires), dielectrics=list(model.dielectrics), port=model.port, f0=model.f0,
+                  span=model.span, fine=model.fine, ground_plane_z=model.ground_plane_z)
     grid = mesh(solid, opts.pml)
     if grid is None:
         raise fdtd.FdtdError("nothing to mesh")
-    args = sim_args(grid, model, port)
+    args = sim_args(grid, model, port, raster)
     sim = (sim_factory or fdtd.Sim.try_new)(*args)
     patches = (patch_fn or fdtd.patches)(sim, 3) if opts.far_field else None
     return Setup(sim, patches, sweep_freqs(model, opts.points), model.f0, model.f0 * 0.5, grid, args)
@@ -383,8 +507,9 @@ def run_gpu(model: Model, opts: Options = None, progress=None, g=None) -> Outcom
     """mod.rs:279-290 on this engine. `g` is an open fieldgrid_b200.gpu.Gpu (opened when None)."""
     from .gpu import Gpu
     opts = opts or Options()
-    s = setup(model, opts)
     g = g or Gpu.open()
+    from .raster import GpuRaster
+    s = setup(model, opts, raster=GpuRaster(g))
     pulse = fdtd.Pulse(s.f0, s.fc)
     rec = fdtd.run(g, s.sim, 0, pulse, extras(s, opts), progress)
     return finish(s, rec, True, far_gpu=g)

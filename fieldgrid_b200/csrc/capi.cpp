@@ -707,4 +707,78 @@ void fg_batch_free(fg_batch* b) {
     delete b;
 }
 
+
+// ---- rasterisation (raster.rs) ----------------------------------------------------------------
+
+static std::vector<double> line_of(const double* v, uint64_t n) { return std::vector<double>(v, v + n); }
+
+static std::vector<double> centres_of(const std::vector<double>& l) {   // grid::centres (grid.rs:61-63)
+    std::vector<double> c;
+    for (size_t i = 0; i + 1 < l.size(); ++i) c.push_back(0.5 * (l[i] + l[i + 1]));
+    return c;
+}
+
+int fg_raster_fill(fg_gpu* g, const double* tris, uint64_t ntri, const double* s0, uint64_t n0, const double* s1,
+                   uint64_t n1, const double* s2, uint64_t n2, int order, uint8_t* inside, uint8_t* thin,
+                   char* err, size_t errlen) {
+    if (!g) return fail(FG_ERR_NO_DEVICE, "no GPU: this engine has no CPU path", err, errlen);
+    if ((ntri && !tris) || !inside || !thin || (order != 0 && order != 1)) return fail(FG_ERR_INVALID, "invalid argument", err, errlen);
+    const std::vector<double> s[3] = {line_of(s0, n0), line_of(s1, n1), line_of(s2, n2)};
+    const size_t dims[3] = {size_t(n0), size_t(n1), size_t(n2)};
+    std::string e;
+    const int rc = raster_fill(g->g, tris, ntri, s, dims, order, inside, thin, e);
+    return rc ? fail(rc, e, err, errlen) : FG_OK;
+}
+
+int fg_raster_solid_edges(fg_gpu* g, const double* tris, uint64_t ntri, const double* x, uint64_t nx,
+                          const double* y, uint64_t ny, const double* z, uint64_t nz, uint8_t* mask,
+                          char* err, size_t errlen) {
+    if (!g) return fail(FG_ERR_NO_DEVICE, "no GPU: this engine has no CPU path", err, errlen);
+    if ((ntri && !tris) || !mask || nx < 2 || ny < 2 || nz < 2) return fail(FG_ERR_INVALID, "invalid argument", err, errlen);
+    const std::vector<double> lines[3] = {line_of(x, nx), line_of(y, ny), line_of(z, nz)};
+    const size_t dims[3] = {size_t(nx), size_t(ny), size_t(nz)};
+    const size_t nn = dims[0] * dims[1] * dims[2];
+    std::vector<uint8_t> inside(nn), thin(nn);
+    for (int c = 0; c < 3; ++c) {
+        // raster.rs:148-151: centres along c, the grid lines along the other axes
+        std::vector<double> s[3] = {lines[0], lines[1], lines[2]};
+        s[c] = centres_of(lines[c]);
+        std::string e;
+        const int rc = raster_fill(g->g, tris, ntri, s, dims, 0, inside.data(), thin.data(), e);
+        if (rc) return fail(rc, e, err, errlen);
+        uint8_t* m = mask + size_t(c) * nn;
+        for (size_t q = 0; q < nn; ++q) m[q] = uint8_t(inside[q] | thin[q]);
+    }
+    return FG_OK;
+}
+
+int fg_raster_solid_cells(fg_gpu* g, const double* tris, uint64_t ntri, const double* x, uint64_t nx,
+                          const double* y, uint64_t ny, const double* z, uint64_t nz, uint8_t* mask,
+                          char* err, size_t errlen) {
+    if (!g) return fail(FG_ERR_NO_DEVICE, "no GPU: this engine has no CPU path", err, errlen);
+    if ((ntri && !tris) || !mask || nx < 2 || ny < 2 || nz < 2) return fail(FG_ERR_INVALID, "invalid argument", err, errlen);
+    const std::vector<double> s[3] = {centres_of(line_of(x, nx)), centres_of(line_of(y, ny)), centres_of(line_of(z, nz))};
+    const size_t dims[3] = {s[0].size(), s[1].size(), s[2].size()};
+    const size_t n = dims[0] * dims[1] * dims[2];
+    std::vector<uint8_t> thin(n);
+    std::string e;
+    const int rc = raster_fill(g->g, tris, ntri, s, dims, 0, mask, thin.data(), e);
+    if (rc) return fail(rc, e, err, errlen);
+    for (size_t q = 0; q < n; ++q) mask[q] = uint8_t(mask[q] | thin[q]);
+    return FG_OK;
+}
+
+int fg_raster_sheet_edges(fg_gpu* g, const double* tris, uint64_t ntri, const double* x, uint64_t nx,
+                          const double* y, uint64_t ny, const double* z, uint64_t nz, uint8_t* mask,
+                          char* err, size_t errlen) {
+    if (!g) return fail(FG_ERR_NO_DEVICE, "no GPU: this engine has no CPU path", err, errlen);
+    if ((ntri && !tris) || !mask || nx < 2 || ny < 2 || nz < 2) return fail(FG_ERR_INVALID, "invalid argument", err, errlen);
+    const std::vector<double> lines[3] = {line_of(x, nx), line_of(y, ny), line_of(z, nz)};
+    std::string e;
+    const int rc = raster_sheet_edges(g->g, tris, ntri, lines, mask, e);
+    return rc ? fail(rc, e, err, errlen) : FG_OK;
+}
+
+int fg_raster_closed(const double* tris, uint64_t ntri) { return (tris && raster_closed(tris, ntri)) ? 1 : 0; }
+
 }  // extern "C"

@@ -51,6 +51,13 @@ struct Gpu {
 // reused. Small copies go straight. Returns a cudaError_t as int.
 int staged_upload(Gpu* g, void* dst, const void* src, size_t bytes, void* stream);
 
+// mesh -> grid rasterisation (raster.cu)
+int raster_fill(Gpu* gpu, const double* tris, uint64_t ntri, const std::vector<double>* samples, const size_t* dims,
+                int order, uint8_t* inside, uint8_t* thin, std::string& err);
+int raster_sheet_edges(Gpu* gpu, const double* tris, uint64_t ntri, const std::vector<double>* lines, uint8_t* mask,
+                       std::string& err);
+bool raster_closed(const double* tris, uint64_t ntri);
+
 int gpu_open(int device, Gpu** out, std::string& err);
 void gpu_close(Gpu* g);
 

@@ -354,6 +354,34 @@ int fg_batch_read(fg_batch* b, uint64_t index, const char* which, float* dst, ui
 int fg_batch_info(const fg_batch* b, fg_batch_options* opt, int* persistent_blocks, double* tuned_ms, uint64_t* steps);
 void fg_batch_free(fg_batch* b);
 
+/* ---- mesh -> grid rasterisation (crates/sims-field/src/raster.rs, bvh.rs) -----------------
+ * Triangles are ntri x 3 vertices x 3 f64 (x, y, z). Masks are bytes, 1 = marked. The ray casts
+ * and the sheet sweep run on the GPU in the reference's f64 arithmetic; g must be open. */
+/* fill (raster.rs:24-104) over the sample lines s0 (n0), s1 (n1), s2 (n2): inside / thin get the
+ * samples filled by ray parity / kept as thin skins (thin excludes inside), indexed over the
+ * samples themselves in order 0 = (i n1 + j) n2 + k or 1 = i + (j + k n1) n0. */
+int fg_raster_fill(fg_gpu* g, const double* tris, uint64_t ntri, const double* s0, uint64_t n0, const double* s1,
+                   uint64_t n1, const double* s2, uint64_t n2, int order, uint8_t* inside, uint8_t* thin,
+                   char* err, size_t errlen);
+/* solid_edges (raster.rs:145-160): per component c, the E edges (node index (i ny + j) nz + k,
+ * mask c * nx ny nz + node) whose midpoints the closed mesh holds, on the grid lines x, y, z. */
+int fg_raster_solid_edges(fg_gpu* g, const double* tris, uint64_t ntri, const double* x, uint64_t nx,
+                          const double* y, uint64_t ny, const double* z, uint64_t nz, uint8_t* mask,
+                          char* err, size_t errlen);
+/* solid_cells (raster.rs:162-173): the cells ((i (ny-1) + j) (nz-1) + k) whose centres the closed
+ * mesh holds. */
+int fg_raster_solid_cells(fg_gpu* g, const double* tris, uint64_t ntri, const double* x, uint64_t nx,
+                          const double* y, uint64_t ny, const double* z, uint64_t nz, uint8_t* mask,
+                          char* err, size_t errlen);
+/* sheet_edges (raster.rs:186-264): per component, the E edges a triangle sheet passes through
+ * (mask as fg_raster_solid_edges). */
+int fg_raster_sheet_edges(fg_gpu* g, const double* tris, uint64_t ntri, const double* x, uint64_t nx,
+                          const double* y, uint64_t ny, const double* z, uint64_t nz, uint8_t* mask,
+                          char* err, size_t errlen);
+/* closed (raster.rs:127-143): 1 when every edge of the mesh is shared by an even number of its
+ * triangles, 0 otherwise (and for an empty mesh). Host code. */
+int fg_raster_closed(const double* tris, uint64_t ntri);
+
 #ifdef __cplusplus
 }
 #endif

@@ -65,6 +65,10 @@ def lib():
         "fgo_sim_axis": (C.c_int, [vp, u32, P(dbl)]),
         "fgo_sim_list": (C.c_int, [vp, cp, P(u64), P(dbl), P(u64)]),
         "fgo_sim_sheets": (C.c_int, [vp, P(u64), P(dbl), P(u64), P(C.c_float), P(u64)]),
+        "fgo_raster_fill": (C.c_int, [P(dbl), u64, P(dbl), u64, P(dbl), u64, P(dbl), u64, P(u64), C.c_int,
+                                      P(C.c_uint8), P(C.c_uint8)]),
+        "fgo_raster_sheet_edges": (C.c_int, [P(dbl), u64, P(dbl), u64, P(dbl), u64, P(dbl), u64, P(C.c_uint8)]),
+        "fgo_raster_closed": (C.c_int, [P(dbl), u64]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -289,3 +293,69 @@ def time_steps(sim: OracleSim, driven, pulse, extras, warmup: int, steps: int) -
     if code:
         raise OracleError(err.value.decode(), code)
     return sec.value
+
+
+# ---- the rasteriser (raster.rs, bvh.rs) ---------------------------------------------------------
+
+def _tris(triangles):
+    return np.ascontiguousarray(np.asarray(triangles, np.float64).reshape(-1, 3, 3))
+
+
+def raster_fill(triangles, samples, dims=None, order: int = 0):
+    """fill (raster.rs:24-104): (inside, thin) byte masks over the index space dims (default: the
+    sample counts), order 0 = (i m1 + j) m2 + k, 1 = i + (j + k m1) m0."""
+    P = C.POINTER
+    t = _tris(triangles)
+    s = [np.ascontiguousarray(np.asarray(x, np.float64)) for x in samples]
+    m = np.array(dims if dims is not None else [len(x) for x in s], np.uint64)
+    total = int(np.prod(m))
+    inside = np.zeros(max(total, 1), np.uint8)
+    thin = np.zeros(max(total, 1), np.uint8)
+    dp = lambda a: a.ctypes.data_as(P(C.c_double))
+    lib().fgo_raster_fill(dp(t), len(t), dp(s[0]), len(s[0]), dp(s[1]), len(s[1]), dp(s[2]), len(s[2]),
+                          m.ctypes.data_as(P(C.c_uint64)), order, inside.ctypes.data_as(P(C.c_uint8)),
+                          thin.ctypes.data_as(P(C.c_uint8)))
+    return inside[:total], thin[:total]
+
+
+def _centres(line):
+    line = np.asarray(line, np.float64)
+    return 0.5 * (line[:-1] + line[1:])
+
+
+def raster_solid_edges(triangles, grid):
+    """solid_edges (raster.rs:145-160): per component, fill with centres along it."""
+    n = grid.dims()
+    out = []
+    for c in range(3):
+        s = [grid.axis(a) if a != c else _centres(grid.axis(a)) for a in range(3)]
+        inside, thin = raster_fill(triangles, s, n, 0)
+        out.append((inside | thin).astype(bool))
+    return out
+
+
+def raster_solid_cells(triangles, grid):
+    """solid_cells (raster.rs:162-173)."""
+    s = [_centres(grid.axis(a)) for a in range(3)]
+    inside, thin = raster_fill(triangles, s, None, 0)
+    return (inside | thin).astype(bool)
+
+
+def raster_sheet_edges(triangles, grid):
+    """sheet_edges (raster.rs:186-264)."""
+    P = C.POINTER
+    t = _tris(triangles)
+    x, y, z = [np.ascontiguousarray(np.asarray(grid.axis(a), np.float64)) for a in range(3)]
+    nn = len(x) * len(y) * len(z)
+    mask = np.zeros(3 * nn, np.uint8)
+    dp = lambda a: a.ctypes.data_as(P(C.c_double))
+    lib().fgo_raster_sheet_edges(dp(t), len(t), dp(x), len(x), dp(y), len(y), dp(z), len(z),
+                                 mask.ctypes.data_as(P(C.c_uint8)))
+    return [mask[c * nn:(c + 1) * nn].astype(bool) for c in range(3)]
+
+
+def raster_closed(triangles) -> bool:
+    """closed (raster.rs:127-143)."""
+    t = _tris(triangles)
+    return bool(lib().fgo_raster_closed(t.ctypes.data_as(C.POINTER(C.c_double)), len(t)))
+

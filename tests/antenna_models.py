@@ -1,11 +1,12 @@
 """The antenna models of sims-antenna's own tests (crates/sims-antenna/tests/fdtd.rs), restated as
 fieldgrid_b200.antenna Models for the tests here: the half-wave dipole (:6-22) and Sheen's
-microstrip patch in its box form (:88-138)."""
+microstrip patch in its box and meshed forms (:88-138)."""
 import math
 
 import numpy as np
 
 from fieldgrid_b200 import antenna as A
+from meshes import cuboid, plate
 
 
 def dipole() -> A.Model:
@@ -15,7 +16,7 @@ def dipole() -> A.Model:
                    port=A.Port((0.0, 0.0, -gap / 2), (0.0, 0.0, gap / 2), 50.0), f0=1.0e9, span=0.2, fine=gap)
 
 
-def sheen() -> A.Model:
+def sheen(meshed: bool = False) -> A.Model:
     mm = 1e-3
     h = 0.794 * mm
     w, l = 12.45 * mm, 16.0 * mm
@@ -27,11 +28,17 @@ def sheen() -> A.Model:
     top = l / 2 + 7.0 * mm
     sheets = [((-gx / 2, edge_y), (gx / 2, top), 0.0), ((x0, y0), (x0 + w, y0 + l), h),
               ((line_x, edge_y), (line_x + lw, y0), h)]
+    board = ((-gx / 2, edge_y, 0.0), (gx / 2, top, h))
     model = A.Model(port=A.Port((line_x + lw / 2, edge_y, 0.0), (line_x + lw / 2, edge_y, h), 50.0),
                     f0=7.5e9, span=0.25, fine=0.4 * mm)
-    for lo, hi, z in sheets:
-        model.metal.append(A.Aabb.new((lo[0], lo[1], z), (hi[0], hi[1], z)))
-    model.dielectrics.append(A.Dielectric(A.Aabb.new((-gx / 2, edge_y, 0.0), (gx / 2, top, h)), 2.2, 0.0))
+    if meshed:
+        for lo, hi, z in sheets:
+            model.parts.append(A.Part(plate(lo, hi, z), A.Metal()))
+        model.parts.append(A.Part(cuboid(board[0], board[1]), A.DielectricStuff(2.2, 0.0)))
+    else:
+        for lo, hi, z in sheets:
+            model.metal.append(A.Aabb.new((lo[0], lo[1], z), (hi[0], hi[1], z)))
+        model.dielectrics.append(A.Dielectric(A.Aabb.new(board[0], board[1]), 2.2, 0.0))
     return model
 
 
@@ -52,3 +59,24 @@ def resonance(freqs, z) -> float:
         if z[q].imag < 0.0 and z[q + 1].imag >= 0.0:
             return float(freqs[q])
     return 0.0
+
+
+class OracleRaster:
+    """The oracle's rasteriser (raster_oracle.cpp) in the shape antenna.setup calls."""
+
+    def solid_cells(self, triangles, grid):
+        from oracle import oracle as O
+        return O.raster_solid_cells(triangles, grid)
+
+    def solid_edges(self, triangles, grid):
+        from oracle import oracle as O
+        return O.raster_solid_edges(triangles, grid)
+
+    def sheet_edges(self, triangles, grid):
+        from oracle import oracle as O
+        return O.raster_sheet_edges(triangles, grid)
+
+    def closed(self, triangles) -> bool:
+        from oracle import oracle as O
+        return O.raster_closed(triangles)
+

@@ -8,7 +8,8 @@ import math
 import numpy as np
 import pytest
 
-from antenna_models import dipole, radiated, resonance
+from antenna_models import OracleRaster, dipole, radiated, resonance, sheen
+from meshes import plate
 from fieldgrid_b200 import antenna as A
 from fieldgrid_b200 import fdtd
 from oracle import oracle as O
@@ -86,3 +87,34 @@ def test_the_oracle_dipole_conserves_power_and_has_dipole_directivity():
     assert abs(eff - 1.0) < 0.01, eff
     assert abs(d - 2.15) < 0.05, d
     assert 960e6 <= res < 1010e6, res
+
+
+def test_an_open_dielectric_mesh_is_refused():
+    """tests/fdtd.rs:167-177 (sims-antenna)."""
+    model = sheen(True)
+    model.parts.append(A.Part(plate([0.0, 0.0], [1e-3, 1e-3], 2e-3), A.DielectricStuff(3.0, 0.0)))
+    with pytest.raises(fdtd.FdtdError, match="^a dielectric part is not a closed mesh$"):
+        A.setup(model, A.Options(far_field=False, max_steps=10), raster=OracleRaster())
+
+
+def test_the_meshed_board_fills_the_cells_of_the_box_board():
+    """Sheen's patch meshed (tests/fdtd.rs:119-127): its board, a closed cuboid whose faces the
+    mesher pins to grid lines (mod.rs:78-88), gives the box board's materials cell for cell, and
+    its metal plates mark edges on the planes z = 0 and z = h only."""
+    meshed, boxed = sheen(True), sheen(False)
+    grid = A.mesh(meshed, 8)
+    r = OracleRaster()
+    m1 = A.materials(grid, meshed, r)
+    m2 = A.materials(grid, boxed)
+    for name in ("eps", "inf", "sigma"):
+        assert np.array_equal(getattr(m1, name), getattr(m2, name)), name
+    assert np.count_nonzero(m1.eps != 1.0) > 1000
+    args = A.sim_args(grid, meshed, meshed.port, r)
+    n = grid.dims()
+    mask = np.asarray(args[2]).reshape(3, *n)
+    h = 0.794e-3
+    ks = set(np.nonzero(mask.any(axis=(0, 1, 2)))[0].tolist())
+    planes = {int(np.argmin(np.abs(grid.z - 0.0))), int(np.argmin(np.abs(grid.z - h)))}
+    assert ks == planes, (ks, planes)
+    assert not mask[2].any()     # flat plates mark no z edges
+

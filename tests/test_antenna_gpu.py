@@ -17,7 +17,7 @@ import math
 import numpy as np
 import pytest
 
-from antenna_models import dipole, radiated, resonance, sheen
+from antenna_models import OracleRaster, dipole, radiated, resonance, sheen
 from fieldgrid_b200 import antenna as A
 from fieldgrid_b200 import fdtd
 from oracle import oracle as O
@@ -62,12 +62,15 @@ def test_the_dipole_on_the_gpu_agrees_with_the_oracle(dipole_out):
     assert abs(tc / tg - 1.0) < 0.01 and abs(pc / pg - 1.0) < 0.01
 
 
-def test_sheens_microstrip_patch_resonates_where_it_was_measured(gpu):
-    out = A.run_gpu(sheen(), A.Options(far_field=False), g=gpu)
+@pytest.mark.parametrize("meshed", [False, True])
+def test_sheens_microstrip_patch_resonates_where_it_was_measured(gpu, meshed):
+    """tests/fdtd.rs:158-165 (sims-antenna), box and meshed (rasterised) forms."""
+    out = A.run_gpu(sheen(meshed), A.Options(far_field=False), g=gpu)
     s11 = np.abs(out.s11())
     q = int(np.argmin(s11))
     f, db = float(out.sweep.freqs[q]), 20.0 * math.log10(s11[q])
-    print(f"sheen: {out.stats.steps} steps, {out.stats.cells} cells: S11 {db:.1f} dB at {f / 1e9:.4f} GHz")
+    print(f"sheen (meshed {meshed}): {out.stats.steps} steps, {out.stats.cells} cells: S11 {db:.1f} dB at "
+          f"{f / 1e9:.4f} GHz")
     assert abs(f / 7.5e9 - 1.0) < 0.015, f
     assert db < -10.0, db
 
@@ -79,3 +82,18 @@ def test_a_volume_result_reports_consistent_gains(dipole_out):
           f"broadside {broadside:.3f}")
     assert abs(broadside - r.dbi) < 0.2, (broadside, r.dbi)
     assert r.gain_dbi((0.0, 0.0, 1.0)) < r.dbi - 20.0
+
+
+def test_the_cuda_rasteriser_builds_the_oracles_sim_arguments(gpu):
+    """The meshed Sheen patch's materials and PEC mask through the CUDA rasteriser equal those
+    through the oracle's, bit for bit."""
+    from fieldgrid_b200.raster import GpuRaster
+    model = sheen(True)
+    grid = A.mesh(model, 8)
+    a = A.sim_args(grid, model, model.port, GpuRaster(gpu))
+    b = A.sim_args(grid, model, model.port, OracleRaster())
+    for name in ("eps", "inf", "sigma", "debye"):
+        assert np.array_equal(getattr(a[1], name), getattr(b[1], name)), name
+    assert np.array_equal(np.asarray(a[2]), np.asarray(b[2]))
+    assert np.asarray(a[2]).any()
+

@@ -19,6 +19,7 @@ same grid.
 from __future__ import annotations
 
 import argparse
+import copy
 import json
 import math
 import os
@@ -69,12 +70,14 @@ def parse():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-extras", action="store_true",
                    help="throughput: skip the batched and adjoint ratios that the line also carries")
-    p.add_argument("--workload", choices=["throughput", "adjoint", "batched", "batched-adjoint"], default="throughput",
+    p.add_argument("--workload", choices=["throughput", "adjoint", "batched", "batched-adjoint", "antenna"],
+                   default="throughput",
                    help="throughput: the 512^3 spheres step (the headline); adjoint: the flux-objective "
                         "gradient over a 32x32x8 design block on 160x160x96 cells, 4000 steps; batched: 192 "
                         "grids of U{48..160}^3 cells stepped together vs one after another, 1500 steps; "
                         "batched-adjoint: the same grids with a 16^3 design block each, their flux gradients "
-                        "together vs one after another")
+                        "together vs one after another; antenna: the 256x256x192 patch antenna with its NTFF box at "
+                        "3 frequencies, 6000 steps, and its far field")
     p.add_argument("--count", type=int, default=192, help="batched: grids in the batch")
     p.add_argument("--group", type=int, default=16, help="batched-adjoint: gradients in flight together")
     p.add_argument("--checkpoints", type=int, default=64, help="adjoint: field checkpoints (0: keep the history)")
@@ -298,6 +301,95 @@ def run_adjoint(args):
     return line
 
 
+def run_antenna(args):
+    """The antenna workload: the patch antenna of 256x256x192 cells (12-cell CPML, PEC ground and
+    patch on a 2-cell substrate, one 50-ohm port) with the near-to-far-field box 3 cells inside the
+    CPML accumulating at 8, 10 and 12 GHz, all 6000 steps device-timed; then the far field on the
+    5-degree theta/phi grid at each frequency (f64, device), and one fg_run of the same steps on
+    host buffers (pack, upload, steps, read-back of the series and NTFF accumulators)."""
+    import numpy as np
+    import torch
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    from fieldgrid_b200 import fdtd
+    from fieldgrid_b200 import workloads as W
+    from fieldgrid_b200.gpu import Gpu, Options
+    g = Gpu.open(Options(device=local))
+    K = args.steps if args.steps != 2000 else 6000
+    Wm = max(args.warmup, 3)
+    kt_steps = 10
+    sc = W.patch_antenna(steps=Wm + K + kt_steps)
+    sim = fdtd.Sim.try_new(*sc.args())
+    pt = fdtd.patches(sim, sc.info["ntff_inset"])
+    sc.extras.ntff = pt.gpu
+    n = sim.dims()
+    nn = n[0] * n[1] * n[2]
+    s = fdtd.Session(g, sim, 0, sc.pulse, sc.extras)
+    stream = torch.cuda.ExternalStream(s.stream)
+    s.step(Wm)
+    s.sync()
+    sampler = ClockSampler(device_id(local))
+    time.sleep(0.3)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    s.step(K)
+    ev1.record(stream)
+    ev1.synchronize()
+    clocks = sampler.stop()
+    ms = max_over_ranks(ev0.elapsed_time(ev1), world)
+    kt = s.kernel_times(kt_steps)
+    launches = s.launches_per_step
+    variant = s.variant
+    s.close()
+    field_parts = [k for k in ("fused_step", "shell_h", "shell_e", "update_h", "update_e") if k in kt]
+    dom_ms = sum(kt[k] for k in field_parts)
+    total_kt = sum(kt.values())
+    peak, peak_src = measured_peaks()
+    achieved = BYTES_PER_NODE * nn / (dom_ms / 1e3) / 1e9
+    # the far field of the accumulated box on the 5-degree grid (37 x 72 directions), per frequency
+    ex = copy.copy(sc.extras)
+    ex.max_steps = K
+    t0 = time.perf_counter()
+    rec = fdtd.run(g, sim, 0, sc.pulse, ex)
+    torch.cuda.synchronize()
+    t_e2e = max_over_ranks(time.perf_counter() - t0, world)
+    th = np.deg2rad(np.arange(0, 181, 5, dtype=np.float64))
+    ph = np.deg2rad(np.arange(0, 360, 5, dtype=np.float64))
+    T, P = np.meshgrid(th, ph, indexing="ij")
+    dirs = np.stack([np.sin(T) * np.cos(P), np.sin(T) * np.sin(P), np.cos(T)], -1).reshape(-1, 3)
+    nf = len(sc.extras.freqs)
+    t0 = time.perf_counter()
+    peaks = []
+    for k, f in enumerate(sc.extras.freqs):
+        far = fdtd.Far.load(pt, rec.ntff, nf, k, f, gpu=g)
+        peaks.append(float(far.intensities(dirs).max()))
+    far_ms = (time.perf_counter() - t0) * 1e3
+    if rank != 0:
+        return None
+    return {
+        "metric": "Mcell-updates/s", "value": job_rate(nn, K, world, ms), "unit": "Mcell/s", "n_gpus": world,
+        "steps": K, "warmup": Wm, "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": sc.name + ", NTFF box at 8/10/12 GHz", "nodes": nn, "pml": sc.info["pml"],
+                   "patches": int(len(pt.area)), "freqs": list(sc.extras.freqs), "variant": variant,
+                   "launches_per_step": launches},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "kernel": "field_update", "kernels": field_parts, "kernel_ms": dom_ms, "peak_source": peak_src},
+        "kernel_ms": {k: round(v, 5) for k, v in kt.items()},
+        "kernel_share": {k: round(v / total_kt, 4) for k, v in kt.items()},
+        "ntff_share": round(kt.get("ntff", 0.0) / total_kt, 4),
+        "gpu_launches": launches * K,
+        "clocks": clocks,
+        "e2e": {"value": job_rate(nn, K, world, t_e2e * 1e3), "unit": "Mcell/s", "h2d_bytes_per_step": rec.h2d / K,
+                "d2h_bytes_per_step": rec.d2h / K,
+                "run": f"one fg_run of {K} steps on host buffers: pack + upload, the steps, read-back of the series "
+                       f"and the NTFF accumulators; wall clock"},
+        "far_field": {"directions": int(len(dirs)), "freqs": nf, "ms": far_ms, "peak_intensity": peaks},
+    }
+
+
 def run_batched(args):
     """The batched workload: the same grids stepped one after another (a session per grid, its
     graphs, the TMA march where a clean box exists) and together (one batch); device-timed
@@ -427,8 +519,8 @@ def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
-    if args.workload in ("adjoint", "batched"):
-        line = (run_adjoint if args.workload == "adjoint" else run_batched)(args)
+    if args.workload in ("adjoint", "batched", "antenna"):
+        line = {"adjoint": run_adjoint, "batched": run_batched, "antenna": run_antenna}[args.workload](args)
         if line is not None:
             print(json.dumps(line), flush=True)
         return 0
@@ -517,7 +609,6 @@ def main():
 
     e2e = None
     if not args.no_e2e:
-        import copy
         ex = copy.copy(sc.extras)
         ex.max_steps = K
         torch.cuda.synchronize()

@@ -242,6 +242,12 @@ struct Session {
     CUtensorMap d1_e[3], d1_h[3], d1_pze[3], d1_pzh[3];            // the one-step march's, per set/slot
     cudaStream_t side = nullptr;
     cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
+    // graph-captured fused steps: the plane DFT and the NTFF accumulation of step n run on `aux`
+    // beside step n + 1 (which only reads the fields they read); step n + 2, which overwrites those
+    // fields, waits for them (aux_done of the same parity), and every captured graph joins them
+    cudaStream_t aux = nullptr;
+    cudaEvent_t aux_ready[2] = {nullptr, nullptr}, aux_done[2] = {nullptr, nullptr};
+    bool aux_on = false, aux_pending[2] = {false, false};
     std::map<int, cudaGraphExec_t> slot_graphs;      // captured steps by (kind, phase t mod 6)
     std::vector<void*> extra_allocs;
 };
@@ -547,6 +553,10 @@ int enqueue_step(Session& s, int parity, std::string& err) {
             mark("wire_h");
             k_wire_h<<<(s.n_wires + 127) / 128, 128, 0, st>>>(s.wires, s.n_wires, e_in, h_in);
         }
+        if (s.aux_on && s.aux_pending[parity]) {   // this step overwrites what step n - 2's extras read
+            FG_CUDA(cudaStreamWaitEvent(st, s.aux_done[parity], 0));
+            s.aux_pending[parity] = false;
+        }
         mark("fused_step");
         const bool tma = s.tma.ok && !s.direct;
         int rc = s.direct && s.boxed
@@ -601,13 +611,26 @@ int enqueue_step(Session& s, int parity, std::string& err) {
         if (probes) mark("probe");
         if (probes) k_probe<<<s.n_ports, 256, 0, st>>>(s.probes, s.port_edges, s.loops, g.cs, e_now, h_now, s.counter, s.sc, s.series);
     }
+    const bool branch = s.aux_on && s.fused && (s.plane_len || s.ntff_len) && !s.quiet;
+    cudaStream_t xs = branch ? s.aux : st;
+    const int xpar = branch ? parity : -1;
+    if (branch) {
+        FG_CUDA(cudaEventRecord(s.aux_ready[parity], st));
+        FG_CUDA(cudaStreamWaitEvent(s.aux, s.aux_ready[parity], 0));
+    }
     if (s.plane_len && !s.quiet) {
         long long q = (long long)g.n0 * g.n1;
         mark("field_dft");
-        k_field_dft<<<unsigned((q + 127) / 128), 128, 0, st>>>(g, s.plane_k, s.sc, s.counter, e_now, h_now, s.plane);
+        k_field_dft<<<unsigned((q + 127) / 128), 128, 0, xs>>>(g, s.plane_k, s.sc, s.counter, xpar, e_now, h_now, s.plane);
     }
     if (s.ntff_len && !s.quiet) mark("ntff");
-    if (s.ntff_len && !s.quiet) k_ntff<<<(s.n_patches + 127) / 128, 128, 0, st>>>(s.patch, s.n_patches, g.cs, s.sc, s.counter, e_now, h_now, s.ntff);
+    if (s.ntff_len && !s.quiet)
+        k_ntff<<<(s.n_patches + 127) / 128, 128, 0, xs>>>(s.patch, s.n_patches, g.cs, s.sc, s.counter, xpar, e_now,
+                                                          h_now, s.ntff);
+    if (branch) {
+        FG_CUDA(cudaEventRecord(s.aux_done[parity], s.aux));
+        s.aux_pending[parity] = true;
+    }
     if (s.n_design && s.fused && (s.quiet || s.design_in_steps)) {
         mark("design_record");
         k_design_record<<<(s.n_design + 127) / 128, 128, 0, st>>>(g, s.design, s.n_design, e_in, h_now, s.psi, s.counter,
@@ -644,7 +667,14 @@ int capture(Session& s, int steps, int parity0, cudaGraphExec_t* out, std::strin
     cudaGraph_t graph;
     FG_CUDA(cudaStreamBeginCapture(s.stream, cudaStreamCaptureModeThreadLocal));
     int rc = FG_OK;
+    s.aux_on = s.aux != nullptr;
     for (int q = 0; q < steps && rc == FG_OK; ++q) rc = enqueue_step(s, (parity0 + q) & 1, err);
+    for (int p = 0; p < 2; ++p)   // the graph ends with its extras joined
+        if (s.aux_pending[p]) {
+            if (rc == FG_OK && cudaStreamWaitEvent(s.stream, s.aux_done[p], 0) != cudaSuccess) rc = FG_ERR_CUDA;
+            s.aux_pending[p] = false;
+        }
+    s.aux_on = false;
     cudaError_t ce = cudaStreamEndCapture(s.stream, &graph);
     if (rc) return rc;
     if (ce != cudaSuccess) { err = std::string("cudaStreamEndCapture: ") + cudaGetErrorString(ce); return FG_ERR_CUDA; }
@@ -1589,8 +1619,11 @@ int session_new(Gpu* gpu, const HostSim& sim, const RunSpec& rs, Session** out, 
         return FG_OK;
     };
     int rc = FG_OK;
+    // the patch records word-major (k_ntff): word m of patch g at m * patches + g
     std::vector<uint32_t> patch_dev(rs.ntff.size());
-    for (size_t q = 0; q < rs.ntff.size(); ++q) patch_dev[q] = q % 13 == 0 ? rs.ntff[q] : uint32_t(dev(rs.ntff[q]));
+    const size_t npatch = rs.ntff.size() / 13;
+    for (size_t q = 0; q < rs.ntff.size(); ++q)
+        patch_dev[(q % 13) * npatch + q / 13] = q % 13 == 0 ? rs.ntff[q] : uint32_t(dev(rs.ntff[q]));
     if (!rs.ntff.empty() && 3ull * uint64_t(cs) >= (1ull << 32)) { err = "the NTFF box needs 64-bit indices on this grid"; return FG_ERR_UNSUPPORTED; }
     rc |= up(s->patch, patch_dev.data(), patch_dev.size() * 4);
     rc |= up(s->sources, src.data(), src.size() * sizeof(DevSource));
@@ -1697,6 +1730,13 @@ int session_new(Gpu* gpu, const HostSim& sim, const RunSpec& rs, Session** out, 
         *out = s.release();
         return FG_OK;
     }
+    if (s->fused && (s->plane_len || s->ntff_len) && s->n_wires == 0 && s->n_sheets == 0) {
+        FG_CUDA(cudaStreamCreateWithFlags(&s->aux, cudaStreamNonBlocking));
+        for (int p = 0; p < 2; ++p) {
+            FG_CUDA(cudaEventCreateWithFlags(&s->aux_ready[p], cudaEventDisableTiming));
+            FG_CUDA(cudaEventCreateWithFlags(&s->aux_done[p], cudaEventDisableTiming));
+        }
+    }
     // graphs: a block of even length (the fused step alternates buffers), a pair and singles
     s->graph_steps = 32;
     rc = capture(*s, s->graph_steps, 0, &s->graph_many, err);
@@ -1721,6 +1761,11 @@ void session_free(Session* s) {
     if (s->side) cudaStreamDestroy(s->side);
     if (s->fork_ev) cudaEventDestroy(s->fork_ev);
     if (s->join_ev) cudaEventDestroy(s->join_ev);
+    if (s->aux) cudaStreamDestroy(s->aux);
+    for (int p = 0; p < 2; ++p) {
+        if (s->aux_ready[p]) cudaEventDestroy(s->aux_ready[p]);
+        if (s->aux_done[p]) cudaEventDestroy(s->aux_done[p]);
+    }
     if (s->arena) cudaFree(s->arena);
     cudaFree(s->design);
     cudaFree(s->hist_e);
@@ -1862,7 +1907,17 @@ int session_read(Session* s, const std::string& which, float* dst, uint64_t len,
         return copy(s->series, n);
     }
     if (which == "plane") return copy(s->plane, s->plane_len);
-    if (which == "ntff") return copy(s->ntff, s->ntff_len);
+    if (which == "ntff") {
+        // the device keeps (frequency, value) major; the record is patch major (cpu.rs:363-415)
+        if (s->ntff_len > len) { err = "destination too small for ntff"; return FG_ERR_INVALID; }
+        std::vector<float> t(s->ntff_len);
+        if (s->ntff_len) FG_CUDA(cudaMemcpy(t.data(), s->ntff, s->ntff_len * 4, cudaMemcpyDeviceToHost));
+        s->d2h_bytes += s->ntff_len * 4;
+        const uint64_t P = uint64_t(s->n_patches), per = uint64_t(s->sc.nf) * 12;
+        for (uint64_t g = 0; g < P; ++g)
+            for (uint64_t m = 0; m < per; ++m) dst[g * per + m] = t[m * P + g];
+        return FG_OK;
+    }
     if (which == "e" || which == "h") {
         float *e, *h;
         latest(s, &e, &h);

@@ -73,6 +73,15 @@ __device__ __forceinline__ long long psi_at(const Geom& g, int a, int i, int j, 
 // The step index n of the running step: the first kernel of step n raised the counter to n + 1.
 __device__ __forceinline__ unsigned step_index(const unsigned* counter) { return *(volatile const unsigned*)counter - 1u; }
 
+// The step index for a kernel that may run beside the next step's kernels (the next step's first
+// kernel opens step n + 1 by incrementing the counter, and the step after that waits for this
+// kernel): the step of parity `parity` among the two the counter can show (parity -1: the kernel
+// runs in order, the counter's step).
+__device__ __forceinline__ unsigned step_of(const unsigned* counter, int parity) {
+    const unsigned n = step_index(counter);
+    return (parity < 0 || int(n & 1u) == parity) ? n : n - 1u;
+}
+
 // cpu.rs:270-273: h[w.h] += sum of four c*E terms, after the H update, with E not yet updated.
 __global__ void k_wire_h(const DevWire* __restrict__ w, int count, const float* __restrict__ e, float* __restrict__ h) {
     int s = blockIdx.x * blockDim.x + threadIdx.x;
@@ -325,11 +334,11 @@ __global__ void k_lumped_probe(const DevSource* __restrict__ src, int ns, DevInd
 
 // cpu.rs:336-361: running DFT of Ex, Ey, Ez (at (n+1) dt) and Hx, Hy (at (n+1/2) dt) on the
 // z-plane k = plane_k; phases formed in f32 like the CPU path.
-__global__ void k_field_dft(Geom g, int plane_k, StepConst sc, const unsigned* __restrict__ counter,
+__global__ void k_field_dft(Geom g, int plane_k, StepConst sc, const unsigned* __restrict__ counter, int parity,
                             const float* __restrict__ e, const float* __restrict__ h, float* __restrict__ acc) {
     const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= (long long)g.n0 * g.n1) return;
-    const unsigned n = step_index(counter);
+    const unsigned n = step_of(counter, parity);
     const float te = (float(n) + 1.0f) * sc.dt, th = (float(n) + 0.5f) * sc.dt;
     const long long id = q * g.p2 + plane_k;
     const float f[5] = {e[id], e[g.cs + id], e[2 * g.cs + id], h[id], h[g.cs + id]};
@@ -354,14 +363,19 @@ __global__ void k_field_dft(Geom g, int plane_k, StepConst sc, const unsigned* _
 }
 
 // cpu.rs:363-415: per NTFF patch, tangential E (2-edge mean) and H (4-edge mean), J = n x H,
-// M = E x n, accumulated with dt e^{-j w t}.
+// M = E x n, accumulated with dt e^{-j w t}. Component-major on the device so a warp's loads and
+// stores coalesce: the patch record's word m of patch g at pidx[m * patches + g], accumulator
+// (frequency k, value c of 12) at acc[(k * 12 + c) * patches + g] (read back in the reference's
+// patch-major order).
 __global__ void k_ntff(const unsigned* __restrict__ pidx, int patches, long long cs, StepConst sc,
-                       const unsigned* __restrict__ counter, const float* __restrict__ e, const float* __restrict__ h,
-                       float* __restrict__ acc) {
+                       const unsigned* __restrict__ counter, int parity, const float* __restrict__ e,
+                       const float* __restrict__ h, float* __restrict__ acc) {
     const int g = blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= patches) return;
-    const unsigned n = step_index(counter);
-    const unsigned* b = pidx + (long long)g * 13;
+    const unsigned n = step_of(counter, parity);
+    unsigned b[13];
+#pragma unroll
+    for (int m = 0; m < 13; ++m) b[m] = pidx[(long long)m * patches + g];
     const unsigned meta = b[0];
     const int axis = meta & 3;
     const float side = (meta & 4) ? 1.0f : -1.0f;
@@ -376,7 +390,6 @@ __global__ void k_ntff(const unsigned* __restrict__ pidx, int patches, long long
     const float jv[3] = {nrm[1] * hf[2] - nrm[2] * hf[1], nrm[2] * hf[0] - nrm[0] * hf[2], nrm[0] * hf[1] - nrm[1] * hf[0]};
     const float mv[3] = {ef[1] * nrm[2] - ef[2] * nrm[1], ef[2] * nrm[0] - ef[0] * nrm[2], ef[0] * nrm[1] - ef[1] * nrm[0]};
     const float te = (float(n) + 1.0f) * sc.dt, th = (float(n) + 0.5f) * sc.dt;
-    float* out = acc + (long long)g * sc.nf * 12;
     for (int k = 0; k < sc.nf; ++k) {
         const float wf = sc.omega[k];
         float pe0, pe1, ph0, ph1;
@@ -387,13 +400,13 @@ __global__ void k_ntff(const unsigned* __restrict__ pidx, int patches, long long
             pe0 = cosf(-wf * te) * sc.dt; pe1 = sinf(-wf * te) * sc.dt;
             ph0 = cosf(-wf * th) * sc.dt; ph1 = sinf(-wf * th) * sc.dt;
         }
-        float* o = out + k * 12;
+        float* o = acc + (long long)k * 12 * patches + g;
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
-            o[2 * c] += ph0 * jv[c];
-            o[2 * c + 1] += ph1 * jv[c];
-            o[6 + 2 * c] += pe0 * mv[c];
-            o[6 + 2 * c + 1] += pe1 * mv[c];
+            o[(long long)(2 * c) * patches] += ph0 * jv[c];
+            o[(long long)(2 * c + 1) * patches] += ph1 * jv[c];
+            o[(long long)(6 + 2 * c) * patches] += pe0 * mv[c];
+            o[(long long)(6 + 2 * c + 1) * patches] += pe1 * mv[c];
         }
     }
 }

@@ -10,9 +10,15 @@
 // sums, and marches that tile (fused_tile, stencil_fused.cuh). Large grids therefore fill the GPU
 // while small ones finish in the same launch, with no per-grid launch or tail.
 //
+// Merged mode (tile 5): one launch of the TMA march over every grid's clean box (k_batch_tma: the
+// grids' tensor maps and march arguments in HBM, one block per tile of any grid), one launch each
+// of the two CPML shell kernels over every grid's shell rows, then the Debye, source and probe
+// launches above: seven launches per step for the whole batch, with each grid's arithmetic that of
+// its own TMA step.
+//
 // The autotuner times a few steps of each candidate (tile shape, blocks per SM of the persistent
-// launch, planes per item) on the real batch, keeps the fastest, resets every grid to step 0 and
-// captures the graphs with it.
+// launch, planes per item; graph branches; the merged launches) on the real batch, keeps the
+// fastest, resets every grid to step 0 and captures the graphs with it.
 //
 // Included at the end of engine.cu (it builds on Session).
 #pragma once
@@ -40,6 +46,7 @@ struct BatchInstance {
     float* series;
     float* e[2];
     float* h[2];
+    int opens;                      // 1: k_batch_begin opens this grid's step (0: its own march does)
 };
 
 // the index b with first[b] <= t < first[b + 1]
@@ -56,7 +63,7 @@ __device__ __forceinline__ int batch_find(const long long* __restrict__ first, i
 // Opens step n of every grid (the counters the later kernels read) and rewinds the work-list.
 __global__ void k_batch_begin(const BatchInstance* __restrict__ bi, int n, unsigned long long* queue) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t < n) *bi[t].counter += 1u;
+    if (t < n && bi[t].opens) *bi[t].counter += 1u;
     if (t == 0) *queue = 0ull;
 }
 
@@ -124,6 +131,7 @@ struct BatchShape {
 // branches run concurrently
 constexpr int BATCH_BRANCHES = 3;          // graph branches, each grid's own step (TMA march + shell)
 constexpr int BATCH_BRANCHES_DIRECT = 4;   // graph branches with the direct-load fused march
+constexpr int BATCH_MERGED = 5;            // one TMA march and one shell launch over all grids
 
 constexpr int BATCH_TILES[3][2] = {{32, 8}, {64, 4}, {32, 4}};
 
@@ -148,7 +156,140 @@ struct Batch {
     std::vector<std::pair<BatchShape, double>> trials;
     cudaEvent_t fork = nullptr;        // graph branches: the fork and one join per grid
     std::vector<cudaEvent_t> join;
+    // merged mode
+    bool merged_ok = false;
+    std::string merged_why;
+    TmaGrid* d_tma = nullptr;          // the merged grids: per-block class tables first, then global ids
+    int* d_tma_block = nullptr;        // per march block: its grid
+    int tma_blocks = 0, tma_blocks_local = 0;   // blocks in all, blocks of the first launch
+    ShellGrid* d_shell = nullptr;
+    int* d_shell_block = nullptr;      // per shell block: its grid
+    int shell_blocks = 0;
+    std::vector<int> merged_rest;      // grids the merged launches leave to their own direct-load march
 };
+
+constexpr auto batch_tma_local =
+    k_batch_tma<TMA_TJ, TMA_TK, uint8_t, TMA_SHAPES[0].stages, TMA_SEGMAX, true, TMA_SHAPES[0].minb>;
+template <typename CID>
+constexpr auto batch_tma_global = k_batch_tma<TMA_TJ, TMA_TK, CID, TMA_SHAPES[0].stages, TMA_SEGMAX, false, TMA_SHAPES[0].minb>;
+
+// f(kernel, smem) for the merged march of grids with (local) or without per-block tables
+template <typename F>
+void with_batch_tma(bool local, int cid_bytes, F&& f) {
+    if (local) f(batch_tma_local, tma_smem_s<uint8_t, true, 0>());
+    else if (cid_bytes == 1) f(batch_tma_global<uint8_t>, tma_smem_s<uint8_t, false, 0>());
+    else if (cid_bytes == 2) f(batch_tma_global<uint16_t>, tma_smem_s<uint16_t, false, 0>());
+    else f(batch_tma_global<uint32_t>, tma_smem_s<uint32_t, false, 0>());
+}
+
+// The merged mode's descriptors: the grids with per-block class tables march in one launch, those
+// with global class ids in a second (as each grid's own session chose); a grid without a TMA march
+// (no clean box) runs its own direct-load march in the step.
+int batch_merged_setup(Batch& B, std::string& err) {
+    B.merged_ok = false;
+    B.merged_rest.clear();
+    B.tma_blocks_local = 0;
+    std::vector<TmaGrid> tg;
+    std::vector<int> tblock, sblock;
+    std::vector<ShellGrid> sg;
+    std::vector<size_t> order;   // the grids with tables first
+    for (int pass = 0; pass < 2; ++pass)
+        for (size_t b = 0; b < B.s.size(); ++b)
+            if (B.s[b]->tma.ok && B.s[b]->tma.shape == 0 && B.s[b]->local == (pass == 0)) order.push_back(b);
+    for (size_t b = 0; b < B.s.size(); ++b)
+        if (!B.s[b]->tma.ok || B.s[b]->tma.shape != 0) B.merged_rest.push_back(int(b));
+    for (size_t b : order) {
+        Session& s = *B.s[b];
+        if (s.local) B.tma_blocks_local = int(tblock.size()) + s.tma.blocks;
+        const TmaPlan& t = s.tma;
+        TmaGrid G{};
+        for (int p = 0; p < 2; ++p) { G.e[p] = t.e[p]; G.h[p] = t.h[p]; G.pzh[p] = t.pz ? t.pzh[p] : t.c; }
+        G.c = t.c;
+        G.pze = t.pz ? t.pze : t.c;
+        // the grid's first block in its launch (the second launch starts after the local grids' blocks)
+        const int first = int(tblock.size()) - (s.local ? 0 : B.tma_blocks_local);
+        for (int p = 0; p < 2; ++p) {   // launch_tma's arguments for input set p
+            float* e_out = p ? s.e : s.e2;
+            float* h_out = p ? s.h : s.h2;
+            float* psi_h_out = p ? s.psi : s.psi_h2;
+            G.a[p] = TmaArgs{s.geom, s.classes, e_out, h_out, s.sc.k_mu, s.clean_lo[2], s.clean_hi[1], s.clean_hi[2],
+                             s.tma_blocks, s.tma_own, -first, 0, s.psi, psi_h_out, s.tables, s.counter, s.error,
+                             s.wait_ns, -0.0f, s.stall_plane};
+        }
+        // blocks index the merged grids (tg), not the batch's grids: some of those march on their own
+        const int gi = int(tg.size());
+        tg.push_back(G);
+        for (int q = 0; q < t.blocks; ++q) tblock.push_back(gi);
+        const unsigned rows = s.shell.ra + s.shell.rb + s.shell.rc;
+        if (rows) {
+            ShellGrid S{};
+            S.g = s.geom;
+            S.b = s.shell;
+            S.kx = s.kax;
+            S.node_class = s.node_class;
+            S.classes = s.classes;
+            for (int p = 0; p < 2; ++p) {
+                S.e_in[p] = p ? s.e2 : s.e;
+                S.h_in[p] = p ? s.h2 : s.h;
+                S.e_out[p] = p ? s.e : s.e2;
+                S.h_out[p] = p ? s.h : s.h2;
+                S.psi_h_in[p] = p ? s.psi_h2 : s.psi;
+                S.psi_h_out[p] = p ? s.psi : s.psi_h2;
+            }
+            S.psi = s.psi;
+            S.k_mu = s.sc.k_mu;
+            S.block0 = int(sblock.size());
+            const unsigned nb = (rows + SHELL_THREADS / 32 - 1) / (SHELL_THREADS / 32);
+            for (unsigned q = 0; q < nb; ++q) sblock.push_back(int(sg.size()));
+            sg.push_back(S);
+        }
+    }
+    // every block's grid and its index in that grid's block list, checked before any launch
+    for (size_t q = 0; q < tblock.size(); ++q) {
+        const int gi = tblock[q];
+        const long long launch_q = (long long)q - (q >= size_t(B.tma_blocks_local) ? B.tma_blocks_local : 0);
+        const long long local = launch_q + tg[size_t(gi)].a[0].block0;
+        const Session* owner = nullptr;
+        for (Session* x : B.s)
+            if (x->tma_blocks == tg[size_t(gi)].a[0].blocks) owner = x;
+        if (gi < 0 || size_t(gi) >= tg.size() || !owner || local < 0 || local >= owner->tma.blocks ||
+            tg[size_t(gi)].a[0].block0 != tg[size_t(gi)].a[1].block0) {
+            err = "internal: a merged march block outside its grid's block list";
+            return FG_ERR_INVALID;
+        }
+    }
+    for (size_t q = 0; q < sblock.size(); ++q) {
+        const int gi = sblock[q];
+        const ShellGrid& S = sg[size_t(gi)];
+        const long long rows = (long long)(q - size_t(S.block0)) * (SHELL_THREADS / 32);
+        if (gi < 0 || size_t(gi) >= sg.size() || rows < 0 || rows >= (long long)(S.b.ra + S.b.rb + S.b.rc)) {
+            err = "internal: a merged shell block outside its grid's rows";
+            return FG_ERR_INVALID;
+        }
+    }
+    cudaError_t ce = cudaSuccess;
+    for (bool local : {true, false})
+        with_batch_tma(local, B.cid_bytes, [&](auto kern, int smem) {
+            if (ce == cudaSuccess) ce = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        });
+    FG_CUDA(ce);
+    FG_CUDA(cudaMalloc(&B.d_tma, std::max<size_t>(tg.size(), 1) * sizeof(TmaGrid)));
+    FG_CUDA(cudaMalloc(&B.d_tma_block, std::max<size_t>(tblock.size(), 1) * sizeof(int)));
+    FG_CUDA(cudaMalloc(&B.d_shell, std::max<size_t>(sg.size(), 1) * sizeof(ShellGrid)));
+    FG_CUDA(cudaMalloc(&B.d_shell_block, std::max<size_t>(sblock.size(), 1) * sizeof(int)));
+    if (!tg.empty()) {
+        FG_CUDA(cudaMemcpy(B.d_tma, tg.data(), tg.size() * sizeof(TmaGrid), cudaMemcpyHostToDevice));
+        FG_CUDA(cudaMemcpy(B.d_tma_block, tblock.data(), tblock.size() * sizeof(int), cudaMemcpyHostToDevice));
+    }
+    if (!sg.empty()) {
+        FG_CUDA(cudaMemcpy(B.d_shell, sg.data(), sg.size() * sizeof(ShellGrid), cudaMemcpyHostToDevice));
+        FG_CUDA(cudaMemcpy(B.d_shell_block, sblock.data(), sblock.size() * sizeof(int), cudaMemcpyHostToDevice));
+    }
+    B.tma_blocks = int(tblock.size());
+    B.shell_blocks = int(sblock.size());
+    B.merged_ok = true;
+    return FG_OK;
+}
 
 template <typename F>
 bool with_batch_march(int cid_bytes, int tile, F&& f) {
@@ -171,6 +312,12 @@ int batch_apply_shape(Batch& B, const BatchShape& sh, std::string& err) {
         s->direct = sh.tile == BATCH_BRANCHES_DIRECT && (sh.seg <= 0 || s->geom.nn < 1000LL * sh.seg);
         // the other grids fill the GPU: long x-segments, few halo planes
         if (s->direct) s->shape.seg = 64;
+    }
+    for (size_t b = 0; b < B.inst.size(); ++b) B.inst[b].opens = 1;
+    if (sh.tile == BATCH_MERGED) {
+        if (!B.merged_ok) { err = "merged batch launches: " + B.merged_why; return FG_ERR_INVALID; }
+        for (int b : B.merged_rest) B.inst[size_t(b)].opens = 0;   // their own march opens their step
+        FG_CUDA(cudaMemcpy(B.d_inst, B.inst.data(), B.inst.size() * sizeof(BatchInstance), cudaMemcpyHostToDevice));
     }
     if (sh.tile >= BATCH_BRANCHES) {
         B.shape = sh;
@@ -206,7 +353,7 @@ int batch_apply_shape(Batch& B, const BatchShape& sh, std::string& err) {
 int batch_enqueue_step(Batch& B, int parity, std::string& err) {
     cudaStream_t st = B.stream;
     const int n = int(B.s.size());
-    if (B.shape.tile >= BATCH_BRANCHES) {
+    if (B.shape.tile >= BATCH_BRANCHES && B.shape.tile != BATCH_MERGED) {
         // fork every grid's stream from the batch stream, step it there, join back
         FG_CUDA(cudaEventRecord(B.fork, st));
         for (int b = 0; b < n; ++b) {
@@ -220,10 +367,42 @@ int batch_enqueue_step(Batch& B, int parity, std::string& err) {
         return FG_OK;
     }
     k_batch_begin<<<(n + 127) / 128, 128, 0, st>>>(B.d_inst, n, B.d_queue);
-    with_batch_march(B.cid_bytes, B.shape.tile, [&](auto kern, int tk, int tj) {
-        kern<<<B.persistent_blocks, dim3(tk, tj), 0, st>>>(B.d_inst, B.d_items, n, B.d_queue, parity);
-        return true;
-    });
+    if (B.shape.tile == BATCH_MERGED) {
+        // every grid's march (its input set `parity`), then every grid's shell H and E; the grids
+        // left out march on their own
+        const int nl = B.tma_blocks_local, ng = B.tma_blocks - B.tma_blocks_local;
+        if (nl > 0)
+            with_batch_tma(true, B.cid_bytes, [&](auto kern, int smem) {
+                kern<<<unsigned(nl), TMA_CONSUMERS + 32, smem, st>>>(B.d_tma, B.d_tma_block, parity);
+            });
+        if (ng > 0)   // the second launch's blocks start at block nl of the list: offset the index
+            with_batch_tma(false, B.cid_bytes, [&](auto kern, int smem) {
+                kern<<<unsigned(ng), TMA_CONSUMERS + 32, smem, st>>>(B.d_tma, B.d_tma_block + nl, parity);
+            });
+        for (int b : B.merged_rest) {
+            Session& S = *B.s[size_t(b)];
+            float *e_in = parity ? S.e2 : S.e, *h_in = parity ? S.h2 : S.h;
+            float *e_out = parity ? S.e : S.e2, *h_out = parity ? S.h : S.h2;
+            if (launch_fused(S.shape, S.cid_bytes, S.geom, S.node_class, S.classes, e_in, h_in, e_out, h_out, S.psi,
+                             parity ? S.psi_h2 : S.psi, parity ? S.psi : S.psi_h2, S.sc.k_mu, S.counter, false, st)) {
+                err = "fused step launch failed";
+                return FG_ERR_CUDA;
+            }
+        }
+        if (B.shell_blocks > 0) {
+            k_batch_shell_h<<<unsigned(B.shell_blocks), SHELL_THREADS, 0, st>>>(B.d_shell, B.d_shell_block, parity);
+            switch (B.cid_bytes) {
+                case 1: k_batch_shell_e<uint8_t><<<unsigned(B.shell_blocks), SHELL_THREADS, 0, st>>>(B.d_shell, B.d_shell_block, parity); break;
+                case 2: k_batch_shell_e<uint16_t><<<unsigned(B.shell_blocks), SHELL_THREADS, 0, st>>>(B.d_shell, B.d_shell_block, parity); break;
+                default: k_batch_shell_e<uint32_t><<<unsigned(B.shell_blocks), SHELL_THREADS, 0, st>>>(B.d_shell, B.d_shell_block, parity); break;
+            }
+        }
+    } else {
+        with_batch_march(B.cid_bytes, B.shape.tile, [&](auto kern, int tk, int tj) {
+            kern<<<B.persistent_blocks, dim3(tk, tj), 0, st>>>(B.d_inst, B.d_items, n, B.d_queue, parity);
+            return true;
+        });
+    }
     if (B.total_edges > 0) {
         const unsigned blocks = unsigned((B.total_edges + 255) / 256);
         switch (B.cid_bytes) {
@@ -251,6 +430,10 @@ void batch_free(Batch* B) {
     cudaFree(B->d_edges);
     cudaFree(B->d_ports);
     cudaFree(B->d_queue);
+    cudaFree(B->d_tma);
+    cudaFree(B->d_tma_block);
+    cudaFree(B->d_shell);
+    cudaFree(B->d_shell_block);
     for (Session* s : B->s) session_free(s);
     if (B->fork) cudaEventDestroy(B->fork);
     for (cudaEvent_t e : B->join) cudaEventDestroy(e);
@@ -262,7 +445,7 @@ int batch_capture(Batch& B, int steps, int parity0, cudaGraphExec_t* out, std::s
     cudaGraph_t graph;
     FG_CUDA(cudaStreamBeginCapture(B.stream, cudaStreamCaptureModeThreadLocal));
     int rc = FG_OK;
-    if (B.shape.tile >= BATCH_BRANCHES) {
+    if (B.shape.tile >= BATCH_BRANCHES && B.shape.tile != BATCH_MERGED) {
         // the grids are independent: each branch runs all the graph's steps, one join at the end
         FG_CUDA(cudaEventRecord(B.fork, B.stream));
         for (size_t b = 0; b < B.s.size() && rc == FG_OK; ++b) {
@@ -273,7 +456,7 @@ int batch_capture(Batch& B, int steps, int parity0, cudaGraphExec_t* out, std::s
             FG_CUDA(cudaStreamWaitEvent(B.stream, B.join[b], 0));
         }
     }
-    for (int q = 0; q < steps && rc == FG_OK && B.shape.tile < BATCH_BRANCHES; ++q)
+    for (int q = 0; q < steps && rc == FG_OK && (B.shape.tile < BATCH_BRANCHES || B.shape.tile == BATCH_MERGED); ++q)
         rc = batch_enqueue_step(B, (parity0 + q) & 1, err);
     cudaError_t ce = cudaStreamEndCapture(B.stream, &graph);
     if (rc) return rc;
@@ -366,6 +549,7 @@ int batch_new(Gpu* gpu, const std::vector<const HostSim*>& sims, const std::vect
         in.series = s.series;
         in.e[0] = s.e; in.e[1] = s.e2;
         in.h[0] = s.h; in.h[1] = s.h2;
+        in.opens = 1;
         B->inst.push_back(in);
         edges[b + 1] = edges[b] + s.n_debye;
         ports[b + 1] = ports[b] + s.n_ports;
@@ -383,7 +567,8 @@ int batch_new(Gpu* gpu, const std::vector<const HostSim*>& sims, const std::vect
     for (auto& e : B->join) FG_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     FG_CUDA(cudaMemcpy(B->d_edges, edges.data(), (n + 1) * 8, cudaMemcpyHostToDevice));
     FG_CUDA(cudaMemcpy(B->d_ports, ports.data(), (n + 1) * 8, cudaMemcpyHostToDevice));
-    int rc = FG_OK;
+    int rc = batch_merged_setup(*B, err);
+    if (rc) return rc;
     // the tuner: each candidate runs a warm-up step then a timed block of steps from the live state
     BatchShape best = fixed;
     if (tune) {
@@ -397,6 +582,7 @@ int batch_new(Gpu* gpu, const std::vector<const HostSim*>& sims, const std::vect
             for (int seg : {16, 32, 64})
                 for (int bps : {0, 2}) cands.push_back(BatchShape{tile, bps, seg});
         cands.push_back(BatchShape{BATCH_BRANCHES, 0, 0});
+        if (B->merged_ok) cands.push_back(BatchShape{BATCH_MERGED, 0, 0});
         for (int below : {0, 300, 1000}) cands.push_back(BatchShape{BATCH_BRANCHES_DIRECT, 0, below});
         for (const BatchShape& sh : cands) {
             if ((rc = batch_apply_shape(*B, sh, err))) break;
@@ -418,6 +604,13 @@ int batch_new(Gpu* gpu, const std::vector<const HostSim*>& sims, const std::vect
         cudaEventDestroy(e1);
         if (rc) return rc;
         B->tuned_ms = best_ms;
+        if (const char* v = std::getenv("FIELDGRID_BATCH_TRIALS"); v && v[0] == '1') {
+            std::fprintf(stderr, "batch tuner: %zu grids, %zu march on their own in the merged mode\n", B->s.size(),
+                         B->merged_rest.size());
+            for (auto& [sh, ms] : B->trials)
+                std::fprintf(stderr, "  tile %d blocks/SM %d seg %d: %.3f ms per step\n", sh.tile, sh.blocks_per_sm,
+                             sh.seg, ms);
+        }
         if ((rc = batch_reset(*B, err))) return rc;
     }
     if ((rc = batch_apply_shape(*B, best, err))) return rc;
@@ -432,7 +625,7 @@ int batch_new(Gpu* gpu, const std::vector<const HostSim*>& sims, const std::vect
 int batch_new_c(Gpu* gpu, const std::vector<const HostSim*>& sims, const std::vector<RunSpec>& specs, bool tune,
                 int tile, int blocks_per_sm, int seg, int graph_steps, Batch** out, std::string& err) {
     BatchShape sh;
-    sh.tile = std::min(std::max(tile, 0), BATCH_BRANCHES_DIRECT);
+    sh.tile = std::min(std::max(tile, 0), BATCH_MERGED);
     sh.blocks_per_sm = std::max(blocks_per_sm, 0);
     sh.seg = seg > 0 ? seg : 32;
     return batch_new(gpu, sims, specs, tune, sh, graph_steps > 0 ? graph_steps : 10, out, err);

@@ -88,12 +88,11 @@ constexpr int SHELL_THREADS = 256;   // 8 rows per block
 // The new H of one row of shell nodes (cpu.rs:48-107): H_c = H_c - k_mu [(dE_v/du) inv_d_u + psi_u
 // - (dE_u/dv) inv_d_v - psi_v], each psi_a updated where the node's slot along a is live. All loads
 // of a node come before its stores.
-__global__ void __launch_bounds__(SHELL_THREADS, 4) k_shell_h(Geom g, ShellRows b, KAxis kx, const float* __restrict__ e_in,
-                                                           const float* __restrict__ h_in, float* __restrict__ h_out,
-                                                           const float* __restrict__ psi_in, float* __restrict__ psi_out,
-                                                           const float* __restrict__ pz_in, float* __restrict__ pz_out,
-                                                           float k_mu) {
-    const unsigned r = blockIdx.x * (SHELL_THREADS / 32) + (threadIdx.x >> 5);
+__device__ __forceinline__ void shell_h_row(const Geom& g, const ShellRows& b, const KAxis& kx, unsigned r,
+                                            const float* __restrict__ e_in, const float* __restrict__ h_in,
+                                            float* __restrict__ h_out, const float* __restrict__ psi_in,
+                                            float* __restrict__ psi_out, const float* __restrict__ pz_in,
+                                            float* __restrict__ pz_out, float k_mu) {
     if (r >= b.ra + b.rb + b.rc) return;
     int i, j;
     bool strips;
@@ -158,12 +157,11 @@ __global__ void __launch_bounds__(SHELL_THREADS, 4) k_shell_h(Geom g, ShellRows 
 // psi_u - (dH_u/dv) inv_dd_v - psi_v], kept where cb == 0; the E psi slabs are updated in place,
 // so every psi read of a node precedes its writes.
 template <typename CID>
-__global__ void __launch_bounds__(SHELL_THREADS) k_shell_e(Geom g, ShellRows b, KAxis kx, const CID* __restrict__ node_class,
-                                                           const DevCoef* __restrict__ classes,
-                                                           const float* __restrict__ h, const float* __restrict__ e_in,
-                                                           float* __restrict__ e_out, float* __restrict__ psi,
-                                                           const float* pz_in, float* pz_out) {
-    const unsigned r = blockIdx.x * (SHELL_THREADS / 32) + (threadIdx.x >> 5);
+__device__ __forceinline__ void shell_e_row(const Geom& g, const ShellRows& b, const KAxis& kx, unsigned r,
+                                            const CID* __restrict__ node_class, const DevCoef* __restrict__ classes,
+                                            const float* __restrict__ h, const float* __restrict__ e_in,
+                                            float* __restrict__ e_out, float* __restrict__ psi, const float* pz_in,
+                                            float* pz_out) {
     if (r >= b.ra + b.rb + b.rc) return;
     int i, j;
     bool strips;
@@ -221,6 +219,63 @@ __global__ void __launch_bounds__(SHELL_THREADS) k_shell_e(Geom g, ShellRows b, 
         e_out[cs + id] = ey;
         e_out[2 * cs + id] = ez;
     }
+}
+
+__global__ void __launch_bounds__(SHELL_THREADS, 4) k_shell_h(Geom g, ShellRows b, KAxis kx, const float* __restrict__ e_in,
+                                                           const float* __restrict__ h_in, float* __restrict__ h_out,
+                                                           const float* __restrict__ psi_in, float* __restrict__ psi_out,
+                                                           const float* __restrict__ pz_in, float* __restrict__ pz_out,
+                                                           float k_mu) {
+    shell_h_row(g, b, kx, blockIdx.x * (SHELL_THREADS / 32) + (threadIdx.x >> 5), e_in, h_in, h_out, psi_in, psi_out,
+                pz_in, pz_out, k_mu);
+}
+
+template <typename CID>
+__global__ void __launch_bounds__(SHELL_THREADS) k_shell_e(Geom g, ShellRows b, KAxis kx, const CID* __restrict__ node_class,
+                                                           const DevCoef* __restrict__ classes,
+                                                           const float* __restrict__ h, const float* __restrict__ e_in,
+                                                           float* __restrict__ e_out, float* __restrict__ psi,
+                                                           const float* pz_in, float* pz_out) {
+    shell_e_row<CID>(g, b, kx, blockIdx.x * (SHELL_THREADS / 32) + (threadIdx.x >> 5), node_class, classes, h, e_in,
+                     e_out, psi, pz_in, pz_out);
+}
+
+// One grid's shell in a merged batch launch: its geometry, rows and buffers per input set (the
+// pointers of the single-grid launches in the fused step of that parity), and its first block.
+struct ShellGrid {
+    Geom g;
+    ShellRows b;
+    KAxis kx;
+    const void* node_class;
+    const DevCoef* classes;
+    const float* e_in[2];
+    const float* h_in[2];
+    float* e_out[2];
+    float* h_out[2];
+    const float* psi_h_in[2];
+    float* psi_h_out[2];
+    float* psi;
+    float k_mu;
+    int block0;
+};
+
+// The shells of many grids in one launch (k_shell_h / k_shell_e per grid): block b walks rows of
+// grid block_grid[b].
+__global__ void __launch_bounds__(SHELL_THREADS, 4) k_batch_shell_h(const ShellGrid* __restrict__ grids,
+                                                                 const int* __restrict__ block_grid, int parity) {
+    const ShellGrid& G = grids[block_grid[blockIdx.x]];
+    const unsigned r = unsigned(int(blockIdx.x) - G.block0) * (SHELL_THREADS / 32) + (threadIdx.x >> 5);
+    shell_h_row(G.g, G.b, G.kx, r, G.e_in[parity], G.h_in[parity], G.h_out[parity], G.psi_h_in[parity],
+                G.psi_h_out[parity], G.psi_h_in[parity], G.psi_h_out[parity], G.k_mu);
+}
+
+template <typename CID>
+__global__ void __launch_bounds__(SHELL_THREADS) k_batch_shell_e(const ShellGrid* __restrict__ grids,
+                                                              const int* __restrict__ block_grid, int parity) {
+    const ShellGrid& G = grids[block_grid[blockIdx.x]];
+    const unsigned r = unsigned(int(blockIdx.x) - G.block0) * (SHELL_THREADS / 32) + (threadIdx.x >> 5);
+    shell_e_row<CID>(G.g, G.b, G.kx, r, static_cast<const CID*>(G.node_class), G.classes, G.h_out[parity],
+                     G.e_in[parity], G.e_out[parity], G.psi, G.psi, G.psi);
 }
 
 }  // namespace fg

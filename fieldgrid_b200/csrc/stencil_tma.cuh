@@ -634,6 +634,36 @@ __global__ void __launch_bounds__(TMA_CONSUMERS + 32, MINB)
         tma_march<TJ, TK, CID, STAGES, SEGMAX, LOCAL, false>(map_e, map_h, map_c, map_pze, map_pzh, a, base);
 }
 
+// One grid of a merged batch launch (k_batch_tma): its tensor maps (64-byte aligned in HBM; a
+// copy reads them there as it reads kernel parameters) and its march arguments for each input
+// set. block0 is minus the grid's first block in the launch, so a.block0 + blockIdx.x indexes the
+// grid's own block list; bump is 0 (the batch opens every grid's step before the march).
+struct alignas(128) TmaGrid {
+    CUtensorMap e[2], h[2], c, pze, pzh[2];
+    TmaArgs a[2];
+};
+
+// The TMA march over the clean boxes of many grids in one launch: block b marches a tile of grid
+// block_grid[b] with that grid's maps and arguments (copied to shared memory first). One launch
+// serves the grids with per-block class tables (LOCAL), another those with global class ids.
+template <int TJ, int TK, typename CID, int STAGES, int SEGMAX, bool LOCAL, int MINB>
+__global__ void __launch_bounds__(TMA_CONSUMERS + 32, MINB)
+    k_batch_tma(const TmaGrid* __restrict__ grids, const int* __restrict__ block_grid, int parity) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    __shared__ __align__(16) TmaArgs sa;
+    unsigned char* base = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
+    const TmaGrid& G = grids[block_grid[blockIdx.x]];
+    static_assert(sizeof(TmaArgs) % 4 == 0, "TmaArgs copies as words");
+    const int* src = reinterpret_cast<const int*>(&G.a[parity]);
+    int* dst = reinterpret_cast<int*>(&sa);
+    for (int q = threadIdx.x; q < int(sizeof(TmaArgs) / 4); q += blockDim.x) dst[q] = src[q];
+    __syncthreads();
+    if (sa.blocks[sa.block0 + int(blockIdx.x)].x & TMA_ZL_TILE)
+        tma_march<TJ, TK, CID, STAGES, SEGMAX, LOCAL, true>(G.e[parity], G.h[parity], G.c, G.pze, G.pzh[parity], sa, base);
+    else
+        tma_march<TJ, TK, CID, STAGES, SEGMAX, LOCAL, false>(G.e[parity], G.h[parity], G.c, G.pze, G.pzh[parity], sa, base);
+}
+
 // Host side ---------------------------------------------------------------------------------
 
 struct TmaPlan {

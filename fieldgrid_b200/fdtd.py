@@ -718,7 +718,7 @@ class Batch:
         o = A.fg_batch_options()
         pb, tm, st = C.c_int(), C.c_double(), C.c_uint64()
         lib().fg_batch_info(self._h, C.byref(o), C.byref(pb), C.byref(tm), C.byref(st))
-        tiles = ["32x8", "64x4", "32x4", "graph branches", "graph branches, direct march"]
+        tiles = ["32x8", "64x4", "32x4", "graph branches", "graph branches, direct march", "merged TMA launches"]
         return {"tile": tiles[o.tile], "blocks_per_sm": o.blocks_per_sm, "seg": o.seg,
                 "persistent_blocks": pb.value, "tuned_ms_per_step": tm.value, "steps": st.value}
 

@@ -326,18 +326,21 @@ int fg_flux_gradient_batch(fg_gpu* g, const fg_sim* const* sims, const uint64_t*
  * own driven port and pulse; every step runs one persistent launch that marches the tiles of all
  * grids from a shared work-list (the direct-load fused march), then one launch each for all
  * grids' Debye edges, sources and port probes, captured in a CUDA graph; or (tile 3) one graph
- * branch per grid, each running that grid's own fused step on its stream, concurrently. Each
+ * branch per grid, each running that grid's own fused step on its stream, concurrently; or (tile 5)
+ * one launch of the TMA march over every grid's clean box and one of each CPML shell kernel over
+ * every grid's shell, then the shared Debye, source and probe launches. Each
  * grid's results are those of stepping it alone (fused step). Grids with thin wires or resistive
  * sheets, or that ask for a plane DFT or NTFF, are refused. With tune = 1 the batch times each
  * candidate (work-list tile 32x8, 64x4 or 32x4 with its persistent blocks per SM and x-planes per
- * work item, and both kinds of graph branches) as a captured graph of a few steps, keeps the fastest and
+ * work item, both kinds of graph branches and the merged launches) as a captured graph of a few steps, keeps the fastest and
  * resets every grid to step 0; with tune = 0 it uses the shape given. */
 typedef struct fg_batch fg_batch;
 typedef struct fg_batch_options {
     int tune;
     int tile;                /* work-list march 0: 32x8, 1: 64x4, 2: 32x4 (k x j); 3: graph branches;
                                 4: graph branches, the grids of fewer than seg thousand nodes (all: seg 0)
-                                with the direct-load march (one launch per grid-step) */
+                                with the direct-load march (one launch per grid-step); 5: merged TMA march
+                                and shell launches over all grids */
     int blocks_per_sm;       /* 0: the occupancy limit */
     int seg;                 /* x-planes per work item; 0: 32 */
     int graph_steps;         /* steps per captured graph; 0: 10 */

@@ -45,10 +45,11 @@ def test_a_batch_steps_each_grid_as_alone(gpu, scenes):
 
 
 @pytest.mark.parametrize("tile,seg,name", [(3, 0, "graph branches"), (4, 0, "graph branches, direct march"),
-                                          (4, 50, "graph branches, direct march")])
+                                          (4, 50, "graph branches, direct march"), (5, 0, "merged TMA launches")])
 def test_graph_branches_step_each_grid_as_alone(gpu, scenes, tile, seg, name):
     """Branches of each grid's own step: the TMA march, the direct-load march for all grids, and
-    the direct-load march for the grids under 50 thousand nodes only (a mix)."""
+    the direct-load march for the grids under 50 thousand nodes only (a mix); and the merged
+    launches (one TMA march and one shell launch of each kind over all grids)."""
     sims = [fdtd.Sim.try_new(*sc.args()) for sc in scenes]
     b = fdtd.Batch(gpu, sims, [sc.pulse for sc in scenes], 64, tune=False, tile=tile, seg=seg, graph_steps=4)
     assert b.info()["tile"] == name
@@ -71,3 +72,30 @@ def test_a_batch_refuses_wires_and_sheets(gpu):
     sc = W.everything(steps=10, fused=True)
     with pytest.raises(fdtd.FdtdError, match="no thin wires"):
         fdtd.Batch(gpu, [fdtd.Sim.try_new(*sc.args())], [sc.pulse], 10)
+
+
+def test_merged_launches_on_larger_uneven_grids(gpu):
+    """The merged mode on grids with Debye spheres, k-layer tiles and shells of different sizes,
+    an odd step count: each grid bit for bit as stepped alone."""
+    scenes = W.batch_grids(count=6, lo=40, hi=96, pml=6, steps=40, seed=5)
+    sims = [fdtd.Sim.try_new(*sc.args()) for sc in scenes]
+    b = fdtd.Batch(gpu, sims, [sc.pulse for sc in scenes], 40, tune=False, tile=5, graph_steps=8)
+    assert b.info()["tile"] == "merged TMA launches"
+    b.step(3)
+    b.step(18)
+    check(gpu, b, scenes, 21)
+    b.close()
+
+
+def test_merged_launches_with_grids_that_march_on_their_own(gpu):
+    """A grid with no clean box for the TMA march (8 cells and a 4-cell CPML) first, then grids
+    that the merged march covers: the first marches on its own inside the merged step, and every
+    grid matches stepping it alone."""
+    scenes = W.batch_grids(count=1, lo=8, hi=8, pml=4, steps=24, seed=3) + \
+        W.batch_grids(count=4, lo=40, hi=72, pml=5, steps=24, seed=9)
+    sims = [fdtd.Sim.try_new(*sc.args()) for sc in scenes]
+    b = fdtd.Batch(gpu, sims, [sc.pulse for sc in scenes], 24, tune=False, tile=5, graph_steps=4)
+    b.step(11)
+    check(gpu, b, scenes, 11)
+    b.close()
+

@@ -65,6 +65,7 @@ int gpu_open(int device, Gpu** out, std::string& err) {
 void gpu_close(Gpu* g) {
     if (!g) return;
     cudaSetDevice(g->device);
+    if (g->spare) cudaFree(g->spare);
     for (int b = 0; b < 2; ++b) {
         if (g->stage_ev[b]) {
             cudaEventSynchronize(static_cast<cudaEvent_t>(g->stage_ev[b]));
@@ -1487,14 +1488,29 @@ int session_new(Gpu* gpu, const HostSim& sim, const RunSpec& rs, Session** out, 
     need += carve_size(64);
     need += carve_size(cp.blocks.size() * sizeof(int4));
     need += carve_size(cp.own.size() * sizeof(int2));
-    size_t free_b = 0, total_b = 0;
-    FG_CUDA(cudaMemGetInfo(&free_b, &total_b));
-    if (need + (size_t(256) << 20) > free_b) {
-        err = std::to_string(sim.cells()) + " cells is more than this GPU can hold";
-        return FG_ERR_TOO_LARGE;
+    // the device's spare arena serves when it holds the need with at most a quarter (+64 MB) more
+    Gpu* gp = s->gpu;
+    if (gp->spare && !(gp->spare_bytes >= need && gp->spare_bytes <= need + need / 4 + (size_t(64) << 20))) {
+        cudaFree(gp->spare);
+        gp->spare = nullptr;
+        gp->spare_bytes = 0;
+    }
+    if (!gp->spare) {
+        size_t free_b = 0, total_b = 0;
+        FG_CUDA(cudaMemGetInfo(&free_b, &total_b));
+        if (need + (size_t(256) << 20) > free_b) {
+            err = std::to_string(sim.cells()) + " cells is more than this GPU can hold";
+            return FG_ERR_TOO_LARGE;
+        }
     }
     FG_CUDA(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
-    FG_CUDA(cudaMalloc(&s->arena, need));
+    if (gp->spare) {
+        s->arena = static_cast<char*>(gp->spare);
+        gp->spare = nullptr;
+        gp->spare_bytes = 0;
+    } else {
+        FG_CUDA(cudaMalloc(&s->arena, need));
+    }
     clk.mark("malloc");
     s->arena_bytes = need;
     char* cur = s->arena;
@@ -1766,7 +1782,15 @@ void session_free(Session* s) {
         if (s->aux_ready[p]) cudaEventDestroy(s->aux_ready[p]);
         if (s->aux_done[p]) cudaEventDestroy(s->aux_done[p]);
     }
-    if (s->arena) cudaFree(s->arena);
+    if (s->arena) {   // kept as the device's spare (the stream is idle), or released
+        Gpu* gp = s->gpu;
+        if (gp && !gp->spare) {
+            gp->spare = s->arena;
+            gp->spare_bytes = s->arena_bytes;
+        } else {
+            cudaFree(s->arena);
+        }
+    }
     cudaFree(s->design);
     cudaFree(s->hist_e);
     cudaFree(s->hist_s);

@@ -44,6 +44,10 @@ struct Gpu {
     // through the two buffers in turn, so filling one overlaps the transfer of the other
     void* stage[2] = {nullptr, nullptr};
     void* stage_ev[2] = {nullptr, nullptr};   // cudaEvent_t: the last transfer out of each buffer
+    // the arena of the last session freed on this device, kept for the next session of a similar
+    // size (runs of one grid after another skip the allocation and its release)
+    void* spare = nullptr;
+    size_t spare_bytes = 0;
 };
 
 // Copies `bytes` from pageable host memory to the device through the Gpu's pinned staging buffers

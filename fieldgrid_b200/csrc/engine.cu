@@ -1477,7 +1477,9 @@ int session_new(Gpu* gpu, const HostSim& sim, const RunSpec& rs, Session** out, 
     need += carve_size(std::max<size_t>(nd, 1) * 8);
     need += carve_size(std::max<size_t>(nd, 1) * 4) * 3;
     need += carve_size(std::max<size_t>(nd * sim.poles.size(), 1) * 4);
-    need += carve_size(std::max<size_t>(nd, 1) * sizeof(DebyeEdge));   // the host records, set-up only
+    // the host records, set-up only: packed to 8 bytes while staged where the device nodes allow
+    const bool pack_debye = nnp < (size_t(1) << 30);
+    need += carve_size(std::max<size_t>(nd, 1) * (pack_debye ? sizeof(PackedDebye) : sizeof(DebyeEdge)));
     need += carve_size(debye_table.size() * 4);
     need += carve_size(std::max<size_t>(t_pulse.size(), 1) * 4);
     need += carve_size(std::max<size_t>(t_dft.size(), 1) * 4) * 2;
@@ -1546,7 +1548,7 @@ int session_new(Gpu* gpu, const HostSim& sim, const RunSpec& rs, Session** out, 
     s->debye_cb = carve<float>(cur, std::max<size_t>(nd, 1));
     s->debye_old = carve<float>(cur, std::max<size_t>(nd, 1));
     s->debye_state = carve<float>(cur, std::max<size_t>(nd * sim.poles.size(), 1));
-    DebyeEdge* debye_raw = carve<DebyeEdge>(cur, std::max<size_t>(nd, 1));
+    void* debye_raw = carve<char>(cur, std::max<size_t>(nd, 1) * (pack_debye ? sizeof(PackedDebye) : sizeof(DebyeEdge)));
     s->debye_table = carve<float>(cur, debye_table.size());
     float* d_pulse = carve<float>(cur, std::max<size_t>(t_pulse.size(), 1));
     float* d_dft = carve<float>(cur, std::max<size_t>(t_dft.size(), 1));
@@ -1650,7 +1652,24 @@ int session_new(Gpu* gpu, const HostSim& sim, const RunSpec& rs, Session** out, 
     rc |= up(s->wires, wires.data(), wires.size() * sizeof(DevWire));
     rc |= up(s->sheets, sheets.data(), sheets.size() * sizeof(DevSheet));
     rc |= up(s->branch, sim.sheet_table.data(), sim.sheet_table.size() * 4);
-    rc |= up(debye_raw, sim.debye_edges.data(), nd * sizeof(DebyeEdge));
+    if (pack_debye && nd) {
+        const DebyeEdge* de = sim.debye_edges.data();
+        const size_t p2 = size_t(g.p2);
+        auto pack = [&](char* buf, size_t off, size_t n) {   // whole records: 1 MB parts hold 2^17 of them
+            PackedDebye* o = reinterpret_cast<PackedDebye*>(buf);
+            const size_t q0 = off / sizeof(PackedDebye), q1 = (off + n) / sizeof(PackedDebye);
+            for (size_t q = q0; q < q1; ++q) {
+                const DebyeEdge& d = de[q];
+                const size_t dv = (d.id / n2) * p2 + d.id % n2;
+                o[q - q0] = PackedDebye{uint32_t(d.comp) << 30 | uint32_t(dv), float(d.dd)};
+            }
+        };
+        const size_t bytes = nd * sizeof(PackedDebye);
+        if (cudaError_t(staged_fill(s->gpu, debye_raw, bytes, st, pack)) != cudaSuccess) return FG_ERR_CUDA;
+        s->h2d_bytes += bytes;
+    } else {
+        rc |= up(debye_raw, sim.debye_edges.data(), nd * sizeof(DebyeEdge));
+    }
     rc |= up(s->debye_table, debye_table.data(), debye_table.size() * 4);
     rc |= up(d_pulse, t_pulse.data(), t_pulse.size() * 4);
     if (!cp.blocks.empty()) rc |= up(s->tma_blocks, cp.blocks.data(), cp.blocks.size() * sizeof(int4));
@@ -1667,8 +1686,14 @@ int session_new(Gpu* gpu, const HostSim& sim, const RunSpec& rs, Session** out, 
     if (nd)
         with_cid([&](auto nc) {
             const unsigned grid = unsigned(std::min<size_t>((nd + 255) / 256, size_t(148) * 16));
-            k_debye_lists<<<grid, 256, 0, st>>>(debye_raw, (long long)nd, nc, s->classes, (long long)n2, (long long)g.p2,
-                                                (long long)cs, s->debye_f, s->debye_dd, s->debye_cb);
+            if (pack_debye)
+                k_debye_lists_packed<<<grid, 256, 0, st>>>(static_cast<const PackedDebye*>(debye_raw), (long long)nd, nc,
+                                                           s->classes, (long long)cs, s->debye_f, s->debye_dd,
+                                                           s->debye_cb);
+            else
+                k_debye_lists<<<grid, 256, 0, st>>>(static_cast<const DebyeEdge*>(debye_raw), (long long)nd, nc,
+                                                    s->classes, (long long)n2, (long long)g.p2, (long long)cs,
+                                                    s->debye_f, s->debye_dd, s->debye_cb);
         });
     if (s->local && !cp.blocks.empty())
         with_cid([&](auto nc) {

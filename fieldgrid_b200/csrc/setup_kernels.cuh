@@ -121,4 +121,28 @@ __global__ void k_debye_lists(const DebyeEdge* __restrict__ edges, long long ne,
     }
 }
 
+// The Debye records as staged to the device: the E component in the top two bits and the device
+// node index below (grids of fewer than 2^30 device nodes), dd already rounded to f32 (the
+// conversion k_debye_lists makes). 8 bytes against the host record's 24.
+struct PackedDebye {
+    uint32_t key;
+    float dd;
+};
+
+template <typename CID>
+__global__ void k_debye_lists_packed(const PackedDebye* __restrict__ edges, long long ne,
+                                     const CID* __restrict__ node_class, const DevCoef* __restrict__ classes,
+                                     long long cs, long long* __restrict__ f, float* __restrict__ dd,
+                                     float* __restrict__ cb) {
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < ne;
+         q += (long long)gridDim.x * blockDim.x) {
+        const PackedDebye d = edges[q];
+        const unsigned comp = d.key >> 30;
+        const long long dev = (long long)(d.key & 0x3fffffffu);
+        f[q] = (long long)comp * cs + dev;
+        dd[q] = d.dd;
+        cb[q] = classes[unsigned(node_class[dev])].cb[comp];
+    }
+}
+
 }  // namespace fg

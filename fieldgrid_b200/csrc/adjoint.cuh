@@ -553,8 +553,10 @@ int flux_gradient(Gpu* gpu, const HostSim& sim, uint64_t driven, double f0, doub
 // backwards are enqueued together, and while they run the next group is prepared and its
 // forwards enqueued, before the group is finished in turn. A group also stops growing when the
 // device's free memory would not hold the next job (estimated from the bytes per node the jobs
-// prepared so far took, with half again to spare): its jobs then wait for a later group, and a
-// group that cannot open beside the running one opens after it. Each job's results are those of
+// prepared so far took, with half again to spare) or when preparing a job runs out of device
+// memory beside jobs in flight (a job's checkpoints and design history grow with its steps and
+// design, not with its nodes): its jobs then wait for a later group, and a group that cannot open
+// beside the running one opens after it. Each job's results are those of
 // running it alone. The first error stops the batch (its message names the job).
 int flux_gradient_batch(Gpu* gpu, const std::vector<const HostSim*>& sims, const std::vector<uint64_t>& driven,
                         const std::vector<std::pair<double, double>>& pulses, const std::vector<FluxSpec>& specs,
@@ -592,7 +594,19 @@ int flux_gradient_batch(Gpu* gpu, const std::vector<const HostSim*>& sims, const
             j->fc = pulses[q].second;
             j->sp = specs[q];
             j->want_grad = true;
-            if ((rc = j->prepare())) fail(q, *j);
+            if ((rc = j->prepare())) {
+                // out of device memory beside jobs already in flight: this job waits for a later
+                // group (its partial buffers go with it); alone, the error stands
+                const bool oom = rc == FG_ERR_TOO_LARGE ||
+                                 (rc == FG_ERR_CUDA && j->err.find("out of memory") != std::string::npos);
+                if (oom && (!G.empty() || holding)) {
+                    j.reset();
+                    cudaGetLastError();
+                    rc = FG_OK;
+                    break;
+                }
+                fail(q, *j);
+            }
             const double after = free_bytes();
             if (before > after) per_node = std::max(per_node, (before - after) / double(sims[q]->nn));
             G.push_back(std::move(j));

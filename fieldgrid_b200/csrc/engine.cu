@@ -27,6 +27,7 @@
 #include "adjoint_kernels.cuh"
 
 #include <cudaTypedefs.h>
+#include <cub/cub.cuh>
 
 namespace fg {
 
@@ -180,6 +181,15 @@ struct Session {
     std::vector<DevInductor> ind_host;
     float* tables = nullptr;        // per block region: LOCAL_CLASSES x (ca[3], cb[3])
     bool local = false;
+    // the Debye ADE folded into the TMA march (setup_kernels.cuh): per-block entry masks, row
+    // offsets, dd and pole state of the folded edges; the list keeps the others
+    bool fold = false;
+    uint8_t* lmask = nullptr;
+    int* drow = nullptr;
+    float* fdd = nullptr;
+    float* fstate = nullptr;
+    int nfold = 0;
+    float fdb[2] = {0.f, 0.f}, fdc[2] = {0.f, 0.f};
     // counts
     int n_sources = 0, n_inductors = 0, n_ports = 0, n_wires = 0, n_sheets = 0, n_debye = 0, n_patches = 0;
     int plane_k = 0;
@@ -315,18 +325,20 @@ template <typename CID, bool LOCAL, int ST>
 using TmaLS = TmaLayout<TMA_TJ, TMA_TK, CID, ST, TMA_SEGMAX, LOCAL, true>;
 template <typename CID, bool LOCAL = false>
 using TmaL = TmaLS<CID, LOCAL, TMA_STAGES>;
-template <typename CID, bool LOCAL, int SHAPE>
+template <typename CID, bool LOCAL, int SHAPE, bool FOLD = false>
 constexpr auto tma_kernel_s =
-    k_tma_step<TMA_TJ, TMA_TK, CID, TMA_SHAPES[SHAPE].stages, TMA_SEGMAX, LOCAL, TMA_SHAPES[SHAPE].minb>;
+    k_tma_step<TMA_TJ, TMA_TK, CID, TMA_SHAPES[SHAPE].stages, TMA_SEGMAX, LOCAL, TMA_SHAPES[SHAPE].minb, FOLD>;
 
 template <typename CID, bool LOCAL, int SHAPE>
 int tma_smem_s() { return TmaLS<CID, LOCAL, TMA_SHAPES[SHAPE].stages>::TOTAL; }
 
-// Calls f(kernel, smem bytes) with the instantiation for (class-id width, local tables, shape).
+// Calls f(kernel, smem bytes) with the instantiation for (class-id width, local tables, shape,
+// the folded Debye ADE).
 template <typename F>
-bool with_tma_kernel(int cid_bytes, bool local, int shape, F&& f) {
+bool with_tma_kernel(int cid_bytes, bool local, bool fold, int shape, F&& f) {
     auto go = [&](auto sh) {
         constexpr int S = decltype(sh)::value;
+        if (local && fold) return f(tma_kernel_s<uint8_t, true, S, true>, tma_smem_s<uint8_t, true, S>());
         if (local) return f(tma_kernel_s<uint8_t, true, S>, tma_smem_s<uint8_t, true, S>());
         if (cid_bytes == 1) return f(tma_kernel_s<uint8_t, false, S>, tma_smem_s<uint8_t, false, S>());
         if (cid_bytes == 2) return f(tma_kernel_s<uint16_t, false, S>, tma_smem_s<uint16_t, false, S>());
@@ -441,9 +453,6 @@ CleanPlan plan_clean(const HostSim& sim, const Geom& g, bool z_layer, int seg_fi
     return out;
 }
 
-// Per block of the TMA step (a TJ x TK tile over one x-segment): the distinct node classes
-// it holds, renumbered from 0, and each node's index into that short list. ok = false when a
-// region holds more than LOCAL_CLASSES classes.
 // Builds the tensor maps of the TMA step: E and H of both buffer sets, and the class ids.
 void plan_tma(Session& s) {
     TmaPlan& t = s.tma;
@@ -493,7 +502,7 @@ void plan_tma(Session& s) {
     }
     cudaError_t ce = cudaSuccess;
     for (int sh = 0; sh < TMA_NSHAPES && ce == cudaSuccess; ++sh)
-        with_tma_kernel(b, s.local, sh, [&](auto kern, int smem) {
+        with_tma_kernel(b, s.local, s.fold, sh, [&](auto kern, int smem) {
             ce = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
             if (sh == t.shape) t.smem = smem;
             return true;
@@ -510,10 +519,19 @@ int launch_tma(Session& s, int parity, float* e_out, float* h_out, float* psi_h_
     const TmaPlan& t = s.tma;
     TmaArgs a{s.geom, s.classes, e_out, h_out, s.sc.k_mu, s.clean_lo[2], s.clean_hi[1], s.clean_hi[2], s.tma_blocks,
               s.tma_own, 0, 1, s.psi, psi_h_out, s.tables, s.counter, s.error, s.wait_ns, -0.0f, s.stall_plane};
+    if (s.fold) {
+        a.lmask = s.lmask;
+        a.drow = s.drow;
+        a.fdd = s.fdd;
+        a.fstate = s.fstate;
+        a.nfold = s.nfold;
+        a.npoles = s.n_poles;
+        for (int k = 0; k < 2; ++k) { a.db[k] = s.fdb[k]; a.dc[k] = s.fdc[k]; }
+    }
     // without k-layer tiles the last two maps are never read
     const CUtensorMap& pze = t.pz ? t.pze : t.c;
     const CUtensorMap& pzh = t.pz ? t.pzh[parity] : t.c;
-    with_tma_kernel(s.cid_bytes, s.local, t.shape, [&](auto kern, int smem) {
+    with_tma_kernel(s.cid_bytes, s.local, s.fold, t.shape, [&](auto kern, int smem) {
         kern<<<unsigned(t.blocks), TMA_CONSUMERS + 32, smem, s.stream>>>(t.e[parity], t.h[parity], t.c, pze, pzh, a);
         return true;
     });
@@ -971,7 +989,7 @@ void launch_tma_slots(Session& s, bool all, int a, int b, cudaStream_t st) {
                  all ? s.tma_blocks : s.c_blocks, all ? s.tma_own : s.c_own, 0, 1, s.zslot[b], s.zslot[b],
                  all ? s.tables : s.c_tables, s.counter, s.error, s.wait_ns, -0.0f, s.stall_plane};
     const unsigned nb = unsigned(all ? s.tma.blocks : s.n_cblocks);
-    with_tma_kernel(s.cid_bytes, s.local, s.tma.shape, [&](auto kern, int smem) {
+    with_tma_kernel(s.cid_bytes, s.local, false, s.tma.shape, [&](auto kern, int smem) {
         kern<<<nb, TMA_CONSUMERS + 32, smem, st>>>(s.d1_e[a], s.d1_h[a], s.tma.c, s.d1_pze[a], s.d1_pzh[a], args);
         return true;
     });
@@ -1695,17 +1713,114 @@ int session_new(Gpu* gpu, const HostSim& sim, const RunSpec& rs, Session** out, 
                                                     s->classes, (long long)n2, (long long)g.p2, (long long)cs,
                                                     s->debye_f, s->debye_dd, s->debye_cb);
         });
+    // the Debye ADE folded into the march (opt-in, FIELDGRID_DEBYE_FOLD=1: at 513^3 the march's
+    // added per-plane work cost more than the separate list kernel): graph-stepped one-step TMA runs
+    // with per-block tables, one pole, no sheets and no design history
+    const char* fv = std::getenv("FIELDGRID_DEBYE_FOLD");
+    bool fold = nd > 0 && s->local && !cp.blocks.empty() && !sp.ok && rs.graphs && s->fused && sim.poles.size() == 1 &&
+                s->n_sheets == 0 && !(rs.design && !rs.design->empty()) && ncls + 1 < (size_t(1) << 29) &&
+                fv && fv[0] == '1';
+    std::vector<void*> scratch;   // set-up only
+    struct Scratch {
+        std::vector<void*>& v;
+        ~Scratch() { for (void* p : v) cudaFree(p); }
+    } scratch_guard{scratch};
+    auto grab = [&](void** p, size_t bytes, bool keep) -> bool {
+        if (cudaMalloc(p, std::max<size_t>(bytes, 4)) != cudaSuccess) { cudaGetLastError(); return false; }
+        (keep ? s->extra_allocs : scratch).push_back(*p);
+        return true;
+    };
+    uint8_t* dmask = nullptr;
+    float* ddn = nullptr;
+    if (fold) fold = grab((void**)&dmask, (nnp + 3) & ~size_t(3), false) && grab((void**)&ddn, size_t(3 * cs) * 4, false) &&
+                     grab((void**)&s->lmask, cp.blocks.size() * LOCAL_CLASSES, true);
+    if (fold) {
+        FG_CUDA(cudaMemsetAsync(dmask, 0, (nnp + 3) & ~size_t(3), st));
+        const unsigned grid = unsigned(std::min<size_t>((nd + 255) / 256, size_t(148) * 16));
+        k_debye_node_mask<<<grid, 256, 0, st>>>(s->debye_f, s->debye_dd, (long long)nd, (long long)cs,
+                                                reinterpret_cast<unsigned*>(dmask), ddn);
+    }
     if (s->local && !cp.blocks.empty())
         with_cid([&](auto nc) {
             k_local_classes<<<unsigned(cp.blocks.size()), 256, 0, st>>>(nc, s->classes, s->tma_blocks, s->tma_own, g.n1,
                                                                        g.n2, g.p2, TMA_TK, cp.lo[2], cp.hi[2],
-                                                                       s->local_ids, s->tables, setup_flag);
+                                                                       s->local_ids, s->tables, setup_flag,
+                                                                       fold ? dmask : nullptr,
+                                                                       fold ? s->lmask : nullptr);
         });
     FG_CUDA(cudaGetLastError());
     int over = 0;
     FG_CUDA(cudaMemcpyAsync(&over, setup_flag, sizeof(int), cudaMemcpyDeviceToHost, st));
     FG_CUDA(cudaStreamSynchronize(st));
-    if (over) s->local = false;   // a region holds more classes than a local table: global ids
+    if (over) {   // a region holds more classes than a local table: global ids, the list's Debye ADE
+        s->local = false;
+        fold = false;
+    }
+    if (fold) {
+        // each (block, owned plane, row)'s folded edges, their offsets, their dd in march order
+        const size_t nrow = cp.blocks.size() * size_t(TMA_SEGMAX) * 8;
+        int *counts = nullptr, *keep = nullptr, *pos = nullptr;
+        void* tmp = nullptr;
+        size_t tmp_bytes = 0, tmp2 = 0;
+        cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, counts, s->drow, int(nrow), st);
+        cub::DeviceScan::ExclusiveSum(nullptr, tmp2, keep, pos, int(nd), st);
+        fold = grab((void**)&counts, nrow * 4, false) && grab((void**)&s->drow, nrow * 4, true) &&
+               grab((void**)&keep, nd * 4, false) && grab((void**)&pos, nd * 4, false) &&
+               grab(&tmp, std::max(tmp_bytes, tmp2), false);
+        if (fold) {
+            FG_CUDA(cudaMemsetAsync(counts, 0, nrow * 4, st));
+            const unsigned nb = unsigned(cp.blocks.size());
+            k_fold_rows<false><<<nb, 256, 0, st>>>(s->tma_blocks, s->tma_own, g.n1, g.n2, g.p2, TMA_TJ, TMA_TK, cp.lo[2],
+                                                  cp.hi[2], TMA_SEGMAX, dmask, (long long)cs, counts, ddn, nullptr);
+            tmp_bytes = std::max(tmp_bytes, tmp2);
+            FG_CUDA(cub::DeviceScan::ExclusiveSum(tmp, tmp_bytes, counts, s->drow, int(nrow), st));
+            int tail[2] = {0, 0};
+            FG_CUDA(cudaMemcpyAsync(&tail[0], s->drow + nrow - 1, 4, cudaMemcpyDeviceToHost, st));
+            FG_CUDA(cudaMemcpyAsync(&tail[1], counts + nrow - 1, 4, cudaMemcpyDeviceToHost, st));
+            FG_CUDA(cudaStreamSynchronize(st));
+            s->nfold = tail[0] + tail[1];
+            const size_t np = sim.poles.size();
+            fold = grab((void**)&s->fdd, size_t(s->nfold) * 4, true) &&
+                   grab((void**)&s->fstate, size_t(s->nfold) * np * 4, true);
+        }
+        if (fold) {
+            FG_CUDA(cudaMemsetAsync(s->fstate, 0, std::max<size_t>(size_t(s->nfold) * sim.poles.size() * 4, 4), st));
+            const unsigned nb = unsigned(cp.blocks.size());
+            k_fold_rows<true><<<nb, 256, 0, st>>>(s->tma_blocks, s->tma_own, g.n1, g.n2, g.p2, TMA_TJ, TMA_TK, cp.lo[2],
+                                                 cp.hi[2], TMA_SEGMAX, dmask, (long long)cs, s->drow, ddn, s->fdd);
+            // the edges left to the list, compacted in list order
+            const unsigned grid = unsigned(std::min<size_t>((nd + 255) / 256, size_t(148) * 16));
+            k_debye_unfolded<<<grid, 256, 0, st>>>(s->debye_f, (long long)nd, ddn, keep);
+            tmp_bytes = std::max(tmp_bytes, tmp2);
+            FG_CUDA(cub::DeviceScan::ExclusiveSum(tmp, tmp_bytes, keep, pos, int(nd), st));
+            int tail[2] = {0, 0};
+            FG_CUDA(cudaMemcpyAsync(&tail[0], pos + nd - 1, 4, cudaMemcpyDeviceToHost, st));
+            FG_CUDA(cudaMemcpyAsync(&tail[1], keep + nd - 1, 4, cudaMemcpyDeviceToHost, st));
+            FG_CUDA(cudaStreamSynchronize(st));
+            const size_t nres = size_t(tail[0]) + size_t(tail[1]);
+            if (size_t(s->nfold) + nres != nd) { err = "internal: folded and listed Debye edges do not add up"; return FG_ERR_INVALID; }
+            long long* f2 = nullptr;
+            float *dd2 = nullptr, *cb2 = nullptr;
+            if (!grab((void**)&f2, nres * 8, true) || !grab((void**)&dd2, nres * 4, true) || !grab((void**)&cb2, nres * 4, true)) {
+                err = "out of device memory for the Debye list";
+                return FG_ERR_CUDA;
+            }
+            k_debye_compact<<<grid, 256, 0, st>>>(s->debye_f, s->debye_dd, s->debye_cb, keep, pos, (long long)nd, f2, dd2,
+                                                  cb2);
+            FG_CUDA(cudaGetLastError());
+            FG_CUDA(cudaStreamSynchronize(st));
+            s->debye_f = f2;
+            s->debye_dd = dd2;
+            s->debye_cb = cb2;
+            s->n_debye = int(nres);
+            for (size_t k = 0; k < std::min<size_t>(sim.poles.size(), 2); ++k) {
+                s->fdb[k] = debye_table[1 + 2 * k];
+                s->fdc[k] = debye_table[2 + 2 * k];
+            }
+        }
+    }
+    s->fold = fold;
+    FG_CUDA(cudaStreamSynchronize(st));   // the scratch goes with scratch_guard
 
     clk.mark("upload");
     if (rs.design && !rs.design->empty()) {
@@ -1745,7 +1860,10 @@ int session_new(Gpu* gpu, const HostSim& sim, const RunSpec& rs, Session** out, 
                      std::to_string(s->shell.ra + s->shell.rb + s->shell.rc) + " rows, " +
                      std::to_string(TMA_SHAPES[s->tma.shape].stages) + " stages, " +
                      std::to_string(TMA_SHAPES[s->tma.shape].minb) + " blocks/SM, " +
-                     (s->local ? "per-block class tables" : "global class table");
+                     (s->local ? "per-block class tables" : "global class table") +
+                     (s->fold ? ", Debye ADE folded into the march for " + std::to_string(s->nfold) + " edges (" +
+                                    std::to_string(s->n_debye) + " on the list)"
+                              : std::string());
     else
         s->variant = s->fused ? fused_name(s->shape) + " (" + s->tma.why + ")" : std::string("separate H+E, 64x4 threads");
     s->launches = count_launches(*s);
@@ -1848,6 +1966,8 @@ int session_reset(Session* s, std::string& err) {
         FG_CUDA(cudaMemsetAsync(s->debye_old, 0, size_t(s->n_debye) * 4, st));
         FG_CUDA(cudaMemsetAsync(s->debye_state, 0, size_t(s->n_debye) * size_t(std::max(s->n_poles, 1)) * 4, st));
     }
+    if (s->fold && s->nfold)
+        FG_CUDA(cudaMemsetAsync(s->fstate, 0, size_t(s->nfold) * size_t(std::max(s->n_poles, 1)) * 4, st));
     if (s->currents_len) FG_CUDA(cudaMemsetAsync(s->currents, 0, s->currents_len * 4, st));
     if (!s->ind_host.empty())
         FG_CUDA(cudaMemcpyAsync(s->inductors, s->ind_host.data(), s->ind_host.size() * sizeof(DevInductor),

@@ -16,15 +16,18 @@ constexpr unsigned LC_EMPTY = 0xffffffffu;
 
 // One CTA per march block region (its owned rows and columns over its planes): the distinct
 // global classes of the region, ranked in increasing id order, become the region's table of at
-// most LOCAL_CLASSES (ca[3], cb[3]) entries and each owned node's 8-bit local id. A region with
-// more classes sets *over and writes nothing; the host then keeps the global ids.
+// most LOCAL_CLASSES (ca[3], cb[3]) entries and each owned node's 8-bit local id. With node masks
+// (dmask: bit c set where the node's E_c carries a Debye edge) the entries are the distinct
+// (class, mask) pairs and lmask gets each entry's mask. A region with more entries sets *over and
+// writes nothing; the host then keeps the global ids. Classes are below 2^29 - 1 with masks.
 template <typename CID>
 __global__ void __launch_bounds__(256) k_local_classes(const CID* __restrict__ node_class,
                                                        const DevCoef* __restrict__ classes,
                                                        const int4* __restrict__ blocks, const int2* __restrict__ own,
                                                        int n1, int n2, int p2, int tk, int lo2, int hi2,
                                                        uint8_t* __restrict__ ids, float* __restrict__ tables,
-                                                       int* over) {
+                                                       int* over, const uint8_t* __restrict__ dmask = nullptr,
+                                                       uint8_t* __restrict__ lmask = nullptr) {
     __shared__ unsigned keys[LC_SLOTS];
     __shared__ unsigned short rank[LC_SLOTS];
     __shared__ int count;
@@ -49,7 +52,7 @@ __global__ void __launch_bounds__(256) k_local_classes(const CID* __restrict__ n
     for (int row = w; row < rows && !full; row += nw) {
         const size_t base = (size_t(i0 + row / nj) * n1 + size_t(jbeg + row % nj)) * p2;
         for (int k = kbeg + lane; k < kend && !full; k += 32) {
-            const unsigned gid = unsigned(node_class[base + k]);
+            const unsigned gid = unsigned(node_class[base + k]) | (dmask ? unsigned(dmask[base + k]) << 29 : 0u);
             if (gid == last) continue;
             last = gid;
             unsigned h = (gid * 2654435761u) & (LC_SLOTS - 1);
@@ -78,7 +81,8 @@ __global__ void __launch_bounds__(256) k_local_classes(const CID* __restrict__ n
         int rk = 0;
         for (int t = 0; t < LC_SLOTS; ++t) rk += (keys[t] != LC_EMPTY && keys[t] < key) ? 1 : 0;
         rank[q] = (unsigned short)rk;
-        const DevCoef c = classes[key];
+        const DevCoef c = classes[dmask ? (key & 0x1fffffffu) : key];
+        if (lmask) lmask[size_t(r) * LOCAL_CLASSES + rk] = uint8_t(key >> 29);
 #pragma unroll
         for (int m = 0; m < 3; ++m) {
             tab[rk * 6 + m] = c.ca[m];
@@ -93,7 +97,7 @@ __global__ void __launch_bounds__(256) k_local_classes(const CID* __restrict__ n
     for (int row = w; row < rows; row += nw) {
         const size_t base = (size_t(i0 + row / nj) * n1 + size_t(jbeg + row % nj)) * p2;
         for (int k = kbeg + lane; k < kend; k += 32) {
-            const unsigned gid = unsigned(node_class[base + k]);
+            const unsigned gid = unsigned(node_class[base + k]) | (dmask ? unsigned(dmask[base + k]) << 29 : 0u);
             if (gid != last) {
                 unsigned h = (gid * 2654435761u) & (LC_SLOTS - 1);
                 for (int probe = 0; probe < LC_SLOTS && keys[h] != gid; ++probe) h = (h + 1) & (LC_SLOTS - 1);
@@ -143,6 +147,106 @@ __global__ void k_debye_lists_packed(const PackedDebye* __restrict__ edges, long
         dd[q] = d.dd;
         cb[q] = classes[unsigned(node_class[dev])].cb[comp];
     }
+}
+
+// ---- the Debye ADE folded into the TMA march's E half ----
+//
+// Folded edges are the Debye edges at the nodes a march block writes through its column pairs
+// (owned rows and planes, columns kbeg .. kend - 1 of the tile): the march applies their ADE right
+// after their E update. They are numbered per block, owned plane and row, and within a row by
+// column then component: the order the march's lanes meet them (a lane's two columns, each's
+// components in turn). The other Debye edges (the shell's, a tile's right-edge column) keep the
+// edge-list kernel.
+
+constexpr unsigned FOLD_TAKEN = 0x7fc0f01du;   // a NaN payload no dd has: marks a folded edge
+
+// Each Debye edge's component bit in its node's byte (4 nodes per word) and its dd in the
+// per-(component, node) scratch ddn (the layout of a field buffer).
+__global__ void k_debye_node_mask(const long long* __restrict__ f, const float* __restrict__ dd, long long ne,
+                                  long long cs, unsigned* __restrict__ mask_words, float* __restrict__ ddn) {
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < ne;
+         q += (long long)gridDim.x * blockDim.x) {
+        const long long fi = f[q];
+        const long long c = fi / cs, dev = fi - c * cs;
+        atomicOr(&mask_words[dev >> 2], (1u << unsigned(c)) << unsigned((dev & 3) * 8));
+        ddn[fi] = dd[q];
+    }
+}
+
+// One CTA per block, a warp per (owned plane, row) at a time, a lane per column pair as in the
+// march: COUNT writes each row's folded-edge count to rows[(block * segmax + plane) * 8 + row];
+// FILL takes rows as the exclusive prefix sums and writes each folded edge's dd in march order,
+// marking it taken in ddn.
+template <bool FILL>
+__global__ void __launch_bounds__(256) k_fold_rows(const int4* __restrict__ blocks, const int2* __restrict__ own,
+                                                   int n1, int n2, int p2, int tj, int tk, int kbeg, int kend,
+                                                   int segmax, const uint8_t* __restrict__ dmask, long long cs,
+                                                   int* __restrict__ rows, float* __restrict__ ddn,
+                                                   float* __restrict__ fdd) {
+    const int bid = blockIdx.x;
+    const int4 b = blocks[bid];
+    const int k0 = b.x & ~TMA_ZL_TILE, j0 = b.y, i0 = b.z, i1 = b.w;
+    const int2 orow = own[bid];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    const int kk = k0 + 2 * lane;
+    for (int u = 0; u < i1 - i0; ++u)
+        for (int r = w; r < tj; r += nw) {
+            const int jj = j0 + r;
+            const bool owned = jj >= orow.x && jj < orow.y && kk >= kbeg && kk < kend && kk < n2 && 2 * lane < tk;
+            const bool live1 = kk + 1 < n2;
+            const long long dev = ((long long)(i0 + u) * n1 + jj) * p2 + kk;
+            unsigned m0 = 0, m1 = 0;
+            if (owned) {
+                m0 = dmask[dev];
+                m1 = live1 ? dmask[dev + 1] : 0u;
+            }
+            const int cnt = __popc(m0) + __popc(m1);
+            int x = cnt;
+            for (int d = 1; d < 32; d <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, x, d);
+                if (lane >= d) x += y;
+            }
+            const long long idx = ((long long)bid * segmax + u) * 8 + r;
+            if (!FILL) {
+                const int total = __shfl_sync(0xffffffffu, x, 31);
+                if (lane == 0) rows[idx] = total;
+            } else if (cnt) {
+                long long q = (long long)rows[idx] + (x - cnt);
+                for (int col = 0; col < 2; ++col) {
+                    const unsigned m = col ? m1 : m0;
+                    for (int c = 0; c < 3; ++c)
+                        if (m >> c & 1u) {
+                            float* slot = ddn + (long long)c * cs + dev + col;
+                            fdd[q++] = *slot;
+                            *slot = __uint_as_float(FOLD_TAKEN);
+                        }
+                }
+            }
+        }
+}
+
+// 1 for the Debye edges the march does not fold (their list stays), 0 for the folded ones.
+__global__ void k_debye_unfolded(const long long* __restrict__ f, long long ne, const float* __restrict__ ddn,
+                                 int* __restrict__ keep) {
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < ne;
+         q += (long long)gridDim.x * blockDim.x)
+        keep[q] = __float_as_uint(ddn[f[q]]) == FOLD_TAKEN ? 0 : 1;
+}
+
+// The unfolded edges' list entries at their positions in the compacted list (pos: exclusive
+// prefix sums of keep).
+__global__ void k_debye_compact(const long long* __restrict__ f, const float* __restrict__ dd,
+                                const float* __restrict__ cb, const int* __restrict__ keep,
+                                const int* __restrict__ pos, long long ne, long long* __restrict__ f2,
+                                float* __restrict__ dd2, float* __restrict__ cb2) {
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < ne;
+         q += (long long)gridDim.x * blockDim.x)
+        if (keep[q]) {
+            const int p = pos[q];
+            f2[p] = f[q];
+            dd2[p] = dd[q];
+            cb2[p] = cb[q];
+        }
 }
 
 }  // namespace fg

@@ -130,7 +130,8 @@ struct TmaLayout {
     static constexpr int NAX = (TJ + 2) + (TK + 4) + (SEGMAX + 2);
     static constexpr int AX = al(NAX * int(sizeof(AxisNode)));
     static constexpr int BARS = al(2 * STAGES * 8);
-    static constexpr int LT = LOCAL ? al(LOCAL_CLASSES * 6 * 4) : 0;  // the block's coefficient table
+    // the block's coefficient table, then (a folded Debye ADE) its entries' Debye masks
+    static constexpr int LT = LOCAL ? al(LOCAL_CLASSES * 6 * 4 + LOCAL_CLASSES) : 0;
     static constexpr int TOTAL = STAGES * STAGE + 2 * HN + AX + BARS + LT + 128;
 };
 
@@ -155,6 +156,14 @@ struct TmaArgs {
     int stall_plane;                     // test knob, -1 in normal runs: the full barrier of this
                                          // plane expects 16 bytes more than its copies deliver, so
                                          // the waits on it run out (the failure path under test)
+    // the Debye ADE folded into the E half (FOLD): the edges at the nodes the block's column
+    // pairs write, in march order (setup_kernels.cuh)
+    const uint8_t* lmask;                // per block: LOCAL_CLASSES masks, bit c: E_c is a Debye edge
+    const int* drow;                     // per (block, owned plane, row): the row's first folded edge
+    const float* fdd;                    // dd per folded edge
+    float* fstate;                       // pole state per folded edge, pole-major (nfold per pole)
+    int nfold, npoles;
+    float db[2], dc[2];                  // the pole table: b_k and c_k (k_debye_post_cb's table)
 };
 
 // The E values around one point that its H update needs (own, +j, +k, +i neighbours).
@@ -385,7 +394,19 @@ constexpr int TMA_ZL_TILE = 1 << 30;
 // One block's march; ZL: the tile reaches the k layer. The shared-memory layout is the ZL one for
 // both (the z boxes sit past the field boxes of each stage), so one launch runs both kinds of tile
 // in the block list's order: neighbouring tiles march together and share their halo columns in L2.
-template <int TJ, int TK, typename CID, int STAGES, int SEGMAX, bool LOCAL, bool ZL>
+// One folded Debye edge of a one-pole model (k_debye_post_cb's arithmetic, in its order): e is the
+// edge's new E, old its E before the step, w its dd and st its pole state (both loaded before the
+// H half); the new state goes to q.
+__device__ __forceinline__ void fold_edge(const TmaArgs& a, float& e, float old, float cb, float w, float st, int q) {
+    float s0 = 0.0f;
+    s0 += 0.5f * (1.0f + a.db[0]) * st;
+    const float next = e - cb * s0;
+    e = next;
+    const float de = next - old;
+    a.fstate[q] = a.db[0] * st + w * a.dc[0] * de;
+}
+
+template <int TJ, int TK, typename CID, int STAGES, int SEGMAX, bool LOCAL, bool ZL, bool FOLD = false>
 __device__ __forceinline__ void tma_march(const CUtensorMap& map_e, const CUtensorMap& map_h, const CUtensorMap& map_c,
                                           const CUtensorMap& map_pze, const CUtensorMap& map_pzh, const TmaArgs& a,
                                           unsigned char* base) {
@@ -429,6 +450,11 @@ __device__ __forceinline__ void tma_march(const CUtensorMap& map_e, const CUtens
     if constexpr (LOCAL) {
         const float* src = a.tables + (long long)bid * (LOCAL_CLASSES * 6);
         for (int q = tid; q < LOCAL_CLASSES * 6; q += blockDim.x) lt[q] = src[q];
+    }
+    uint8_t* lm = reinterpret_cast<uint8_t*>(lt + LOCAL_CLASSES * 6);   // FOLD: the entries' Debye masks
+    if constexpr (FOLD) {
+        static_assert(LOCAL, "the folded Debye ADE reads its masks from the per-block tables");
+        for (int q = tid; q < LOCAL_CLASSES; q += blockDim.x) lm[q] = a.lmask[(long long)bid * LOCAL_CLASSES + q];
     }
     __syncthreads();
 
@@ -494,6 +520,11 @@ __device__ __forceinline__ void tma_march(const CUtensorMap& map_e, const CUtens
     const float2 mz = make_float2(a.neg0, a.neg0);
     float pyx = 0.f, pzx = 0.f;                                         // warp 0's extra point's
     bool bad = false;
+    // FOLD: the row's first folded edge in the next owned plane, loaded a plane ahead
+    int fnext = 0;
+    if constexpr (FOLD) {
+        if (r >= 0) fnext = a.drow[(long long)bid * SEGMAX * 8 + r];
+    }
     for (int p = p_first; p < i1; ++p) {
         const int u = p - p_first;
         const int s = u % STAGES, s1 = (u + 1) % STAGES;
@@ -514,6 +545,54 @@ __device__ __forceinline__ void tma_march(const CUtensorMap& map_e, const CUtens
         const bool in = i + 1 < g.n0;
         const long long plane = (long long)i * g.n1 * g.p2;
         const bool own = own_row && !pre;
+
+        // the pair's two class ids in one aligned load (c is even)
+        unsigned id0 = 0, id1 = 0;
+        if (!pre && own_row && live0) {
+            if constexpr (sizeof(CID) == 1) {
+                const unsigned v = *reinterpret_cast<const uint16_t*>(CL + r * L::CW + c);
+                id0 = v & 0xffu;
+                id1 = v >> 8;
+            } else if constexpr (sizeof(CID) == 2) {
+                const unsigned v = *reinterpret_cast<const uint32_t*>(CL + r * L::CW + c);
+                id0 = v & 0xffffu;
+                id1 = v >> 16;
+            } else {
+                id0 = CL[r * L::CW + c];
+                id1 = CL[r * L::CW + c + 1];
+            }
+        }
+        // FOLD: the pair's folded Debye edges (column c's components, then column c + 1's), their
+        // numbers (a scan over the row's lanes) and their dd and state, loaded before the H half so
+        // that it hides the loads
+        unsigned fm = 0;           // bits 0-2: column c's components, 3-5: column c + 1's
+        int fq = 0;
+        float fw[6], fs[6];
+        if constexpr (FOLD) {
+            if (!pre) {
+                if (own_row && live0) fm = unsigned(lm[id0]) | (live1 ? unsigned(lm[id1]) << 3 : 0u);
+                const int cnt = __popc(fm);
+                int x = cnt;
+#pragma unroll
+                for (int d = 1; d < 32; d <<= 1) {
+                    const int y = __shfl_up_sync(0xffffffffu, x, d);
+                    if (lane >= d) x += y;
+                }
+                fq = fnext + (x - cnt);
+                int q = fq;
+#pragma unroll
+                for (int t = 0; t < 6; ++t) {
+                    fw[t] = 0.f;
+                    fs[t] = 0.f;
+                    if (fm >> t & 1u) {
+                        fw[t] = a.fdd[q];
+                        fs[t] = a.fstate[q];
+                        ++q;
+                    }
+                }
+                if (r >= 0 && p + 1 < i1) fnext = a.drow[((long long)bid * SEGMAX + (p + 1 - i0)) * 8 + r];
+            }
+        }
 
         // 1. new H: the pair (two columns, one packed update), and warp 0's extra point
         EPair nb{};
@@ -573,20 +652,6 @@ __device__ __forceinline__ void tma_march(const CUtensorMap& map_e, const CUtens
         // 2. new E on the owned points
         if (!pre) {
             if (own_row && live0) {
-                // the pair's two class ids in one aligned load (c is even)
-                unsigned id0, id1;
-                if constexpr (sizeof(CID) == 1) {
-                    const unsigned v = *reinterpret_cast<const uint16_t*>(CL + r * L::CW + c);
-                    id0 = v & 0xffu;
-                    id1 = v >> 8;
-                } else if constexpr (sizeof(CID) == 2) {
-                    const unsigned v = *reinterpret_cast<const uint32_t*>(CL + r * L::CW + c);
-                    id0 = v & 0xffffu;
-                    id1 = v >> 16;
-                } else {
-                    id0 = CL[r * L::CW + c];
-                    id1 = CL[r * L::CW + c + 1];
-                }
                 const CoefRef cf0 = coef_of<LOCAL>(a, lt, id0);
                 const CoefRef cf1 = coef_of<LOCAL>(a, lt, live1 ? id1 : id0);
                 const float2 hzj = *reinterpret_cast<const float2*>(hn + 2 * NC + no - L::NW);
@@ -598,6 +663,17 @@ __device__ __forceinline__ void tma_march(const CUtensorMap& map_e, const CUtens
                 const float* ze = ZL ? ZE + (r + 1) * g.pw : nullptr;
                 e_pair<ZL>(a, mz, cf0, cf1, ex, ey, ez, hxp, hyp, hzp, hzj, hxj, hyk, hxk, pyp, pzp, ai.inv_dd, ej, ek2, i,
                            jj, kk, live1, q0.ak, q1.ak, ze, zc);
+                if constexpr (FOLD) {
+                    if (fm) {   // in the fill's order: column c's components, then column c + 1's
+                        int q = fq;
+                        if (fm & 1u) fold_edge(a, ex.x, nb.x.x, cf0.cb[0], fw[0], fs[0], q++);
+                        if (fm & 2u) fold_edge(a, ey.x, nb.y.x, cf0.cb[1], fw[1], fs[1], q++);
+                        if (fm & 4u) fold_edge(a, ez.x, nb.z.x, cf0.cb[2], fw[2], fs[2], q++);
+                        if (fm & 8u) fold_edge(a, ex.y, nb.x.y, cf1.cb[0], fw[3], fs[3], q++);
+                        if (fm & 16u) fold_edge(a, ey.y, nb.y.y, cf1.cb[1], fw[4], fs[4], q++);
+                        if (fm & 32u) fold_edge(a, ez.y, nb.z.y, cf1.cb[2], fw[5], fs[5], q++);
+                    }
+                }
                 float* o = a.e_out + plane + goff;
                 *reinterpret_cast<float2*>(o) = ex;
                 *reinterpret_cast<float2*>(o + g.cs) = ey;
@@ -621,7 +697,7 @@ __device__ __forceinline__ void tma_march(const CUtensorMap& map_e, const CUtens
     // the last plane's stage (E(i1)) was waited on by the final iteration; nothing is in flight
 }
 
-template <int TJ, int TK, typename CID, int STAGES, int SEGMAX, bool LOCAL, int MINB>
+template <int TJ, int TK, typename CID, int STAGES, int SEGMAX, bool LOCAL, int MINB, bool FOLD = false>
 __global__ void __launch_bounds__(TMA_CONSUMERS + 32, MINB)
     k_tma_step(const __grid_constant__ CUtensorMap map_e, const __grid_constant__ CUtensorMap map_h,
                const __grid_constant__ CUtensorMap map_c, const __grid_constant__ CUtensorMap map_pze,
@@ -629,9 +705,9 @@ __global__ void __launch_bounds__(TMA_CONSUMERS + 32, MINB)
     extern __shared__ __align__(128) unsigned char smem_raw[];
     unsigned char* base = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
     if (a.blocks[a.block0 + int(blockIdx.x)].x & TMA_ZL_TILE)
-        tma_march<TJ, TK, CID, STAGES, SEGMAX, LOCAL, true>(map_e, map_h, map_c, map_pze, map_pzh, a, base);
+        tma_march<TJ, TK, CID, STAGES, SEGMAX, LOCAL, true, FOLD>(map_e, map_h, map_c, map_pze, map_pzh, a, base);
     else
-        tma_march<TJ, TK, CID, STAGES, SEGMAX, LOCAL, false>(map_e, map_h, map_c, map_pze, map_pzh, a, base);
+        tma_march<TJ, TK, CID, STAGES, SEGMAX, LOCAL, false, FOLD>(map_e, map_h, map_c, map_pze, map_pzh, a, base);
 }
 
 // One grid of a merged batch launch (k_batch_tma): its tensor maps (64-byte aligned in HBM; a

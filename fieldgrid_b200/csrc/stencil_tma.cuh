@@ -132,7 +132,9 @@ struct TmaLayout {
     static constexpr int BARS = al(2 * STAGES * 8);
     // the block's coefficient table, then (a folded Debye ADE) its entries' Debye masks
     static constexpr int LT = LOCAL ? al(LOCAL_CLASSES * 6 * 4 + LOCAL_CLASSES) : 0;
-    static constexpr int TOTAL = STAGES * STAGE + 2 * HN + AX + BARS + LT + 128;
+    // ZL: per consumer warp, the k-layer CPML terms of its row (two components x TK columns)
+    static constexpr int ZR = al((TJ + 1) * 2 * TK * 4);
+    static constexpr int TOTAL = STAGES * STAGE + 2 * HN + AX + BARS + LT + ZR + 128;
 };
 
 struct TmaArgs {
@@ -309,24 +311,13 @@ struct EPair {
     float2 x, y, z, zj, xj, yk, xk, zi, yi;
 };
 
-// The k-layer CPML terms of one column of a pair (z_terms on a single point, fed by the pair's t).
-template <int F>
-__device__ __forceinline__ void z_col(const TmaArgs& a, const AxisNode& ak, float d01, float d10, float& t01,
-                                      float& t10, bool run0, bool run1, const float* zrow, int zc, int i, int j,
-                                      bool own) {
-    float d[3][2] = {{0.f, d01}, {d10, 0.f}, {0.f, 0.f}};
-    float t[3][2] = {{0.f, t01}, {t10, 0.f}, {0.f, 0.f}};
-    z_terms<F>(a, ak, d, t, run0, run1, zrow, zc, i, j, own);
-    t01 = t[0][1];
-    t10 = t[1][0];
-}
-
 // New H of a column pair outside the CPML (h_node on both columns at once); dk, kn per column.
+// ZL: zr points at the pair's k-layer terms in its warp's row buffer (component 0 at zr, 1 at
+// zr + zs), formed by the row's dense pass; zf bit 0 / 1: column c / c + 1 has a live H slot.
 template <bool ZL>
 __device__ __forceinline__ void h_pair(const TmaArgs& a, float2 mz, const EPair& n, float2& hx, float2& hy, float2& hz, float di,
                                        float dj, float2 dk, bool jn, bool kn0, bool kn1, bool in, bool live1,
-                                       const AxisNode* ak0, const AxisNode* ak1, const float* zrow, int zc, int i,
-                                       int j, bool own) {
+                                       const float* zr, int zs, unsigned zf) {
     using namespace f2;
     const float2 d00 = sub(n.zj, n.z), d01 = sub(n.yk, n.y);
     const float2 d10 = sub(n.xk, n.x), d11 = sub(n.zi, n.z);
@@ -335,8 +326,13 @@ __device__ __forceinline__ void h_pair(const TmaArgs& a, float2 mz, const EPair&
     float2 t10 = mul(d10, dk, mz), t11 = mul(d11, bc(di), mz);
     const float2 t20 = mul(d20, bc(di), mz), t21 = mul(d21, bc(dj), mz);
     if constexpr (ZL) {
-        z_col<1>(a, *ak0, d01.x, d10.x, t01.x, t10.x, jn && kn0, kn0 && in, zrow, zc, i, j, own);
-        if (live1) z_col<1>(a, *ak1, d01.y, d10.y, t01.y, t10.y, jn && kn1, kn1 && in, zrow, zc, i, j, own);
+        if (zf & 3u) {   // z_terms<1>'s additions, in its order (t += r after the product)
+            const float2 r0 = *reinterpret_cast<const float2*>(zr), r1 = *reinterpret_cast<const float2*>(zr + zs);
+            if ((zf & 1u) && jn && kn0) t01.x = t01.x + r0.x;
+            if ((zf & 1u) && kn0 && in) t10.x = t10.x + r1.x;
+            if (live1 && (zf & 2u) && jn && kn1) t01.y = t01.y + r0.y;
+            if (live1 && (zf & 2u) && kn1 && in) t10.y = t10.y + r1.y;
+        }
     }
     const float2 km = bc(a.k_mu);
     const float2 nx = sub(hx, mul(km, sub(t00, t01), mz));
@@ -348,13 +344,13 @@ __device__ __forceinline__ void h_pair(const TmaArgs& a, float2 mz, const EPair&
 }
 
 // New E of a column pair outside the CPML (e_node on both columns); hj: H at j - 1, hk: H at k - 1
-// (columns c - 1 and c), p: H of plane i - 1.
+// (columns c - 1 and c), p: H of plane i - 1. ZL: as h_pair, zf bit 2 / 3: column c / c + 1 has a
+// live E slot.
 template <bool ZL>
 __device__ __forceinline__ void e_pair(const TmaArgs& a, float2 mz, const CoefRef& c0, const CoefRef& c1, float2& ex, float2& ey,
                                        float2& ez, float2 hx, float2 hy, float2 hz, float2 hzj, float2 hxj, float2 hyk,
                                        float2 hxk, float2 py, float2 pz, float ei, float ej, float2 ek, int i, int j,
-                                       int k, bool live1, const AxisNode* ak0, const AxisNode* ak1, const float* zrow,
-                                       int zc) {
+                                       int k, bool live1, const float* zr, int zs, unsigned zf) {
     using namespace f2;
     const float2 d00 = sub(hz, hzj), d01 = sub(hy, hyk);
     const float2 d10 = sub(hx, hxk), d11 = sub(hz, pz);
@@ -366,8 +362,13 @@ __device__ __forceinline__ void e_pair(const TmaArgs& a, float2 mz, const CoefRe
     const bool r10 = c0.cb[1] != 0.0f && k > 0 && i > 0, r11 = live1 && c1.cb[1] != 0.0f && i > 0;
     const bool r20 = c0.cb[2] != 0.0f && i > 0 && j > 0, r21 = live1 && c1.cb[2] != 0.0f && i > 0 && j > 0;
     if constexpr (ZL) {
-        z_col<0>(a, *ak0, d01.x, d10.x, t01.x, t10.x, r00, r10, zrow, zc, i, j, true);
-        if (live1) z_col<0>(a, *ak1, d01.y, d10.y, t01.y, t10.y, r01, r11, zrow, zc, i, j, true);
+        if (zf & 12u) {   // z_terms<0>'s additions
+            const float2 r0 = *reinterpret_cast<const float2*>(zr), r1 = *reinterpret_cast<const float2*>(zr + zs);
+            if ((zf & 4u) && r00) t01.x = t01.x + r0.x;
+            if ((zf & 4u) && r10) t10.x = t10.x + r1.x;
+            if ((zf & 8u) && r01) t01.y = t01.y + r0.y;
+            if ((zf & 8u) && r11) t10.y = t10.y + r1.y;
+        }
     }
     const float2 nx = add(mul(make_float2(c0.ca[0], c1.ca[0]), ex, mz), mul(make_float2(c0.cb[0], c1.cb[0]), sub(t00, t01), mz));
     const float2 ny = add(mul(make_float2(c0.ca[1], c1.ca[1]), ey, mz), mul(make_float2(c0.cb[1], c1.cb[1]), sub(t10, t11), mz));
@@ -421,6 +422,7 @@ __device__ __forceinline__ void tma_march(const CUtensorMap& map_e, const CUtens
     uint64_t* full = reinterpret_cast<uint64_t*>(base + STAGES * L::STAGE + 2 * L::HN + L::AX);
     uint64_t* empty = full + STAGES;
     float* lt = reinterpret_cast<float*>(base + STAGES * L::STAGE + 2 * L::HN + L::AX + L::BARS);
+    float* zr_all = reinterpret_cast<float*>(base + STAGES * L::STAGE + 2 * L::HN + L::AX + L::BARS + L::LT);
 
     const Geom& g = a.g;
     const int tid = threadIdx.x;
@@ -520,6 +522,21 @@ __device__ __forceinline__ void tma_march(const CUtensorMap& map_e, const CUtens
     const float2 mz = make_float2(a.neg0, a.neg0);
     float pyx = 0.f, pzx = 0.f;                                         // warp 0's extra point's
     bool bad = false;
+    // ZL: the tile columns [zc0, zc1) with a live k slot (the layer is contiguous within a tile),
+    // the pair's slot flags (bits 0/1: H slot of column c / c + 1, bits 2/3: E slot) and the warp's
+    // row buffer of k-layer terms (component 0 at column c, component 1 at TK + c)
+    int zc0 = TK, zc1 = 0;
+    unsigned zf = 0;
+    float* zw = zr_all + w * (2 * TK);
+    if constexpr (ZL) {
+        const AxisNode &z0 = axk[c + 1], &z1 = axk[c + 2];
+        const bool in0 = kk < g.n2, in1 = kk + 1 < g.n2;
+        zf = (in0 && z0.slot_h >= 0 ? 1u : 0u) | (in1 && z1.slot_h >= 0 ? 2u : 0u) |
+             (in0 && z0.slot_e >= 0 ? 4u : 0u) | (in1 && z1.slot_e >= 0 ? 8u : 0u);
+        const bool h0 = (zf & 5u) != 0, h1 = (zf & 10u) != 0;
+        zc0 = int(__reduce_min_sync(0xffffffffu, unsigned(h0 ? c : (h1 ? c + 1 : TK))));
+        zc1 = int(__reduce_max_sync(0xffffffffu, unsigned(h1 ? c + 2 : (h0 ? c + 1 : 0))));
+    }
     // FOLD: the row's first folded edge in the next owned plane, loaded a plane ahead
     int fnext = 0;
     if constexpr (FOLD) {
@@ -594,6 +611,29 @@ __device__ __forceinline__ void tma_march(const CUtensorMap& map_e, const CUtens
             }
         }
 
+        // ZL: the row's k-layer H terms (z_terms<1> on every live point of the row's layer columns),
+        // one lane per (component, column): component 0 is Hx's (dEy/dk), 1 is Hy's (dEx/dk)
+        if constexpr (ZL) {
+            const int nz = zc1 - zc0;
+            __syncwarp();
+            for (int t = lane; t < 2 * nz; t += 32) {
+                const int cp = t >= nz ? 1 : 0, cc = zc0 + t - cp * nz, kq = k0 + cc;
+                const AxisNode& ak = axk[cc + 1];
+                const int sl = ak.slot_h;
+                const bool kn = kq + 1 < g.n2;
+                if (row_live && kq < g.n2 && sl >= 0 && (cp ? kn && in : q0.jn && kn)) {
+                    const int off = (r + 1) * L::EW + cc + 4 + (cp ? 0 : EC);
+                    const float d = E[off + 1] - E[off];
+                    const float rv = ak.bh * ZH[(r + 1) * g.pw + cp * zc + sl] + ak.ch * d * ak.raw_inv_d;
+                    zw[cp * TK + cc] = rv;
+                    const int kp = k0 + (cc & ~1);
+                    if (!pre && r >= 0 && jj >= orow.x && jj < orow.y && kp >= a.kbeg && kp < a.kend)
+                        a.psi_h_out[g.psi_off[9 + cp * 3 + 2] + ((long long)i * g.n1 + jj) * g.pw + sl] = rv;
+                }
+            }
+            __syncwarp();
+        }
+
         // 1. new H: the pair (two columns, one packed update), and warp 0's extra point
         EPair nb{};
         float2 hxp = make_float2(0.f, 0.f), hyp = hxp, hzp = hxp;
@@ -610,9 +650,7 @@ __device__ __forceinline__ void tma_march(const CUtensorMap& map_e, const CUtens
             hxp = *reinterpret_cast<const float2*>(H + ho);
             hyp = *reinterpret_cast<const float2*>(H + HC + ho);
             hzp = *reinterpret_cast<const float2*>(H + 2 * HC + ho);
-            const float* zr = ZL ? ZH + (r + 1) * g.pw : nullptr;
-            h_pair<ZL>(a, mz, nb, hxp, hyp, hzp, ai.inv_d, dj, dk2, q0.jn, q0.kn, q1.kn, in, live1, q0.ak, q1.ak, zr, zc, i,
-                       jj, own);
+            h_pair<ZL>(a, mz, nb, hxp, hyp, hzp, ai.inv_d, dj, dk2, q0.jn, q0.kn, q1.kn, in, live1, zw + c, TK, zf);
             *reinterpret_cast<float2*>(hn + no) = hxp;
             *reinterpret_cast<float2*>(hn + NC + no) = hyp;
             *reinterpret_cast<float2*>(hn + 2 * NC + no) = hzp;
@@ -650,6 +688,31 @@ __device__ __forceinline__ void tma_march(const CUtensorMap& map_e, const CUtens
         }
 
         // 2. new E on the owned points
+        // ZL: the row's k-layer E terms (z_terms<0> on its owned live points, psi updated in place):
+        // component 0 is Ex's (dHy/dk), 1 is Ey's (dHx/dk), from the new H tile
+        if constexpr (ZL) {
+            if (!pre) {
+                const int nz = zc1 - zc0;
+                __syncwarp();
+                for (int t = lane; t < 2 * nz; t += 32) {
+                    const int cp = t >= nz ? 1 : 0, cc = zc0 + t - cp * nz, kq = k0 + cc, kp = k0 + (cc & ~1);
+                    const AxisNode& ak = axk[cc + 1];
+                    const int sl = ak.slot_e;
+                    if (r >= 0 && row_live && kq < g.n2 && sl >= 0 && jj >= orow.x && jj < orow.y && kp >= a.kbeg &&
+                        kp < a.kend) {
+                        const CoefRef cf = coef_of<LOCAL>(a, lt, CL[r * L::CW + cc]);
+                        if ((cp ? cf.cb[1] : cf.cb[0]) != 0.0f && kq > 0 && (cp ? i > 0 : jj > 0)) {
+                            const int off = (r + 1) * L::NW + cc + 2 + (cp ? 0 : NC);
+                            const float d = hn[off] - hn[off - 1];
+                            const float rv = ak.be * ZE[(r + 1) * g.pw + cp * zc + sl] + ak.ce * d * ak.raw_inv_dd;
+                            zw[cp * TK + cc] = rv;
+                            a.psi_e[g.psi_off[cp * 3 + 2] + ((long long)i * g.n1 + jj) * g.pw + sl] = rv;
+                        }
+                    }
+                }
+                __syncwarp();
+            }
+        }
         if (!pre) {
             if (own_row && live0) {
                 const CoefRef cf0 = coef_of<LOCAL>(a, lt, id0);
@@ -660,9 +723,8 @@ __device__ __forceinline__ void tma_march(const CUtensorMap& map_e, const CUtens
                 // a dead second column keeps E = 0
                 float2 ex = make_float2(nb.x.x, live1 ? nb.x.y : 0.f), ey = make_float2(nb.y.x, live1 ? nb.y.y : 0.f);
                 float2 ez = make_float2(nb.z.x, live1 ? nb.z.y : 0.f);
-                const float* ze = ZL ? ZE + (r + 1) * g.pw : nullptr;
                 e_pair<ZL>(a, mz, cf0, cf1, ex, ey, ez, hxp, hyp, hzp, hzj, hxj, hyk, hxk, pyp, pzp, ai.inv_dd, ej, ek2, i,
-                           jj, kk, live1, q0.ak, q1.ak, ze, zc);
+                           jj, kk, live1, zw + c, TK, zf);
                 if constexpr (FOLD) {
                     if (fm) {   // in the fill's order: column c's components, then column c + 1's
                         int q = fq;

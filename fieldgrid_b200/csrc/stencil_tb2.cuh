@@ -572,7 +572,7 @@ __global__ void __launch_bounds__(TB_THREADS, 1)
                const __grid_constant__ CUtensorMap map_c, const __grid_constant__ CUtensorMap map_zh,
                const __grid_constant__ CUtensorMap map_ze, Tb2Args a) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    unsigned char* base = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
+    unsigned char* base = tma::align128(smem_raw);
     if (a.blocks[blockIdx.x].x & TMA_ZL_TILE)
         tb2_march<STAGES, true>(map_e, map_h, map_c, map_zh, map_ze, a, base);
     else

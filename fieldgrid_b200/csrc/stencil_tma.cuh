@@ -30,6 +30,11 @@ namespace tma {
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return uint32_t(__cvta_generic_to_shared(p)); }
 
+// The first 128-byte boundary at or after p (a dynamic shared-memory array). The offset is added to
+// the array's own pointer, so the compiler still sees a shared-memory address and emits shared
+// loads and stores (an integer round trip of the pointer would leave generic accesses).
+__device__ __forceinline__ unsigned char* align128(unsigned char* p) { return p + ((128u - (smem_u32(p) & 127u)) & 127u); }
+
 __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
 }
@@ -765,7 +770,7 @@ __global__ void __launch_bounds__(TMA_CONSUMERS + 32, MINB)
                const __grid_constant__ CUtensorMap map_c, const __grid_constant__ CUtensorMap map_pze,
                const __grid_constant__ CUtensorMap map_pzh, TmaArgs a) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    unsigned char* base = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
+    unsigned char* base = tma::align128(smem_raw);
     if (a.blocks[a.block0 + int(blockIdx.x)].x & TMA_ZL_TILE)
         tma_march<TJ, TK, CID, STAGES, SEGMAX, LOCAL, true, FOLD>(map_e, map_h, map_c, map_pze, map_pzh, a, base);
     else
@@ -789,7 +794,7 @@ __global__ void __launch_bounds__(TMA_CONSUMERS + 32, MINB)
     k_batch_tma(const TmaGrid* __restrict__ grids, const int* __restrict__ block_grid, int parity) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     __shared__ __align__(16) TmaArgs sa;
-    unsigned char* base = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
+    unsigned char* base = tma::align128(smem_raw);
     const TmaGrid& G = grids[block_grid[blockIdx.x]];
     static_assert(sizeof(TmaArgs) % 4 == 0, "TmaArgs copies as words");
     const int* src = reinterpret_cast<const int*>(&G.a[parity]);

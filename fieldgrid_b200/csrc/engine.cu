@@ -259,6 +259,13 @@ struct Session {
     cudaStream_t aux = nullptr;
     cudaEvent_t aux_ready[2] = {nullptr, nullptr}, aux_done[2] = {nullptr, nullptr};
     bool aux_on = false, aux_pending[2] = {false, false};
+    // captured TMA steps with a CPML shell: k_shell_h runs on `shell_st` beside the march (it reads
+    // the step's inputs only), at the lowest priority and the march at the highest, so that its
+    // blocks take the room two march blocks leave on an SM; k_shell_e joins both
+    cudaStream_t shell_st = nullptr;
+    cudaEvent_t shell_fork = nullptr, shell_join = nullptr;
+    int prio_lo = 0, prio_hi = 0;
+    bool capturing = false;
     std::map<int, cudaGraphExec_t> slot_graphs;      // captured steps by (kind, phase t mod 6)
     std::vector<void*> extra_allocs;
 };
@@ -532,7 +539,21 @@ int launch_tma(Session& s, int parity, float* e_out, float* h_out, float* psi_h_
     const CUtensorMap& pze = t.pz ? t.pze : t.c;
     const CUtensorMap& pzh = t.pz ? t.pzh[parity] : t.c;
     with_tma_kernel(s.cid_bytes, s.local, s.fold, t.shape, [&](auto kern, int smem) {
-        kern<<<unsigned(t.blocks), TMA_CONSUMERS + 32, smem, s.stream>>>(t.e[parity], t.h[parity], t.c, pze, pzh, a);
+        if (s.capturing && s.shell_st) {
+            cudaLaunchConfig_t cfg{};
+            cfg.gridDim = dim3(unsigned(t.blocks));
+            cfg.blockDim = dim3(TMA_CONSUMERS + 32);
+            cfg.dynamicSmemBytes = size_t(smem);
+            cfg.stream = s.stream;
+            cudaLaunchAttribute at[1];
+            at[0].id = cudaLaunchAttributePriority;
+            at[0].val.priority = s.prio_hi;
+            cfg.attrs = at;
+            cfg.numAttrs = 1;
+            cudaLaunchKernelEx(&cfg, kern, t.e[parity], t.h[parity], t.c, pze, pzh, a);
+        } else {
+            kern<<<unsigned(t.blocks), TMA_CONSUMERS + 32, smem, s.stream>>>(t.e[parity], t.h[parity], t.c, pze, pzh, a);
+        }
         return true;
     });
     return cudaPeekAtLastError() == cudaSuccess ? 0 : 1;
@@ -576,8 +597,30 @@ int enqueue_step(Session& s, int parity, std::string& err) {
             FG_CUDA(cudaStreamWaitEvent(st, s.aux_done[parity], 0));
             s.aux_pending[parity] = false;
         }
-        mark("fused_step");
         const bool tma = s.tma.ok && !s.direct;
+        const unsigned shell_rows = s.shell.ra + s.shell.rb + s.shell.rc;
+        const bool shell_side = tma && shell_rows > 0 && s.capturing && s.shell_st;
+        if (shell_side) {
+            // the shell's H update beside the march (both read only the step's inputs)
+            FG_CUDA(cudaEventRecord(s.shell_fork, st));
+            FG_CUDA(cudaStreamWaitEvent(s.shell_st, s.shell_fork, 0));
+            const unsigned gs = (shell_rows + SHELL_SIDE_THREADS / 32 - 1) / (SHELL_SIDE_THREADS / 32);
+            cudaLaunchConfig_t cfg{};
+            cfg.gridDim = dim3(gs);
+            cfg.blockDim = dim3(SHELL_SIDE_THREADS);
+            cfg.stream = s.shell_st;
+            cudaLaunchAttribute at[1];
+            at[0].id = cudaLaunchAttributePriority;
+            at[0].val.priority = s.prio_lo;
+            cfg.attrs = at;
+            cfg.numAttrs = 1;
+            FG_CUDA(cudaLaunchKernelEx(&cfg, k_shell_h_side, g, s.shell, s.kax, (const float*)e_in, (const float*)h_in,
+                                       h_out, (const float*)(parity ? s.psi_h2 : s.psi), parity ? s.psi : s.psi_h2,
+                                       (const float*)(parity ? s.psi_h2 : s.psi), parity ? s.psi : s.psi_h2,
+                                       s.sc.k_mu));
+            FG_CUDA(cudaEventRecord(s.shell_join, s.shell_st));
+        }
+        mark("fused_step");
         int rc = s.direct && s.boxed
                      ? launch_fused_box(s.cid_bytes, g, s.node_class, s.classes, e_in, h_in, e_out, h_out, s.psi,
                                         parity ? s.psi_h2 : s.psi, parity ? s.psi : s.psi_h2, s.sc.k_mu, s.counter,
@@ -588,14 +631,17 @@ int enqueue_step(Session& s, int parity, std::string& err) {
                                     parity ? s.psi_h2 : s.psi, parity ? s.psi : s.psi_h2, s.sc.k_mu, s.counter,
                                     s.n_wires > 0, st);
         if (rc) { err = "fused step launch failed"; return FG_ERR_CUDA; }
-        const unsigned shell_rows = s.shell.ra + s.shell.rb + s.shell.rc;
         if (tma && shell_rows > 0) {
             // the CPML shell around the march's clean box, one warp per row
             const unsigned gb = (shell_rows + SHELL_THREADS / 32 - 1) / (SHELL_THREADS / 32);
-            mark("shell_h");
-            k_shell_h<<<gb, SHELL_THREADS, 0, st>>>(g, s.shell, s.kax, e_in, h_in, h_out, parity ? s.psi_h2 : s.psi,
-                                                    parity ? s.psi : s.psi_h2, parity ? s.psi_h2 : s.psi,
-                                                    parity ? s.psi : s.psi_h2, s.sc.k_mu);
+            if (shell_side) {
+                FG_CUDA(cudaStreamWaitEvent(st, s.shell_join, 0));
+            } else {
+                mark("shell_h");
+                k_shell_h<<<gb, SHELL_THREADS, 0, st>>>(g, s.shell, s.kax, e_in, h_in, h_out, parity ? s.psi_h2 : s.psi,
+                                                        parity ? s.psi : s.psi_h2, parity ? s.psi_h2 : s.psi,
+                                                        parity ? s.psi : s.psi_h2, s.sc.k_mu);
+            }
             mark("shell_e");
             switch (s.cid_bytes) {
                 case 1: k_shell_e<uint8_t><<<gb, SHELL_THREADS, 0, st>>>(g, s.shell, s.kax, (const uint8_t*)s.node_class, s.classes, h_out, e_in, e_out, s.psi, s.psi, s.psi); break;
@@ -687,7 +733,9 @@ int capture(Session& s, int steps, int parity0, cudaGraphExec_t* out, std::strin
     FG_CUDA(cudaStreamBeginCapture(s.stream, cudaStreamCaptureModeThreadLocal));
     int rc = FG_OK;
     s.aux_on = s.aux != nullptr;
+    s.capturing = true;
     for (int q = 0; q < steps && rc == FG_OK; ++q) rc = enqueue_step(s, (parity0 + q) & 1, err);
+    s.capturing = false;
     for (int p = 0; p < 2; ++p)   // the graph ends with its extras joined
         if (s.aux_pending[p]) {
             if (rc == FG_OK && cudaStreamWaitEvent(s.stream, s.aux_done[p], 0) != cudaSuccess) rc = FG_ERR_CUDA;
@@ -697,7 +745,7 @@ int capture(Session& s, int steps, int parity0, cudaGraphExec_t* out, std::strin
     cudaError_t ce = cudaStreamEndCapture(s.stream, &graph);
     if (rc) return rc;
     if (ce != cudaSuccess) { err = std::string("cudaStreamEndCapture: ") + cudaGetErrorString(ce); return FG_ERR_CUDA; }
-    ce = cudaGraphInstantiate(out, graph, 0);
+    ce = cudaGraphInstantiate(out, graph, s.shell_st ? cudaGraphInstantiateFlagUseNodePriority : 0);
     cudaGraphDestroy(graph);
     if (ce != cudaSuccess) { err = std::string("cudaGraphInstantiate: ") + cudaGetErrorString(ce); return FG_ERR_CUDA; }
     return FG_OK;
@@ -1896,6 +1944,17 @@ int session_new(Gpu* gpu, const HostSim& sim, const RunSpec& rs, Session** out, 
             FG_CUDA(cudaEventCreateWithFlags(&s->aux_done[p], cudaEventDisableTiming));
         }
     }
+    {
+        // the shell's H update beside the march in captured steps (FIELDGRID_SHELL_SIDE=0: after it)
+        const char* sv = std::getenv("FIELDGRID_SHELL_SIDE");
+        const bool off = sv && sv[0] == '0';
+        if (!off && s->fused && s->tma.ok && !s->direct && s->shell.ra + s->shell.rb + s->shell.rc > 0) {
+            FG_CUDA(cudaDeviceGetStreamPriorityRange(&s->prio_lo, &s->prio_hi));
+            FG_CUDA(cudaStreamCreateWithPriority(&s->shell_st, cudaStreamNonBlocking, s->prio_lo));
+            FG_CUDA(cudaEventCreateWithFlags(&s->shell_fork, cudaEventDisableTiming));
+            FG_CUDA(cudaEventCreateWithFlags(&s->shell_join, cudaEventDisableTiming));
+        }
+    }
     // graphs: a block of even length (the fused step alternates buffers), a pair and singles
     s->graph_steps = 32;
     rc = capture(*s, s->graph_steps, 0, &s->graph_many, err);
@@ -1918,6 +1977,9 @@ void session_free(Session* s) {
     for (auto& kv : s->slot_graphs) cudaGraphExecDestroy(kv.second);
     for (void* p : s->extra_allocs) cudaFree(p);
     if (s->side) cudaStreamDestroy(s->side);
+    if (s->shell_st) cudaStreamDestroy(s->shell_st);
+    if (s->shell_fork) cudaEventDestroy(s->shell_fork);
+    if (s->shell_join) cudaEventDestroy(s->shell_join);
     if (s->fork_ev) cudaEventDestroy(s->fork_ev);
     if (s->join_ev) cudaEventDestroy(s->join_ev);
     if (s->aux) cudaStreamDestroy(s->aux);

@@ -230,6 +230,23 @@ __global__ void __launch_bounds__(SHELL_THREADS, 4) k_shell_h(Geom g, ShellRows 
                 pz_in, pz_out, k_mu);
 }
 
+// k_shell_h in blocks of four rows (128 threads, 64 registers): the launch that runs beside the
+// march in a captured step, one block of it fitting on an SM next to two march blocks (2 x 288
+// threads x 96 registers + 128 x 64 of the 65,536), so the shell's latency-bound row walks fill
+// the march's idle issue slots instead of following it.
+constexpr int SHELL_SIDE_THREADS = 128;
+__global__ void __launch_bounds__(SHELL_SIDE_THREADS, 8) k_shell_h_side(Geom g, ShellRows b, KAxis kx,
+                                                                  const float* __restrict__ e_in,
+                                                                  const float* __restrict__ h_in,
+                                                                  float* __restrict__ h_out,
+                                                                  const float* __restrict__ psi_in,
+                                                                  float* __restrict__ psi_out,
+                                                                  const float* __restrict__ pz_in,
+                                                                  float* __restrict__ pz_out, float k_mu) {
+    shell_h_row(g, b, kx, blockIdx.x * (SHELL_SIDE_THREADS / 32) + (threadIdx.x >> 5), e_in, h_in, h_out, psi_in,
+                psi_out, pz_in, pz_out, k_mu);
+}
+
 template <typename CID>
 __global__ void __launch_bounds__(SHELL_THREADS) k_shell_e(Geom g, ShellRows b, KAxis kx, const CID* __restrict__ node_class,
                                                            const DevCoef* __restrict__ classes,

@@ -139,7 +139,9 @@ struct TmaLayout {
     static constexpr int LT = LOCAL ? al(LOCAL_CLASSES * 6 * 4 + LOCAL_CLASSES) : 0;
     // ZL: per consumer warp, the k-layer CPML terms of its row (two components x TK columns)
     static constexpr int ZR = al((TJ + 1) * 2 * TK * 4);
-    static constexpr int TOTAL = STAGES * STAGE + 2 * HN + AX + BARS + LT + ZR + 128;
+    // ZL: the k factors (b, c, raw) of the block's columns k0-1 .. k0+TK+2, for H then for E
+    static constexpr int ZK = al(2 * (TK + 4) * 16);
+    static constexpr int TOTAL = STAGES * STAGE + 2 * HN + AX + BARS + LT + ZR + ZK + 128;
 };
 
 struct TmaArgs {
@@ -428,6 +430,8 @@ __device__ __forceinline__ void tma_march(const CUtensorMap& map_e, const CUtens
     uint64_t* empty = full + STAGES;
     float* lt = reinterpret_cast<float*>(base + STAGES * L::STAGE + 2 * L::HN + L::AX + L::BARS);
     float* zr_all = reinterpret_cast<float*>(base + STAGES * L::STAGE + 2 * L::HN + L::AX + L::BARS + L::LT);
+    float4* zkh = reinterpret_cast<float4*>(base + STAGES * L::STAGE + 2 * L::HN + L::AX + L::BARS + L::LT + L::ZR);
+    float4* zke = zkh + (TK + 4);
 
     const Geom& g = a.g;
     const int tid = threadIdx.x;
@@ -453,6 +457,12 @@ __device__ __forceinline__ void tma_march(const CUtensorMap& map_e, const CUtens
         else if (q < TJ + 2 + TK + 4) v = g.ax[2][min(max(k0 - 1 + (q - TJ - 2), 0), g.n2 - 1)];
         else v = g.ax[0][min(p_first + (q - TJ - 2 - TK - 4), g.n0 - 1)];
         axj[q] = v;
+        if constexpr (ZL) {
+            if (q >= TJ + 2 && q < TJ + 2 + TK + 4) {
+                zkh[q - TJ - 2] = make_float4(v.bh, v.ch, v.raw_inv_d, 0.f);
+                zke[q - TJ - 2] = make_float4(v.be, v.ce, v.raw_inv_dd, 0.f);
+            }
+        }
     }
     if constexpr (LOCAL) {
         const float* src = a.tables + (long long)bid * (LOCAL_CLASSES * 6);
@@ -542,6 +552,27 @@ __device__ __forceinline__ void tma_march(const CUtensorMap& map_e, const CUtens
         zc0 = int(__reduce_min_sync(0xffffffffu, unsigned(h0 ? c : (h1 ? c + 1 : TK))));
         zc1 = int(__reduce_max_sync(0xffffffffu, unsigned(h1 ? c + 2 : (h0 ? c + 1 : 0))));
     }
+    // ZL: the lane's own item of the dense passes (t = lane < 2 (zc1 - zc0)), its plane-invariant
+    // parts formed once: bit 0 the H term is live (all but the i+1 test), 1 it is stored, 2 the E
+    // term is live (all but the class's cb and the i > 0 test); bits 8-14 the column, 15 the
+    // component, 16-23 the H slot, 24-31 the E slot; zoe / zoh its offsets in the E box / new-H tile
+    unsigned zi = 0;
+    int zoe = 0, zoh = 0;
+    if constexpr (ZL) {
+        const int nz = zc1 - zc0;
+        if (lane < 2 * nz) {
+            const int cp = lane >= nz ? 1 : 0, cc = zc0 + lane - cp * nz, kq = k0 + cc, kp = k0 + (cc & ~1);
+            const AxisNode& ak = axk[cc + 1];
+            const bool kn = kq + 1 < g.n2;
+            const bool opt = r >= 0 && jj >= orow.x && jj < orow.y && kp >= a.kbeg && kp < a.kend;
+            const bool hl = row_live && kq < g.n2 && ak.slot_h >= 0 && (cp ? kn : q0.jn && kn);
+            const bool el = opt && row_live && kq < g.n2 && ak.slot_e >= 0 && kq > 0 && (cp || jj > 0);
+            zi = (hl ? 1u : 0u) | (hl && opt ? 2u : 0u) | (el ? 4u : 0u) | (unsigned(cc) << 8) | (unsigned(cp) << 15) |
+                 (unsigned(max(ak.slot_h, 0)) << 16) | (unsigned(max(ak.slot_e, 0)) << 24);
+            zoe = (r + 1) * L::EW + cc + 4 + (cp ? 0 : EC);
+            zoh = (r + 1) * L::NW + cc + 2 + (cp ? 0 : NC);
+        }
+    }
     // FOLD: the row's first folded edge in the next owned plane, loaded a plane ahead
     int fnext = 0;
     if constexpr (FOLD) {
@@ -620,8 +651,18 @@ __device__ __forceinline__ void tma_march(const CUtensorMap& map_e, const CUtens
         // one lane per (component, column): component 0 is Hx's (dEy/dk), 1 is Hy's (dEx/dk)
         if constexpr (ZL) {
             const int nz = zc1 - zc0;
+            const long long zpl = (long long)i * g.n1 * g.pw;   // the plane's first z-slab row
             __syncwarp();
-            for (int t = lane; t < 2 * nz; t += 32) {
+            if ((zi & 1u) && (!(zi & 0x8000u) || in)) {
+                const int cc = int(zi >> 8 & 127u), cp = int(zi >> 15 & 1u), sl = int(zi >> 16 & 255u);
+                const float4 f = zkh[cc + 1];
+                const float d = E[zoe + 1] - E[zoe];
+                const float rv = f.x * ZH[(r + 1) * g.pw + cp * zc + sl] + f.y * d * f.z;
+                zw[cp * TK + cc] = rv;
+                if ((zi & 2u) && !pre)
+                    a.psi_h_out[(cp ? g.psi_off[9 + 1 * 3 + 2] : g.psi_off[9 + 0 * 3 + 2]) + zpl + (jj * g.pw + sl)] = rv;
+            }
+            for (int t = lane + 32; t < 2 * nz; t += 32) {   // layers wider than 16 columns in a tile
                 const int cp = t >= nz ? 1 : 0, cc = zc0 + t - cp * nz, kq = k0 + cc;
                 const AxisNode& ak = axk[cc + 1];
                 const int sl = ak.slot_h;
@@ -698,8 +739,20 @@ __device__ __forceinline__ void tma_march(const CUtensorMap& map_e, const CUtens
         if constexpr (ZL) {
             if (!pre) {
                 const int nz = zc1 - zc0;
+                const long long zpl = (long long)i * g.n1 * g.pw;
                 __syncwarp();
-                for (int t = lane; t < 2 * nz; t += 32) {
+                if (zi & 4u) {
+                    const int cc = int(zi >> 8 & 127u), cp = int(zi >> 15 & 1u), sl = int(zi >> 24);
+                    const CoefRef cf = coef_of<LOCAL>(a, lt, CL[r * L::CW + cc]);
+                    if ((cp ? cf.cb[1] : cf.cb[0]) != 0.0f && (!cp || i > 0)) {
+                        const float4 f = zke[cc + 1];
+                        const float d = hn[zoh] - hn[zoh - 1];
+                        const float rv = f.x * ZE[(r + 1) * g.pw + cp * zc + sl] + f.y * d * f.z;
+                        zw[cp * TK + cc] = rv;
+                        a.psi_e[(cp ? g.psi_off[1 * 3 + 2] : g.psi_off[0 * 3 + 2]) + zpl + (jj * g.pw + sl)] = rv;
+                    }
+                }
+                for (int t = lane + 32; t < 2 * nz; t += 32) {
                     const int cp = t >= nz ? 1 : 0, cc = zc0 + t - cp * nz, kq = k0 + cc, kp = k0 + (cc & ~1);
                     const AxisNode& ak = axk[cc + 1];
                     const int sl = ak.slot_e;

@@ -451,7 +451,9 @@ int batch_capture(Batch& B, int steps, int parity0, cudaGraphExec_t* out, std::s
         for (size_t b = 0; b < B.s.size() && rc == FG_OK; ++b) {
             Session& S = *B.s[b];
             FG_CUDA(cudaStreamWaitEvent(S.stream, B.fork, 0));
+            S.capturing = S.shell_st != nullptr;   // the grid's shell H update beside its march
             for (int q = 0; q < steps && rc == FG_OK; ++q) rc = enqueue_step(S, (parity0 + q) & 1, err);
+            S.capturing = false;
             FG_CUDA(cudaEventRecord(B.join[b], S.stream));
             FG_CUDA(cudaStreamWaitEvent(B.stream, B.join[b], 0));
         }
@@ -461,7 +463,7 @@ int batch_capture(Batch& B, int steps, int parity0, cudaGraphExec_t* out, std::s
     cudaError_t ce = cudaStreamEndCapture(B.stream, &graph);
     if (rc) return rc;
     if (ce != cudaSuccess) { err = std::string("cudaStreamEndCapture: ") + cudaGetErrorString(ce); return FG_ERR_CUDA; }
-    ce = cudaGraphInstantiate(out, graph, 0);
+    ce = cudaGraphInstantiate(out, graph, cudaGraphInstantiateFlagUseNodePriority);
     cudaGraphDestroy(graph);
     if (ce != cudaSuccess) { err = std::string("cudaGraphInstantiate: ") + cudaGetErrorString(ce); return FG_ERR_CUDA; }
     return FG_OK;

@@ -1933,6 +1933,18 @@ int session_new(Gpu* gpu, const HostSim& sim, const RunSpec& rs, Session** out, 
         PhaseClock& c;
         ~Done() { c.mark("graphs"); }
     } done{clk};
+    {
+        // the shell's H update beside the march in captured steps, the
+        // session's own graphs or a batch's branches (FIELDGRID_SHELL_SIDE=0: after it)
+        const char* sv = std::getenv("FIELDGRID_SHELL_SIDE");
+        const bool off = sv && sv[0] == '0';
+        if (!off && !s->slots && s->fused && s->tma.ok && !s->direct && s->shell.ra + s->shell.rb + s->shell.rc > 0) {
+            FG_CUDA(cudaDeviceGetStreamPriorityRange(&s->prio_lo, &s->prio_hi));
+            FG_CUDA(cudaStreamCreateWithPriority(&s->shell_st, cudaStreamNonBlocking, s->prio_lo));
+            FG_CUDA(cudaEventCreateWithFlags(&s->shell_fork, cudaEventDisableTiming));
+            FG_CUDA(cudaEventCreateWithFlags(&s->shell_join, cudaEventDisableTiming));
+        }
+    }
     if (!rs.graphs || s->slots) {
         *out = s.release();
         return FG_OK;
@@ -1942,17 +1954,6 @@ int session_new(Gpu* gpu, const HostSim& sim, const RunSpec& rs, Session** out, 
         for (int p = 0; p < 2; ++p) {
             FG_CUDA(cudaEventCreateWithFlags(&s->aux_ready[p], cudaEventDisableTiming));
             FG_CUDA(cudaEventCreateWithFlags(&s->aux_done[p], cudaEventDisableTiming));
-        }
-    }
-    {
-        // the shell's H update beside the march in captured steps (FIELDGRID_SHELL_SIDE=0: after it)
-        const char* sv = std::getenv("FIELDGRID_SHELL_SIDE");
-        const bool off = sv && sv[0] == '0';
-        if (!off && s->fused && s->tma.ok && !s->direct && s->shell.ra + s->shell.rb + s->shell.rc > 0) {
-            FG_CUDA(cudaDeviceGetStreamPriorityRange(&s->prio_lo, &s->prio_hi));
-            FG_CUDA(cudaStreamCreateWithPriority(&s->shell_st, cudaStreamNonBlocking, s->prio_lo));
-            FG_CUDA(cudaEventCreateWithFlags(&s->shell_fork, cudaEventDisableTiming));
-            FG_CUDA(cudaEventCreateWithFlags(&s->shell_join, cudaEventDisableTiming));
         }
     }
     // graphs: a block of even length (the fused step alternates buffers), a pair and singles

@@ -163,7 +163,7 @@ int fg_sim_coefs(const fg_sim* sim, uint32_t comp, float* ca, float* cb) {
     if (!sim || comp > 2 || !ca || !cb) return FG_ERR_INVALID;
     const HostSim& s = *sim->s;
     for (size_t id = 0; id < s.nn; ++id) {
-        const Coef& c = s.classes[s.node_class[id]];
+        const Coef& c = s.classes[s.cls(id)];
         ca[id] = c.ca[comp];
         cb[id] = c.cb[comp];
     }

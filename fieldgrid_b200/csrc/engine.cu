@@ -12,6 +12,7 @@
 #include <map>
 #include <memory>
 #include <set>
+#include <type_traits>
 #include <string>
 #include <vector>
 
@@ -879,7 +880,7 @@ SlotPlan plan_slots(const HostSim& sim, const Geom& g, bool z_layer, const std::
                     if (k < 0 || k >= g.n2) continue;
                     const uint64_t id = (uint64_t(i) * n1 + uint64_t(j)) * n2 + uint64_t(k);
                     Key key;
-                    key.gid = sim.node_class[id];
+                    key.gid = sim.cls(id);
                     dd_of(id, key.dd);
                     if (key.gid == last.gid && std::memcmp(key.dd, last.dd, 12) == 0) {
                         idp[(size_t(i - (i0 - 1)) * 16 + size_t(r + 1)) * TB_CW + size_t(cc + 1)] = last_val;
@@ -1644,22 +1645,35 @@ int session_new(Gpu* gpu, const HostSim& sim, const RunSpec& rs, Session** out, 
     FG_CUDA(cudaMemsetAsync(s->arena, 0, need, st));
     // node classes, narrowed and laid out with the row pitch while they are staged for the upload
     {
-        const uint32_t* src_c = sim.node_class.data();
+        const uint32_t* src32 = sim.node_class.data();     // one of the two holds the ids
+        const uint16_t* src16 = sim.node_class16.data();
+        const bool s16 = !sim.node_class16.empty();
         const int cb = s->cid_bytes;
         const size_t p2 = size_t(g.p2);
+        // columns [k0, kn) of row r into o as cb-byte ids, the pitch padding (k >= n2) zero
+        auto row = [&](auto* in, auto* o, size_t k0, size_t kn) {
+            using T = std::remove_pointer_t<decltype(o)>;
+            const size_t kv = std::min(kn, n2);
+            for (size_t k = k0; k < kv; ++k) o[k - k0] = T(in[k]);
+            for (size_t k = std::max(k0, n2); k < kn; ++k) o[k - k0] = T(0);
+        };
         auto narrow = [&](char* buf, size_t off, size_t n) {
             // bytes [off, off + n) of the pitched array: elements off / cb .. (off + n) / cb
             const size_t e0 = off / size_t(cb), e1 = (off + n) / size_t(cb);
             size_t e = e0;
             while (e < e1) {
                 const size_t r = e / p2, k0 = e % p2, kn = std::min(p2, k0 + (e1 - e));
-                const uint32_t* in = src_c + r * n2;
                 char* o = buf + (e - e0) * size_t(cb);
-                for (size_t k = k0; k < kn; ++k) {
-                    const uint32_t v = k < n2 ? in[k] : 0u;
-                    if (cb == 1) o[k - k0] = char(uint8_t(v));
-                    else if (cb == 2) reinterpret_cast<uint16_t*>(o)[k - k0] = uint16_t(v);
-                    else reinterpret_cast<uint32_t*>(o)[k - k0] = v;
+                if (s16) {
+                    const uint16_t* in = src16 + r * n2;
+                    if (cb == 1) row(in, reinterpret_cast<uint8_t*>(o), k0, kn);
+                    else if (cb == 2) row(in, reinterpret_cast<uint16_t*>(o), k0, kn);
+                    else row(in, reinterpret_cast<uint32_t*>(o), k0, kn);
+                } else {
+                    const uint32_t* in = src32 + r * n2;
+                    if (cb == 1) row(in, reinterpret_cast<uint8_t*>(o), k0, kn);
+                    else if (cb == 2) row(in, reinterpret_cast<uint16_t*>(o), k0, kn);
+                    else row(in, reinterpret_cast<uint32_t*>(o), k0, kn);
                 }
                 e += kn - k0;
             }
@@ -1956,10 +1970,10 @@ int session_new(Gpu* gpu, const HostSim& sim, const RunSpec& rs, Session** out, 
             FG_CUDA(cudaEventCreateWithFlags(&s->aux_done[p], cudaEventDisableTiming));
         }
     }
-    // graphs: a block of even length (the fused step alternates buffers), a pair and singles
+    // graphs: a pair and singles now, a block of even length (the fused step alternates buffers)
+    // when a run first steps that far (a short run never needs it)
     s->graph_steps = 32;
-    rc = capture(*s, s->graph_steps, 0, &s->graph_many, err);
-    if (!rc) rc = capture(*s, 2, 0, &s->graph_two, err);
+    rc = capture(*s, 2, 0, &s->graph_two, err);
     if (!rc) rc = capture(*s, 1, 0, &s->graph_one[0], err);
     if (!rc && s->fused) rc = capture(*s, 1, 1, &s->graph_one[1], err);
     if (rc) { session_free(s.release()); return rc; }
@@ -2041,7 +2055,7 @@ int session_reset(Session* s, std::string& err) {
 }
 
 int session_step(Session* s, uint64_t k, std::string& err) {
-    if (!s->slots && !s->graph_many && !s->graph_one[0]) { err = "this session steps only as part of a batch"; return FG_ERR_INVALID; }
+    if (!s->slots && !s->graph_one[0]) { err = "this session steps only as part of a batch"; return FG_ERR_INVALID; }
     FG_CUDA(cudaSetDevice(s->gpu->device));
     uint64_t done = 0;
     if (s->slots) {
@@ -2065,6 +2079,10 @@ int session_step(Session* s, uint64_t k, std::string& err) {
         const uint64_t left = k - done;
         const int parity = s->fused ? int(s->steps & 1) : 0;
         if (parity == 0 && left >= uint64_t(s->graph_steps)) {
+            if (!s->graph_many) {
+                const int rc = capture(*s, s->graph_steps, 0, &s->graph_many, err);
+                if (rc) return rc;
+            }
             FG_CUDA(cudaGraphLaunch(s->graph_many, s->stream));
             done += s->graph_steps;
             s->steps += s->graph_steps;

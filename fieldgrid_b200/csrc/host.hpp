@@ -101,7 +101,9 @@ struct HostSim {
     size_t nn = 0;
     double dt = 0;
     Axis ax[3];
-    std::vector<uint32_t> node_class;   // nn entries
+    std::vector<uint32_t> node_class;     // nn entries, or empty when node_class16 holds them
+    std::vector<uint16_t> node_class16;   // nn entries when there are at most 65,536 classes
+    uint32_t cls(size_t id) const { return node_class16.empty() ? node_class[id] : uint32_t(node_class16[id]); }
     std::vector<Coef> classes;
     std::vector<PortDef> ports;
     std::vector<std::vector<SrcEdge>> port_src;
@@ -116,8 +118,8 @@ struct HostSim {
 
     size_t cells() const { return (n[0] - 1) * (n[1] - 1) * (n[2] - 1); }
     size_t idx(size_t i, size_t j, size_t k) const { return (i * n[1] + j) * n[2] + k; }
-    float ca(uint32_t c, size_t id) const { return classes[node_class[id]].ca[c]; }
-    float cb(uint32_t c, size_t id) const { return classes[node_class[id]].cb[c]; }
+    float ca(uint32_t c, size_t id) const { return classes[cls(id)].ca[c]; }
+    float cb(uint32_t c, size_t id) const { return classes[cls(id)].cb[c]; }
 };
 
 double time_step(const std::vector<double>* line);

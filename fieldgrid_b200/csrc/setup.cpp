@@ -555,13 +555,21 @@ int sim_try_new(const fg_sim_spec* spec, HostSim** out, std::string& err) {
             remap[t].push_back(g);
         }
     }
+    // the global ids, in 16 bits when the classes allow (half the host memory, and half the bytes the
+    // upload reads)
+    const bool narrow = S.classes.size() <= size_t(65536);
+    if (narrow) S.node_class16.resize(nn);
 #pragma omp parallel num_threads(threads)
     {
         int t = omp_get_thread_num();
         const auto& rm = remap[t];
         size_t a = loc[t].i0 * n[1] * n[2], b = loc[t].i1 * n[1] * n[2];
-        for (size_t id = a; id < b; ++id) S.node_class[id] = rm[S.node_class[id]];
+        if (narrow)
+            for (size_t id = a; id < b; ++id) S.node_class16[id] = uint16_t(rm[S.node_class[id]]);
+        else
+            for (size_t id = a; id < b; ++id) S.node_class[id] = rm[S.node_class[id]];
     }
+    if (narrow) std::vector<uint32_t>().swap(S.node_class);
     for (uint32_t c = 0; c < 3; ++c)
         for (int t = 0; t < threads; ++t)
             S.debye_edges.insert(S.debye_edges.end(), loc[t].debye[c].begin(), loc[t].debye[c].end());

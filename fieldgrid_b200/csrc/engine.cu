@@ -1738,9 +1738,16 @@ int session_new(Gpu* gpu, const HostSim& sim, const RunSpec& rs, Session** out, 
         auto pack = [&](char* buf, size_t off, size_t n) {   // whole records: 1 MB parts hold 2^17 of them
             PackedDebye* o = reinterpret_cast<PackedDebye*>(buf);
             const size_t q0 = off / sizeof(PackedDebye), q1 = (off + n) / sizeof(PackedDebye);
+            // the edges run in node order within a component: the row of the previous edge (its
+            // first node rb, its index r) serves until an edge leaves it, so few edges divide
+            uint64_t rb = 0, r = 0;   // row 0; an edge before rb wraps past n2 and divides
             for (size_t q = q0; q < q1; ++q) {
                 const DebyeEdge& d = de[q];
-                const size_t dv = (d.id / n2) * p2 + d.id % n2;
+                if (d.id - rb >= n2) {
+                    r = d.id / n2;
+                    rb = r * n2;
+                }
+                const size_t dv = r * p2 + (d.id - rb);
                 o[q - q0] = PackedDebye{uint32_t(d.comp) << 30 | uint32_t(dv), float(d.dd)};
             }
         };
